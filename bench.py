@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Build + closest-hit trace throughput on B200 (one JSON line on rank 0).
+
+A step is one pass of the hot path over one batch of synthetic input: build a
+BVH over the mesh, then trace every ray of the batch. The default workload is
+the 4,194,304-triangle clustered scene with 16,777,216 incoherent rays
+(1024 Gaussian clusters, sigma 0.02, vertex offsets +-0.005; origins uniform in
+the scene box, directions uniform on the sphere; 60-bit Morton codes).
+
+value      build throughput, Mtris/s, inputs resident in HBM (CUDA events);
+           trace_mrays_s gives the closest-hit throughput of the same steps.
+e2e        the same metrics through the C ABI with pinned host buffers: the
+           H2D copy of the mesh plus the build (and a read-back of the node
+           counts), then the H2D copy of the rays, the trace and the D2H copy
+           of all hit records.
+roofline   the radix-sort pass (the build's HBM-bound kernel): algorithmic
+           bytes n * 2 * (K + 4) per pass over its average CUDA-event duration.
+Multi-GPU: one process per GPU (torchrun), every rank builds and traces its
+own scene of the same size (independent units, no collective on the data
+path); the reported time is the max over ranks.
+
+--impl reference times the CPU restatement of the same algorithms (the
+reference has no CPU path of its own) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mtris/s build + Mrays/s closest-hit; batched & fwd+bwd vs plain, same B200"
+SEED = 0xC0FFEE
+
+CONFIGS = {
+    "ploc4m": dict(workload="clustered 4,194,304 tris (1024 clusters), 16,777,216 sphere rays, 60-bit",
+                   mesh="clustered", n=4194304, rays=16777216, bits=60, method="lbvh", config_id=1),
+    "lbvh64k": dict(workload="uniform 65,536 tris, 1,048,576 targeted rays, 30-bit", mesh="uniform",
+                    n=65536, rays=1048576, bits=30, method="lbvh", config_id=0),
+}
+DEFAULT_CONFIG = "ploc4m"
+
+
+def make_inputs(cfg, rank):
+    import hippie_b200 as hp
+    seed = SEED + cfg["config_id"] + 1000 * rank
+    if cfg["mesh"] == "uniform":
+        v, t = hp.gen.uniform_mesh(seed, cfg["n"], 0.01)
+        rays = hp.gen.rays_targeted(seed + 1, cfg["rays"], -0.5, 1.5)
+    else:
+        v, t = hp.gen.clustered_mesh(seed, cfg["n"], 1024, 0.02, 0.005)
+        box = np.concatenate([v.min(0), v.max(0)]).astype(np.float32)
+        rays = hp.gen.rays_sphere(seed + 1, cfg["rays"], box)
+    return v, t, rays
+
+
+def build_params(cfg):
+    import hippie_b200 as hp
+    kw = dict(method=cfg["method"], morton_bits=cfg["bits"])
+    if cfg["method"] == "ploc":
+        kw.update(ploc_radius=16, ploc_max_radius=256, ploc_adaptive=0)
+    return hp.BuildParams(**kw)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "50",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), line.strip()))
+
+    def window(self, t0, t1):
+        self.t0, self.t1 = t0, t1
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for ts, line in self.samples:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            rows.append((ts, parts))
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        inside = [r for r in rows if self.t0 is not None and self.t0 - 0.05 <= r[0] <= self.t1 + 0.05]
+        use = inside or rows
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(p[1]) for _, p in use if num(p[1]) is not None]
+        mx = [num(p[2]) for _, p in use if num(p[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, p in use for i in range(4) if p[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(use), "in_window": bool(inside)}
+
+
+def peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def committed_traffic(name):
+    """DRAM bytes per launch of a kernel from a committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(name)
+        except ValueError:
+            return None
+    return None
+
+
+def cpu_baseline(cfg, v, t, rays, budget_s=20.0):
+    """Time the CPU restatement (oracle) on a bounded sample of the workload."""
+    import oracle
+    oracle.load()
+    cores = os.cpu_count() or 1
+    n = cfg["n"]
+    m = min(n, 262144)
+    tt = np.ascontiguousarray(t[:m])
+    t0 = time.perf_counter()
+    r = oracle.build_lbvh(v, tt, bits=cfg["bits"])
+    b_s = time.perf_counter() - t0
+    # scale the sample so build + trace fit the budget
+    m2 = int(min(n, m * max(1.0, 0.5 * budget_s / max(b_s, 1e-3))))
+    if m2 > m:
+        tt = np.ascontiguousarray(t[:m2])
+        t0 = time.perf_counter()
+        r = oracle.build_lbvh(v, tt, bits=cfg["bits"])
+        b_s = time.perf_counter() - t0
+        m = m2
+    k = min(rays.shape[0], 1 << 18)
+    t0 = time.perf_counter()
+    oracle.trace(r["nodes"], r["woop"], r["tri_idx"], rays[:k])
+    tr_s = time.perf_counter() - t0
+    return {"value": m / b_s / 1e6, "unit": "Mtris/s", "cores": cores, "kind": "port",
+            "sample": f"LBVH build of the first {m} triangles; trace of {k} rays on that BVH",
+            "trace_mrays_s": k / tr_s / 1e6}
+
+
+def run_reference(args, cfg, rank):
+    """CPU restatement of the path, timed on the host cores (rank 0 only)."""
+    if rank != 0:
+        return 0
+    import oracle
+    v, t, rays = make_inputs(cfg, 0)
+    oracle.load()
+    steps, warmup = args.steps, args.warmup
+    budget = 150.0 / max(1, steps + warmup)
+    n = cfg["n"]
+    m = min(n, 131072)
+    t0 = time.perf_counter()
+    oracle.build_lbvh(v, np.ascontiguousarray(t[:m]), bits=cfg["bits"])
+    dt = time.perf_counter() - t0
+    m = int(min(n, max(m, m * 0.6 * budget / max(dt, 1e-4))))
+    tm = np.ascontiguousarray(t[:m])
+    k = min(rays.shape[0], 1 << 17)
+    bt, tt = [], []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        r = oracle.build_lbvh(v, tm, bits=cfg["bits"])
+        t1 = time.perf_counter()
+        oracle.trace(r["nodes"], r["woop"], r["tri_idx"], rays[:k])
+        t2 = time.perf_counter()
+        if i >= warmup:
+            bt.append(t1 - t0)
+            tt.append(t2 - t1)
+    b = float(np.mean(bt))
+    tr = float(np.mean(tt))
+    val = m / b / 1e6
+    cores = os.cpu_count() or 1
+    line = {"metric": METRIC, "value": val, "unit": "Mtris/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * (b + tr), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "method": cfg["method"], "sample_tris": m, "sample_rays": k},
+            "trace_mrays_s": k / tr / 1e6,
+            "cpu_baseline": {"value": val, "unit": "Mtris/s", "cores": cores, "kind": "port",
+                             "sample": f"first {m} triangles built, {k} rays traced per step"},
+            "e2e": {"value": val, "unit": "Mtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, cfg, rank)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import hippie_b200 as hp
+    from hippie_b200 import _lib
+    lib = _lib.load()
+    ctx = hp.Context(local)
+    v, t, rays = make_inputs(cfg, rank)
+    n, nr = t.shape[0], rays.shape[0]
+    Vh = torch.from_numpy(v).pin_memory()
+    Th = torch.from_numpy(t).pin_memory()
+    Rh = torch.from_numpy(rays).pin_memory()
+    V, T, R = Vh.cuda(), Th.cuda(), Rh.cuda()
+    RES = torch.empty((nr, 4), dtype=torch.int32, device="cuda")
+    RESh = torch.empty((nr, 4), dtype=torch.int32).pin_memory()
+    params = build_params(cfg)
+    bvh = ctx.build(V, T, params)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ctx.build(V, T, params, bvh=bvh)
+        ctx.trace(bvh, R, results=RES)
+    torch.cuda.synchronize()
+    ctx.check()
+
+    # ---- timed region: inputs resident in HBM (mesh 200 MB + rays 512 MB, larger than L2) ----
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.hp_launch_count()
+    w0 = time.time()
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        ctx.build(V, T, params, bvh=bvh)
+        ev[k][1].record(stream)
+        ctx.trace(bvh, R, results=RES)
+        ev[k][2].record(stream)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    barrier()
+    launches = lib.hp_launch_count() - launches0
+    clocks.window(w0, w1)
+    time.sleep(0.1)
+    clocks.stop()
+    ctx.check()
+    build_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+    trace_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    step_ms = float(ev[0][0].elapsed_time(ev[-1][2])) / args.steps
+    if world > 1:
+        tt = torch.tensor([build_ms, trace_ms, step_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        build_ms, trace_ms, step_ms = tt.tolist()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e_b, e2e_t = [], []
+    for k in range(max(3, args.steps // 2)):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        V.copy_(Vh, non_blocking=True)
+        T.copy_(Th, non_blocking=True)
+        ctx.build(V, T, params, bvh=bvh)
+        bvh.sync()
+        b = time.perf_counter()
+        R.copy_(Rh, non_blocking=True)
+        ctx.trace(bvh, R, results=RES)
+        RESh.copy_(RES, non_blocking=True)
+        torch.cuda.synchronize()
+        c = time.perf_counter()
+        e2e_b.append(b - a)
+        e2e_t.append(c - b)
+    e2e_b_s, e2e_t_s = float(np.median(e2e_b)), float(np.median(e2e_t))
+    if world > 1:
+        tt = torch.tensor([e2e_b_s, e2e_t_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_b_s, e2e_t_s = tt.tolist()
+
+    # ---- roofline of the radix-sort pass (per-pass CUDA events on the build stream) ----
+    lib.hp_profile_reset(ctx.h)
+    lib.hp_profile_enable(ctx.h, 1)
+    ctx.build(V, T, params, bvh=bvh)
+    torch.cuda.synchronize()
+    import ctypes as C
+    phases = {}
+    passes = []
+    for i in range(1, lib.hp_profile_count(ctx.h)):
+        nm = C.create_string_buffer(64)
+        ms = C.c_float()
+        lib.hp_profile_get(ctx.h, i, nm, 64, C.byref(ms))
+        name = nm.value.decode()
+        phases[name] = phases.get(name, 0.0) + ms.value
+        if name == "sort_pass":
+            passes.append(ms.value)
+    lib.hp_profile_enable(ctx.h, 0)
+    lib.hp_profile_reset(ctx.h)
+    kb = 4 if cfg["bits"] <= 32 else 8
+    pass_bytes = n * 2 * (kb + 4)
+    pass_ms = float(np.mean(passes)) if passes else float("nan")
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    peak, peak_kind = peak_hbm()
+    traffic = committed_traffic("sort_pass")
+
+    line = {
+        "metric": METRIC, "value": world * n / (build_ms * 1e-3) / 1e6, "unit": "Mtris/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "method": cfg["method"], "triangles": n, "rays": nr,
+                   "morton_bits": cfg["bits"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (mesh 200 MB, rays 512 MB)"},
+        "trace_mrays_s": world * nr / (trace_ms * 1e-3) / 1e6,
+        "build_ms": build_ms, "trace_ms": trace_ms,
+        "phases_ms": {k: round(x, 4) for k, x in phases.items()},
+        "e2e": {"value": world * n / e2e_b_s / 1e6, "unit": "Mtris/s",
+                "trace_mrays_s": world * nr / e2e_t_s / 1e6,
+                "h2d_bytes_per_step": int(v.nbytes + t.nbytes + rays.nbytes),
+                "d2h_bytes_per_step": int(nr * 16 + 8)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix sort pass)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": pass_bytes,
+                     "launch_ms": pass_ms},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, v, t, rays)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del bvh
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

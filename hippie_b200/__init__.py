@@ -1,0 +1,255 @@
+"""hippie_b200 — B200-native LBVH/PLOC BVH construction and closest-hit traversal.
+
+Python access to the C ABI (include/hippie_b200.h) for tests and benchmarks.
+Device buffers are torch CUDA tensors (plumbing only); all computation happens
+in the CUDA kernels of libhippie_b200.so.
+
+Mirrors the reference's builder / tracer objects (src/hippie/rt/bvh/BVHBuilder.h,
+rt/bvh/HipBVH.h, rt/tracer/HipTracer.h) as `Context.build`, `BVH`, `Context.trace`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT, HP_TRACE_STATS,
+                   HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, load)
+
+__all__ = ["Context", "BVH", "BuildParams", "Env", "HPError", "gen", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
+           "HP_METHOD_ATR", "HP_TRACE_ANY_HIT", "HP_TRACE_STATS", "load"]
+
+
+def _ptr(t):
+    return C.c_void_p(0) if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class BuildParams:
+    """hp_build_params with the reference's defaults (environment/AppEnvironment.cpp:52-75)."""
+
+    def __init__(self, **kw):
+        self.c = hp_build_params()
+        load().hp_build_params_default(C.byref(self.c))
+        for k, v in kw.items():
+            if k == "method" and isinstance(v, str):
+                v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR}[v]
+            setattr(self.c, k, v)
+
+    def __getattr__(self, k):
+        return getattr(self.__dict__["c"], k)
+
+
+class Env:
+    """Environment file (Environment / AppEnvironment) with the reference's keys."""
+
+    def __init__(self):
+        self.h = C.c_void_p()
+        check(load().hp_env_create(C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            load().hp_env_destroy(self.h)
+            self.h = None
+
+    def read_string(self, text: str):
+        check(load().hp_env_read_string(self.h, text.encode()))
+        return self
+
+    def read_file(self, path: str):
+        check(load().hp_env_read_file(self.h, str(path).encode()))
+        return self
+
+    def get_int(self, name):
+        v = C.c_int32()
+        check(load().hp_env_get_int(self.h, name.encode(), C.byref(v)))
+        return v.value
+
+    def get_float(self, name):
+        v = C.c_float()
+        check(load().hp_env_get_float(self.h, name.encode(), C.byref(v)))
+        return v.value
+
+    def get_bool(self, name):
+        v = C.c_int32()
+        check(load().hp_env_get_bool(self.h, name.encode(), C.byref(v)))
+        return bool(v.value)
+
+    def get_string(self, name):
+        buf = C.create_string_buffer(4096)
+        check(load().hp_env_get_string(self.h, name.encode(), buf, 4096))
+        return buf.value.decode()
+
+    def build_params(self) -> BuildParams:
+        p = BuildParams()
+        check(load().hp_env_build_params(self.h, C.byref(p.c)))
+        return p
+
+
+class BVH:
+    """A built BVH (HipBVH): 64-byte binary nodes, Woop triangles, triangle indices."""
+
+    def __init__(self, ctx: "Context"):
+        self.ctx = ctx
+        self.c = hp_bvh()
+
+    def __del__(self):
+        if getattr(self, "c", None) is not None and self.c.impl:
+            load().hp_bvh_free(self.ctx.h, C.byref(self.c))
+
+    def sync(self, stream=None):
+        check(load().hp_bvh_sync(self.ctx.h, C.byref(self.c), _stream_ptr(stream)))
+        return self
+
+    @property
+    def num_nodes(self):
+        return self.c.num_interior + self.c.num_leaf
+
+    def cost(self, stream=None) -> float:
+        v = C.c_double()
+        check(load().hp_bvh_cost(self.ctx.h, C.byref(self.c), C.byref(v), _stream_ptr(stream)))
+        return v.value
+
+    def validate(self, verts, tris, stream=None) -> bool:
+        m = _mesh(verts, tris)
+        ok = C.c_int32()
+        check(load().hp_bvh_validate(self.ctx.h, C.byref(self.c), C.byref(m), C.byref(ok), _stream_ptr(stream)))
+        return bool(ok.value)
+
+    def download(self, stream=None):
+        """Copy nodes (N x 16 int32), woop (n x 12 float32) and triangle indices to the host."""
+        self.sync(stream)
+        nodes = np.zeros((self.num_nodes, 16), np.int32)
+        woop = np.zeros((self.c.num_refs, 12), np.float32)
+        tri = np.zeros(self.c.num_refs, np.int32)
+        check(load().hp_bvh_download(self.ctx.h, C.byref(self.c), nodes.ctypes.data, woop.ctypes.data,
+                                     tri.ctypes.data, _stream_ptr(stream)))
+        return nodes, woop, tri
+
+
+def _mesh(verts, tris) -> hp_mesh:
+    m = hp_mesh()
+    m.vertices = verts.data_ptr() if verts is not None and verts.numel() else None
+    m.triangles = tris.data_ptr() if tris is not None and tris.numel() else None
+    m.num_vertices = verts.shape[0] if verts is not None else 0
+    m.num_triangles = tris.shape[0] if tris is not None else 0
+    return m
+
+
+class Context:
+    """One hp_ctx per device and host thread (library scratch arena + error words)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        check(load().hp_ctx_create(C.byref(self.h), device))
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().hp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def check(self, stream=None):
+        check(load().hp_ctx_check(self.h, _stream_ptr(stream)))
+
+    def build(self, verts, tris, params: BuildParams | None = None, bvh: BVH | None = None, taps=None,
+              stream=None) -> BVH:
+        """Build (or rebuild into `bvh`) over float32 (V,3) vertices and int32 (T,3) triangles."""
+        params = params or BuildParams()
+        bvh = bvh or BVH(self)
+        m = _mesh(verts, tris)
+        tp = None
+        if taps is not None:
+            tp = hp_build_taps()
+            for k, v in taps.items():
+                setattr(tp, k, v.data_ptr())
+        check(load().hp_build(self.h, C.byref(m), C.byref(params.c), C.byref(bvh.c),
+                              C.byref(tp) if tp is not None else None, _stream_ptr(stream)))
+        return bvh
+
+    def refit(self, bvh: BVH, verts, tris, stream=None):
+        m = _mesh(verts, tris)
+        check(load().hp_refit(self.h, C.byref(bvh.c), C.byref(m), _stream_ptr(stream)))
+
+    def trace(self, bvh: BVH, rays, results=None, stats=None, any_hit=False, stream=None):
+        """rays: float32 (R, 8) CUDA tensor. Returns int32 (R, 4) results (and stats if given)."""
+        import torch
+        n = rays.shape[0]
+        if results is None:
+            results = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+        flags = (HP_TRACE_ANY_HIT if any_hit else 0) | (HP_TRACE_STATS if stats is not None else 0)
+        check(load().hp_trace(self.h, C.byref(bvh.c), _ptr(rays), n, _ptr(results), _ptr(stats), flags,
+                              _stream_ptr(stream)))
+        return results
+
+    def adjoint(self, verts, tris, rays, results, dl_dtuv, dl_dverts=None, stream=None):
+        import torch
+        if dl_dverts is None:
+            dl_dverts = torch.zeros_like(verts)
+        m = _mesh(verts, tris)
+        check(load().hp_trace_adjoint(self.h, C.byref(m), _ptr(rays), _ptr(results), _ptr(dl_dtuv),
+                                      rays.shape[0], _ptr(dl_dverts), _stream_ptr(stream)))
+        return dl_dverts
+
+    def radix_sort(self, keys, vals=None, bits=None, stream=None):
+        import torch
+        kb = keys.element_size()
+        bits = bits or 8 * kb
+        ko = torch.empty_like(keys)
+        vo = torch.empty(keys.shape[0], dtype=torch.int32, device=keys.device)
+        check(load().hp_radix_sort(self.h, _ptr(keys), _ptr(vals), _ptr(ko), _ptr(vo), keys.shape[0], kb, bits,
+                                   _stream_ptr(stream)))
+        return ko, vo
+
+
+class gen:
+    """Synthetic inputs (host numpy arrays) from the library's deterministic generators."""
+
+    @staticmethod
+    def uniform_mesh(seed, n, half_extent=0.01):
+        v = np.empty((3 * n, 3), np.float32)
+        t = np.empty((n, 3), np.int32)
+        check(load().hp_gen_uniform_mesh(seed, n, half_extent, v.ctypes.data, t.ctypes.data))
+        return v, t
+
+    @staticmethod
+    def clustered_mesh(seed, n, clusters=1024, sigma=0.02, half_extent=0.005):
+        v = np.empty((3 * n, 3), np.float32)
+        t = np.empty((n, 3), np.int32)
+        check(load().hp_gen_clustered_mesh(seed, n, clusters, sigma, half_extent, v.ctypes.data, t.ctypes.data))
+        return v, t
+
+    @staticmethod
+    def heightfield(seed, nx=512, ny=1024, sx=1.0, sy=2.0, waves=16):
+        v = np.empty((nx * ny, 3), np.float32)
+        t = np.empty((2 * (nx - 1) * (ny - 1), 3), np.int32)
+        check(load().hp_gen_heightfield(seed, nx, ny, sx, sy, waves, v.ctypes.data, t.ctypes.data))
+        return v, t
+
+    @staticmethod
+    def rays_targeted(seed, n, lo=-0.5, hi=1.5):
+        r = np.empty((n, 8), np.float32)
+        check(load().hp_gen_rays_targeted(seed, n, lo, hi, r.ctypes.data))
+        return r
+
+    @staticmethod
+    def rays_sphere(seed, n, box):
+        r = np.empty((n, 8), np.float32)
+        b = np.ascontiguousarray(box, np.float32)
+        check(load().hp_gen_rays_sphere(seed, n, b.ctypes.data, r.ctypes.data))
+        return r
+
+    @staticmethod
+    def rays_grid_down(seed, nx, ny, sx=1.0, sy=2.0, z0=1.0):
+        r = np.empty((nx * ny, 8), np.float32)
+        check(load().hp_gen_rays_grid_down(seed, nx, ny, sx, sy, z0, r.ctypes.data))
+        return r

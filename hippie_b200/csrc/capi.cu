@@ -1,0 +1,512 @@
+// C ABI entry points: context and scratch arena, BVH objects, build / refit /
+// trace / adjoint dispatch, host-side cost and validation.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "hp_device.cuh"
+#include "hp_internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+thread_local int64_t g_launches = 0;
+}
+
+void hp_count_launch(int k) { g_launches += k; }
+
+void hp_mark(hp_ctx* ctx, cudaStream_t s, const char* name) {
+    if (!ctx || !ctx->profiling) return;
+    if (ctx->num_marks == ctx->cap_marks) {
+        int cap = ctx->cap_marks ? 2 * ctx->cap_marks : 64;
+        hp_prof_mark* m = new hp_prof_mark[cap];
+        for (int i = 0; i < ctx->num_marks; ++i) m[i] = ctx->marks[i];
+        for (int i = ctx->num_marks; i < cap; ++i) cudaEventCreate(&m[i].ev);
+        delete[] ctx->marks;
+        ctx->marks = m;
+        ctx->cap_marks = cap;
+    }
+    hp_prof_mark& mk = ctx->marks[ctx->num_marks++];
+    std::snprintf(mk.name, sizeof(mk.name), "%s", name);
+    cudaEventRecord(mk.ev, s);
+}
+
+void hp_set_error(const std::string& msg) { g_last_error = msg; }
+
+hp_status hp_fail(hp_status code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+hp_status hp_cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return HP_ERR_OOM;
+    }
+    return HP_ERR_CUDA;
+}
+
+hp_status hp_ctx_reserve(hp_ctx* ctx, size_t bytes, cudaStream_t stream) {
+    if (bytes <= ctx->arena_bytes) return HP_OK;
+    // Growing the arena: wait for work that may still use the old one.
+    HP_CUDA(cudaDeviceSynchronize());
+    if (ctx->arena) HP_CUDA(cudaFree(ctx->arena));
+    ctx->arena = nullptr;
+    ctx->arena_bytes = 0;
+    size_t grow = std::max(bytes, bytes + bytes / 8);
+    cudaError_t e = cudaMalloc(&ctx->arena, grow);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&ctx->arena, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return hp_fail(HP_ERR_OOM, "scratch arena: cannot allocate " + std::to_string(bytes) + " bytes");
+        }
+        grow = bytes;
+    }
+    ctx->arena_bytes = grow;
+    (void)stream;
+    return HP_OK;
+}
+
+namespace {
+
+hp_status check_mesh(const hp_mesh* m) {
+    if (!m) return hp_fail(HP_ERR_ARG, "mesh is null");
+    if (m->num_triangles < 0 || m->num_vertices < 0) return hp_fail(HP_ERR_ARG, "negative mesh size");
+    if (m->num_triangles > 0 && (!m->vertices || !m->triangles))
+        return hp_fail(HP_ERR_ARG, "mesh pointers are null");
+    if (m->num_triangles >= (int64_t(1) << 29))
+        return hp_fail(HP_ERR_ARG, "mesh too large: at most 2^29 - 1 triangles per BVH");
+    return HP_OK;
+}
+
+hp_status check_params(const hp_build_params* p) {
+    if (!p) return hp_fail(HP_ERR_ARG, "build params are null");
+    if (p->morton_bits < 6 || p->morton_bits > 60) return hp_fail(HP_ERR_ARG, "morton_bits must be in [6,60]");
+    if (p->ct <= 0.0f || p->ci <= 0.0f) return hp_fail(HP_ERR_ARG, "ct and ci must be positive");
+    if (p->max_leaf_size <= 0 || p->max_leaf_size > 1024) return hp_fail(HP_ERR_ARG, "max_leaf_size must be in (0,1024]");
+    if (p->method == HP_METHOD_PLOC) {
+        if (p->ploc_max_radius < 1) return hp_fail(HP_ERR_ARG, "ploc_max_radius must be positive");
+        if (p->ploc_radius < 1 || p->ploc_radius > p->ploc_max_radius)
+            return hp_fail(HP_ERR_ARG, "ploc_radius must be in [1, ploc_max_radius]");
+    } else if (p->method == HP_METHOD_ATR) {
+        if (p->atr_iterations < 0 || p->atr_iterations > 25) return hp_fail(HP_ERR_ARG, "atr_iterations must be in [0,25]");
+        if (p->atr_treelet < 4 || p->atr_treelet > 30) return hp_fail(HP_ERR_ARG, "atr_treelet must be in [4,30]");
+    } else if (p->method != HP_METHOD_LBVH) {
+        return hp_fail(HP_ERR_ARG, "unknown build method");
+    }
+    return HP_OK;
+}
+
+hp_status bvh_alloc(hp_bvh* out, int64_t n) {
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
+    if (b && b->capacity >= n && b->nodes) return HP_OK;
+    if (b) {
+        cudaFree(b->nodes);
+        cudaFree(b->woop);
+        cudaFree(b->tri_idx);
+        cudaFree(b->counters);
+        cudaFree(b->info);
+    } else {
+        b = new hp_bvh_impl();
+        out->impl = b;
+    }
+    *b = hp_bvh_impl();
+    const int64_t cap = std::max<int64_t>(n, 2);
+    const int64_t max_nodes = std::max<int64_t>(2 * cap - 1, 3);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&b->nodes, max_nodes * sizeof(hp_node_bin));
+    if (e == cudaSuccess) e = cudaMalloc(&b->woop, 3 * cap * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc(&b->tri_idx, cap * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->counters, cap * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->info, sizeof(hp_bvh_info));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(b->nodes); cudaFree(b->woop); cudaFree(b->tri_idx); cudaFree(b->counters); cudaFree(b->info);
+        *b = hp_bvh_impl();
+        return hp_fail(HP_ERR_OOM, "BVH allocation failed for " + std::to_string(n) + " references");
+    }
+    HP_CUDA(cudaMemset(b->info, 0, sizeof(hp_bvh_info)));
+    b->capacity = cap;
+    out->nodes = b->nodes;
+    out->woop = b->woop;
+    out->tri_indices = b->tri_idx;
+    out->capacity_refs = cap;
+    return HP_OK;
+}
+
+float ord2f_host(uint32_t u) {
+    uint32_t v = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    float f;
+    std::memcpy(&f, &v, 4);
+    return f;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hp_last_error(void) { return g_last_error.c_str(); }
+int32_t hp_abi_version(void) { return HP_ABI_VERSION; }
+int64_t hp_launch_count(void) { return g_launches; }
+
+hp_status hp_profile_enable(hp_ctx* ctx, int32_t on) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_profile_enable: null context");
+    ctx->profiling = on != 0;
+    return HP_OK;
+}
+
+hp_status hp_profile_reset(hp_ctx* ctx) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_profile_reset: null context");
+    ctx->num_marks = 0;
+    return HP_OK;
+}
+
+int32_t hp_profile_count(hp_ctx* ctx) { return ctx ? ctx->num_marks : 0; }
+
+// Phase i (>= 1) is the interval from mark i-1 to mark i, named after mark i.
+hp_status hp_profile_get(hp_ctx* ctx, int32_t i, char* name, int64_t name_size, float* ms) {
+    if (!ctx || i < 1 || i >= ctx->num_marks) return hp_fail(HP_ERR_ARG, "hp_profile_get: bad index");
+    HP_CUDA(cudaEventSynchronize(ctx->marks[i].ev));
+    float t = 0.0f;
+    HP_CUDA(cudaEventElapsedTime(&t, ctx->marks[i - 1].ev, ctx->marks[i].ev));
+    if (ms) *ms = t;
+    if (name && name_size > 0) std::snprintf(name, (size_t)name_size, "%s", ctx->marks[i].name);
+    return HP_OK;
+}
+
+hp_status hp_ctx_create(hp_ctx** out, int32_t device) {
+    if (!out) return hp_fail(HP_ERR_ARG, "hp_ctx_create: null output");
+    *out = nullptr;
+    int count = 0;
+    HP_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return hp_fail(HP_ERR_ARG, "hp_ctx_create: no such device");
+    HP_CUDA(cudaSetDevice(device));
+    hp_ctx* c = new hp_ctx();
+    c->device = device;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) { delete c; return hp_cuda_fail(e, "cudaGetDeviceProperties"); }
+    c->sm_count = prop.multiProcessorCount;
+    c->l2_bytes = prop.l2CacheSize;
+    e = cudaMalloc(&c->d_status, 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, 64 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_status, 64 * sizeof(int));
+    if (e != cudaSuccess) {
+        cudaFree(c->d_status);
+        delete c;
+        return hp_cuda_fail(e, "hp_ctx_create");
+    }
+    *out = c;
+    return HP_OK;
+}
+
+hp_status hp_ctx_destroy(hp_ctx* ctx) {
+    if (!ctx) return HP_OK;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    cudaFree(ctx->arena);
+    cudaFree(ctx->d_status);
+    cudaFreeHost(ctx->h_status);
+    for (int i = 0; i < ctx->cap_marks; ++i) cudaEventDestroy(ctx->marks[i].ev);
+    delete[] ctx->marks;
+    delete ctx;
+    return HP_OK;
+}
+
+hp_status hp_ctx_check(hp_ctx* ctx, void* stream) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_check: null context");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_CUDA(cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    HP_CUDA(cudaStreamSynchronize(s));
+    if (ctx->h_status[0] != 0) {
+        int code = ctx->h_status[0], info = ctx->h_status[1];
+        HP_CUDA(cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(int), s));
+        HP_CUDA(cudaStreamSynchronize(s));
+        const char* what = code == HP_DEV_SPIN_LIMIT ? "bounded wait gave up"
+                         : code == HP_DEV_BAD_INDEX ? "index out of range"
+                         : code == HP_DEV_STACK_OVERFLOW ? "traversal stack overflow"
+                         : code == HP_DEV_BAD_INPUT ? "invalid input (vertex index out of range)"
+                                                    : "device error";
+        return hp_fail(HP_ERR_DEVICE_STATUS, std::string("kernel reported: ") + what + " (info " +
+                                                 std::to_string(info) + ")");
+    }
+    return HP_OK;
+}
+
+void hp_build_params_default(hp_build_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->method = HP_METHOD_LBVH;
+    p->morton_bits = 60;
+    p->ploc_radius = 1;
+    p->ploc_max_radius = 512;
+    p->ploc_adaptive = 0;
+    p->atr_iterations = 2;
+    p->atr_treelet = 20;
+    p->ct = 3.0f;
+    p->ci = 2.0f;
+    p->max_leaf_size = 8;
+    p->adaptive_leaf = 1;
+}
+
+hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh* out,
+                   const hp_build_taps* taps, void* stream) {
+    if (!ctx || !out) return hp_fail(HP_ERR_ARG, "hp_build: null argument");
+    HP_TRY(check_mesh(m));
+    HP_TRY(check_params(p));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int64_t n = m->num_triangles;
+    HP_TRY(bvh_alloc(out, n));
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
+    out->num_refs = n;
+    out->method = p->method;
+    out->ct = p->ct;
+    out->ci = p->ci;
+    out->num_interior = out->num_leaf = -1;
+    if (n == 0) {
+        HP_CUDA(cudaMemsetAsync(b->info, 0, sizeof(hp_bvh_info), s));
+        return HP_OK;
+    }
+    hp_mark(ctx, s, "begin");
+    if (p->method == HP_METHOD_PLOC && n > 1) return hp_ploc_build(ctx, m, p, b, taps, s);
+    if (p->method == HP_METHOD_ATR) return hp_fail(HP_ERR_UNSUPPORTED, "ATR builder not available in this build");
+    return hp_lbvh_build(ctx, m, p, b, taps, s);
+}
+
+hp_status hp_bvh_sync(hp_ctx* ctx, hp_bvh* bvh, void* stream) {
+    if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_sync: null argument");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(bvh->impl);
+    hp_bvh_info info;
+    HP_CUDA(cudaMemcpyAsync(&info, b->info, sizeof(info), cudaMemcpyDeviceToHost, s));
+    HP_CUDA(cudaStreamSynchronize(s));
+    HP_TRY(hp_ctx_check(ctx, stream));
+    bvh->num_interior = info.num_interior;
+    bvh->num_leaf = info.num_leaf;
+    for (int k = 0; k < 6; ++k) bvh->scene_box[k] = ord2f_host(info.box_ord[k]);
+    for (int k = 0; k < 3; ++k) bvh->morton_scale[k] = info.scale[k];
+    return HP_OK;
+}
+
+hp_status hp_bvh_download(hp_ctx* ctx, hp_bvh* bvh, void* nodes_host, void* woop_host, int32_t* tri_host,
+                          void* stream) {
+    HP_TRY(hp_bvh_sync(ctx, bvh, stream));
+    const int64_t count = (int64_t)bvh->num_interior + bvh->num_leaf;
+    const int64_t n = bvh->num_refs;
+    if (nodes_host && count > 0)
+        HP_CUDA(cudaMemcpy(nodes_host, bvh->nodes, count * sizeof(hp_node_bin), cudaMemcpyDeviceToHost));
+    if (woop_host && n > 0)
+        HP_CUDA(cudaMemcpy(woop_host, bvh->woop, n * 3 * sizeof(float4), cudaMemcpyDeviceToHost));
+    if (tri_host && n > 0)
+        HP_CUDA(cudaMemcpy(tri_host, bvh->tri_indices, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh) {
+    (void)ctx;
+    if (!bvh) return HP_OK;
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(bvh->impl);
+    if (b) {
+        cudaFree(b->nodes);
+        cudaFree(b->woop);
+        cudaFree(b->tri_idx);
+        cudaFree(b->counters);
+        cudaFree(b->info);
+        delete b;
+    }
+    std::memset(bvh, 0, sizeof(*bvh));
+    return HP_OK;
+}
+
+namespace {
+struct host_node {
+    float f[12];
+    int32_t c0, c1, size, parent;
+};
+static_assert(sizeof(host_node) == 64, "host node");
+
+float area_of(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
+    if (!(mnx <= mxx && mny <= mxy && mnz <= mxz)) return 0.0f;
+    float dx = mxx - mnx, dy = mxy - mny, dz = mxz - mnz;
+    return 2.0f * std::fmaf(dz, dx, std::fmaf(dx, dy, dy * dz));
+}
+
+// Union of the two child boxes stored in a node (HipBVHNodeN<2>::getBoundingBox).
+void node_box(const host_node& n, float* mn, float* mx) {
+    mn[0] = std::min(n.f[0], n.f[4]); mx[0] = std::max(n.f[1], n.f[5]);
+    mn[1] = std::min(n.f[2], n.f[6]); mx[1] = std::max(n.f[3], n.f[7]);
+    mn[2] = std::min(n.f[8], n.f[10]); mx[2] = std::max(n.f[9], n.f[11]);
+}
+
+hp_status fetch_nodes(hp_ctx* ctx, hp_bvh* bvh, std::vector<host_node>& nodes, void* stream) {
+    HP_TRY(hp_bvh_sync(ctx, bvh, stream));
+    const int64_t count = (int64_t)bvh->num_interior + bvh->num_leaf;
+    nodes.resize(count);
+    if (count)
+        HP_CUDA(cudaMemcpy(nodes.data(), bvh->nodes, count * sizeof(host_node), cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+}  // namespace
+
+hp_status hp_bvh_cost(hp_ctx* ctx, const hp_bvh* bvh_in, double* cost, void* stream) {
+    if (!ctx || !bvh_in || !cost || !bvh_in->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_cost: null argument");
+    hp_bvh bvh = *bvh_in;
+    std::vector<host_node> nodes;
+    HP_TRY(fetch_nodes(ctx, &bvh, nodes, stream));
+    const float* sb = bvh.scene_box;
+    const double scene_area = area_of(sb[0], sb[1], sb[2], sb[3], sb[4], sb[5]);
+    double c = 0.0;
+    for (const host_node& n : nodes) {
+        float mn[3], mx[3];
+        node_box(n, mn, mx);
+        double a = area_of(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) / scene_area;
+        if (n.size < 0) c += (double)bvh.ci * a * (double)(~n.size);
+        else c += (double)bvh.ct * a;
+    }
+    *cost = c;
+    return HP_OK;
+}
+
+// HipBVH::validate (rt/bvh/HipBVH.cpp:157-307): every triangle referenced once,
+// parent links, node sizes, non-empty leaves whose box overlaps their
+// triangles, every node reachable exactly once. Also checks that child boxes
+// contain the triangles below them.
+hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh_in, const hp_mesh* m, int32_t* valid,
+                          void* stream) {
+    if (!ctx || !bvh_in || !valid || !bvh_in->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: null argument");
+    HP_TRY(check_mesh(m));
+    *valid = 0;
+    hp_bvh bvh = *bvh_in;
+    std::vector<host_node> nodes;
+    HP_TRY(fetch_nodes(ctx, &bvh, nodes, stream));
+    const int64_t n = bvh.num_refs;
+    if (n != m->num_triangles) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: mesh does not match the BVH");
+    if (n == 0) { *valid = nodes.empty(); return HP_OK; }
+    std::vector<int32_t> tri(n), tris(3 * m->num_triangles);
+    std::vector<float> verts(3 * m->num_vertices);
+    HP_CUDA(cudaMemcpy(tri.data(), bvh.tri_indices, n * 4, cudaMemcpyDeviceToHost));
+    HP_CUDA(cudaMemcpy(tris.data(), m->triangles, tris.size() * 4, cudaMemcpyDeviceToHost));
+    HP_CUDA(cudaMemcpy(verts.data(), m->vertices, verts.size() * 4, cudaMemcpyDeviceToHost));
+    bool ok = true;
+    std::string why;
+    auto bad = [&](const std::string& w) { if (ok) why = w; ok = false; };
+    const int64_t count = (int64_t)nodes.size();
+    std::vector<int> seen(count, 0), tri_seen(n, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        if (tri[i] < 0 || tri[i] >= n) { bad("invalid triangle index"); break; }
+        tri_seen[tri[i]]++;
+    }
+    for (int64_t i = 0; i < n && ok; ++i)
+        if (tri_seen[i] != 1) bad("triangle not referenced exactly once");
+    std::vector<int64_t> stack{0};
+    if (count == 0) bad("no nodes");
+    else seen[0] = 1;
+    if (ok && nodes[0].parent != -1) bad("root parent is not -1");
+    while (ok && !stack.empty()) {
+        int64_t ni = stack.back();
+        stack.pop_back();
+        const host_node& nd = nodes[ni];
+        if (nd.size >= 0) {
+            if (ni >= bvh.num_interior) { bad("interior node in the leaf range"); break; }
+            int64_t size = 0;
+            for (int c = 0; c < 2; ++c) {
+                int32_t raw = c == 0 ? nd.c0 : nd.c1;
+                int64_t ci = raw < 0 ? ~raw : raw;
+                if (ci <= 0 || ci >= count) { bad("child index out of range"); break; }
+                const host_node& ch = nodes[ci];
+                if ((raw < 0) != (ch.size < 0)) { bad("child leaf flag mismatch"); break; }
+                if (ch.parent != ni) { bad("invalid parent index"); break; }
+                size += ch.size < 0 ? ~ch.size : ch.size;
+                seen[ci]++;
+                stack.push_back(ci);
+                // the child box stored here must contain the child's own box
+                float cmn[3], cmx[3];
+                node_box(ch, cmn, cmx);
+                const float* f = nd.f;
+                float bmn[3] = {f[4 * c + 0], f[4 * c + 2], f[8 + 2 * c]};
+                float bmx[3] = {f[4 * c + 1], f[4 * c + 3], f[9 + 2 * c]};
+                bool empty_child = (ch.size < 0) && (ch.c0 == ch.c1);
+                for (int a = 0; a < 3 && !empty_child; ++a)
+                    if (cmn[a] < bmn[a] || cmx[a] > bmx[a]) { bad("child box not enclosed"); break; }
+            }
+            if (ok && size != nd.size) bad("invalid node size");
+        } else {
+            if (ni < bvh.num_interior) { bad("leaf node in the interior range"); break; }
+            int32_t b0 = nd.c0, e0 = nd.c1;
+            if (b0 > e0 || b0 < 0 || e0 > n || (b0 == e0 && n != 1)) { bad("invalid leaf bounds"); break; }
+            if (e0 - b0 != ~nd.size) { bad("leaf size does not match its range"); break; }
+            float mn[3], mx[3];
+            node_box(nd, mn, mx);
+            for (int32_t r = b0; r < e0 && ok; ++r) {
+                const int32_t t = tri[r];
+                for (int k = 0; k < 3; ++k) {
+                    int32_t vi = tris[3 * (int64_t)t + k];
+                    if (vi < 0 || vi >= m->num_vertices) { bad("vertex index out of range"); break; }
+                    for (int a = 0; a < 3; ++a) {
+                        float x = verts[3 * (int64_t)vi + a];
+                        if (x < mn[a] || x > mx[a]) { bad("triangle is not in its leaf box"); break; }
+                    }
+                }
+            }
+        }
+    }
+    for (int64_t i = 0; i < count && ok; ++i)
+        if (seen[i] != 1) bad("node not referenced exactly once");
+    if (!ok) hp_set_error("validate: " + why);
+    *valid = ok ? 1 : 0;
+    return HP_OK;
+}
+
+hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
+    if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_refit: null argument");
+    HP_TRY(check_mesh(m));
+    if (m->num_triangles != bvh->num_refs) return hp_fail(HP_ERR_ARG, "hp_refit: mesh does not match the BVH");
+    return hp_refit_launch(ctx, reinterpret_cast<hp_bvh_impl*>(bvh->impl), bvh->num_refs, m,
+                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays, int32_t* results,
+                   int32_t* stats, uint32_t flags, void* stream) {
+    if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_trace: null argument");
+    if (num_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace: negative ray count");
+    if (num_rays > 0 && (!rays || !results)) return hp_fail(HP_ERR_ARG, "hp_trace: null ray or result buffer");
+    return hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays,
+                           num_rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays, const int32_t* results,
+                           const float* dl_dtuv, int64_t num_rays, float* dl_dvertices, void* stream) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_trace_adjoint: null context");
+    HP_TRY(check_mesh(m));
+    if (num_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_adjoint: negative ray count");
+    if (num_rays > 0 && (!rays || !results || !dl_dtuv || !dl_dvertices))
+        return hp_fail(HP_ERR_ARG, "hp_trace_adjoint: null buffer");
+    return hp_adjoint_launch(ctx, m, rays, results, dl_dtuv, num_rays, dl_dvertices,
+                             reinterpret_cast<cudaStream_t>(stream));
+}
+
+hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in, void* keys_out,
+                        int32_t* vals_out, int64_t n, int32_t key_bytes, int32_t bits, void* stream) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_radix_sort: null context");
+    if (key_bytes != 4 && key_bytes != 8) return hp_fail(HP_ERR_ARG, "hp_radix_sort: key_bytes must be 4 or 8");
+    if (bits < 1 || bits > 8 * key_bytes) return hp_fail(HP_ERR_ARG, "hp_radix_sort: bits out of range");
+    if (n < 0 || n >= (int64_t(1) << 30)) return hp_fail(HP_ERR_ARG, "hp_radix_sort: n out of range");
+    if (n == 0) return HP_OK;
+    if (!keys_in || !keys_out || !vals_out) return hp_fail(HP_ERR_ARG, "hp_radix_sort: null buffer");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    hp_sort_plan plan = hp_sort_make_plan(n, key_bytes, bits);
+    const size_t hist_bytes = hp_carve::pad(hp_sort_hist_bytes(plan.passes));
+    HP_TRY(hp_ctx_reserve(ctx, hp_carve::pad(plan.scratch_bytes) + hist_bytes, s));
+    hp_carve cv(ctx->arena);
+    void* scratch = cv.take<char>(plan.scratch_bytes);
+    uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false, ctx->d_status, ctx};
+    return hp_sort_run(plan, a, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+// Host-side internal declarations shared by the library's translation units.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/hippie_b200.h"
+
+struct hp_node_bin;
+
+// ---- error handling ------------------------------------------------------
+void hp_set_error(const std::string& msg);
+hp_status hp_fail(hp_status code, const std::string& msg);
+hp_status hp_cuda_fail(cudaError_t e, const char* what);
+#define HP_CUDA(call)                                                \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return hp_cuda_fail(e_, #call);       \
+    } while (0)
+#define HP_TRY(call)                                                 \
+    do {                                                             \
+        hp_status s_ = (call);                                       \
+        if (s_ != HP_OK) return s_;                                  \
+    } while (0)
+
+// ---- device-side BVH summary -------------------------------------------------
+struct hp_bvh_info {
+    int32_t num_interior;
+    int32_t num_leaf;
+    uint32_t box_ord[6];    // scene box as order-preserving uints (min xyz, max xyz)
+    float scale[3];         // Morton scale actually used
+    int32_t pad;
+};
+
+struct hp_bvh_impl {
+    hp_node_bin* nodes = nullptr;
+    float4* woop = nullptr;
+    int32_t* tri_idx = nullptr;
+    int32_t* counters = nullptr;   // refit termination counters [capacity]
+    hp_bvh_info* info = nullptr;   // device
+    int64_t capacity = 0;          // references
+};
+
+// ---- context: scratch arena, error words, phase events ------------------------
+struct hp_prof_mark {
+    cudaEvent_t ev;
+    char name[32];
+};
+
+struct hp_ctx {
+    int device = 0;
+    int sm_count = 148;
+    size_t l2_bytes = 0;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    int* d_status = nullptr;       // [64] device error words and counters
+    int* h_status = nullptr;       // pinned mirror
+    bool profiling = false;
+    hp_prof_mark* marks = nullptr; // event pool
+    int num_marks = 0;
+    int cap_marks = 0;
+};
+
+// Record a phase boundary on the stream when profiling is enabled.
+void hp_mark(hp_ctx* ctx, cudaStream_t s, const char* name);
+// Count kernel launches made by the library on this thread.
+void hp_count_launch(int k = 1);
+
+hp_status hp_ctx_reserve(hp_ctx* ctx, size_t bytes, cudaStream_t stream);
+
+// Bump allocator over the context arena (256-byte aligned pieces).
+struct hp_carve {
+    char* base;
+    size_t off = 0;
+    explicit hp_carve(char* b) : base(b) {}
+    template <typename T> T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += bytes;
+        return p;
+    }
+    static size_t pad(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+};
+
+// ---- radix sort ------------------------------------------------------------
+struct hp_sort_plan {
+    int64_t n = 0;
+    int key_bytes = 4;
+    int bits = 32;
+    int passes = 0;
+    int tile = 0;
+    int64_t tiles = 0;
+    size_t scratch_bytes = 0;      // keys/vals ping-pong + histograms + status
+};
+hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits);
+// Histograms [passes][256] (uint32) must be zero before the first key is
+// counted; hp_sort_run zeroes them itself unless hist_ready is set, in which
+// case the caller has already filled them (the Morton kernel does).
+struct hp_sort_args {
+    const void* keys_in;
+    const int32_t* vals_in;        // nullptr: values are 0..n-1
+    void* keys_out;
+    int32_t* vals_out;
+    void* scratch;                 // plan.scratch_bytes
+    uint32_t* hist;                // [passes*256]; inside or outside scratch
+    bool hist_ready;
+    int* status;                   // device error word
+    hp_ctx* ctx;                   // for phase marks (may be null)
+};
+hp_status hp_sort_run(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream_t stream);
+size_t hp_sort_hist_bytes(int passes);
+
+// ---- single-pass scans --------------------------------------------------------
+// Exclusive prefix sums of two int arrays at once (a: na items, b: nb items),
+// written to a_out / b_out; totals written to totals[0], totals[1].
+size_t hp_scan2_scratch_bytes(int64_t n);
+void hp_scan2_sum(const int32_t* a, int64_t na, const int32_t* b, int64_t nb,
+                  int32_t* a_out, int32_t* b_out, int32_t* totals, void* scratch,
+                  int* status, cudaStream_t stream);
+// Exclusive max-scan of in[0..n) with identity -1 into out.
+void hp_scan_max_excl(const int32_t* in, int64_t n, int32_t* out, void* scratch,
+                      int* status, cudaStream_t stream);
+
+// ---- LBVH / collapse --------------------------------------------------------------
+size_t hp_lbvh_scratch_bytes(int64_t n, int key_bytes, int bits);
+hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
+                        hp_bvh_impl* out, const hp_build_taps* taps, cudaStream_t stream);
+hp_status hp_ploc_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
+                        hp_bvh_impl* out, const hp_build_taps* taps, cudaStream_t stream);
+hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
+                          cudaStream_t stream);
+
+// ---- trace / adjoint ---------------------------------------------------------------
+hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                          int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
+                          cudaStream_t stream);
+hp_status hp_adjoint_launch(hp_ctx* ctx, const hp_mesh* m, const float* rays,
+                            const int32_t* results, const float* dl_dtuv, int64_t num_rays,
+                            float* dl_dvertices, cudaStream_t stream);
+
+inline int hp_div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }

@@ -1,0 +1,526 @@
+// LBVH construction: triangle boxes and scene box, Morton keys, radix sort,
+// Karras hierarchy emission, one bottom-up climb that refits boxes, counts
+// subtree sizes, evaluates the SAH collapse rule and woopifies triangles, and
+// a collapse into the reference's 64-byte binary node layout.
+//
+// Reference path (src/hippie/): LBVHBuilder::build rt/bvh/LBVHBuilder.cpp:183-241
+//   setupBoxes            rt/bvh/LBVHBuilderKernels.cu:65-98
+//   computeMortonCodes60  rt/bvh/LBVHBuilderKernels.cu:131-160
+//   RadixSort::sort       radix_sort/RadixSort.cpp:181-238
+//   setupLeaves           rt/bvh/LBVHBuilderKernels.cu:162-195
+//   construct60           rt/bvh/LBVHBuilderKernels.cu:11-63,226-252
+//   refit                 rt/bvh/LBVHBuilderKernels.cu:254-305
+//   BVHCollapser::collapseAdaptive rt/bvh/BVHCollapser.cpp:521-597 and its kernels
+//                         rt/bvh/BVHCollapserKernels.cu:11-526
+//   woopifyTriangles      rt/bvh/HipBVHKernels.cu:12-65
+//
+// Collapse numbering. The reference numbers the collapsed tree breadth-first
+// with global atomics, so its node order depends on scheduling. Here every
+// node of an LBVH covers a contiguous range [lo, hi] of sorted references, so
+// the collapse is decided and numbered without any top-down pass:
+//   * a node is removed iff a state-0 ("better as a leaf") node strictly
+//     contains its range; state-0 ranges are scattered as maxHi[lo] = hi and
+//     an exclusive max-scan over positions answers that query for any range;
+//   * surviving interior nodes are numbered in order of their split position
+//     (in-order), with the root moved to index 0; leaves are numbered by the
+//     first sorted reference they hold;
+//   * each collapsed leaf holds a contiguous range of sorted references, so
+//     the sorted triangle order is already leaf-contiguous and no reordering
+//     pass is needed.
+// The tree this produces is the reference's tree up to node numbering and the
+// order of triangles inside a leaf (which the reference leaves to atomics).
+#include <algorithm>
+#include <cuda_runtime.h>
+#include "hp_device.cuh"
+#include "hp_internal.h"
+
+namespace {
+
+constexpr int TB = 256;
+
+__device__ __forceinline__ void load_vertex(const float* __restrict__ v, int64_t nv, int idx,
+                                            float& x, float& y, float& z, int* err) {
+    if (idx < 0 || idx >= nv) {
+        hp_report(err, HP_DEV_BAD_INPUT, idx);
+        idx = 0;
+    }
+    x = __ldg(v + 3 * (int64_t)idx + 0);
+    y = __ldg(v + 3 * (int64_t)idx + 1);
+    z = __ldg(v + 3 * (int64_t)idx + 2);
+}
+
+struct tri_verts {
+    float x0, y0, z0, x1, y1, z1, x2, y2, z2;
+};
+
+__device__ __forceinline__ tri_verts load_tri(const float* __restrict__ v, int64_t nv,
+                                              const int32_t* __restrict__ t, int64_t tri, int* err) {
+    tri_verts r;
+    int a = __ldg(t + 3 * tri + 0), b = __ldg(t + 3 * tri + 1), c = __ldg(t + 3 * tri + 2);
+    load_vertex(v, nv, a, r.x0, r.y0, r.z0, err);
+    load_vertex(v, nv, b, r.x1, r.y1, r.z1, err);
+    load_vertex(v, nv, c, r.x2, r.y2, r.z2, err);
+    return r;
+}
+
+// Per-triangle boxes (setupBoxes) and the scene box as their union
+// (SceneLoader.cpp:144-153 computes it over triangle boxes at load time).
+__global__ void __launch_bounds__(TB) k_tri_boxes(const float* __restrict__ verts, int64_t nv,
+                                                  const int32_t* __restrict__ tris, int64_t n,
+                                                  float4* __restrict__ bmin, float4* __restrict__ bmax,
+                                                  uint32_t* box_ord, int* err) {
+    float mn[3] = {HP_MAX_FLOAT, HP_MAX_FLOAT, HP_MAX_FLOAT};
+    float mx[3] = {-HP_MAX_FLOAT, -HP_MAX_FLOAT, -HP_MAX_FLOAT};
+    for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TB) {
+        tri_verts t = load_tri(verts, nv, tris, i, err);
+        float ax = fminf(fminf(t.x0, t.x1), t.x2), ay = fminf(fminf(t.y0, t.y1), t.y2),
+              az = fminf(fminf(t.z0, t.z1), t.z2);
+        float bx = fmaxf(fmaxf(t.x0, t.x1), t.x2), by = fmaxf(fmaxf(t.y0, t.y1), t.y2),
+              bz = fmaxf(fmaxf(t.z0, t.z1), t.z2);
+        bmin[i] = make_float4(ax, ay, az, 0.0f);
+        bmax[i] = make_float4(bx, by, bz, 0.0f);
+        mn[0] = fminf(mn[0], ax); mn[1] = fminf(mn[1], ay); mn[2] = fminf(mn[2], az);
+        mx[0] = fmaxf(mx[0], bx); mx[1] = fmaxf(mx[1], by); mx[2] = fmaxf(mx[2], bz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(HP_FULL_MASK, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(HP_FULL_MASK, mx[k], o));
+        }
+    }
+    __shared__ float s[TB / 32][6];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 3; ++k) { s[warp][k] = mn[k]; s[warp][3 + k] = mx[k]; }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        int k = threadIdx.x;
+        float r = s[0][k];
+        for (int w = 1; w < TB / 32; ++w) r = (k < 3) ? fminf(r, s[w][k]) : fmaxf(r, s[w][k]);
+        if (k < 3) atomicMin(&box_ord[k], hp_f2ord(r));
+        else atomicMax(&box_ord[k], hp_f2ord(r));
+    }
+}
+
+__global__ void k_init_build(hp_bvh_info* info, uint32_t* hist, int hist_words) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < hist_words) hist[i] = 0;
+    if (i < 6) info->box_ord[i] = (i < 3) ? 0xffffffffu : 0u;
+    if (i == 0) { info->num_interior = 0; info->num_leaf = 0; }
+}
+
+// Morton keys (computeMortonCodes60) fused with the radix sort's per-pass digit
+// histograms. scale = 1/diagonal is taken with __fdividef, the approximate
+// quotient the reference's fast-math JIT build produces for `1.0f / diag`.
+template <typename K>
+__global__ void __launch_bounds__(TB) k_morton(const float4* __restrict__ bmin,
+                                               const float4* __restrict__ bmax, int64_t n,
+                                               hp_bvh_info* info, int bits, int passes,
+                                               K* __restrict__ keys, uint32_t* hist) {
+    __shared__ uint32_t sh[8 * 256];
+    for (int i = threadIdx.x; i < passes * 256; i += TB) sh[i] = 0;
+    float smin[3], scale[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        smin[k] = hp_ord2f(info->box_ord[k]);
+        float d = __fsub_rn(hp_ord2f(info->box_ord[3 + k]), smin[k]);
+        scale[k] = __fdividef(1.0f, d);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 3) info->scale[threadIdx.x] = scale[threadIdx.x];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TB) {
+        float4 a = bmin[i], b = bmax[i];
+        uint64_t key = hp_morton_key(a.x, a.y, a.z, b.x, b.y, b.z, smin, scale, bits);
+        keys[i] = (K)key;
+        for (int p = 0; p < passes; ++p) {
+            int w = min(8, bits - 8 * p);
+            atomicAdd(&sh[p * 256 + (uint32_t)((key >> (8 * p)) & ((1u << w) - 1u))], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += TB)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// delta (rt/bvh/HipBVHUtil.h:17-33): common prefix length of keys i and j, with
+// the index prefix appended for equal keys; -1 outside [0, n).
+template <typename K> __device__ __forceinline__ int kdelta(const K* k, int n, int i, int j);
+template <> __device__ __forceinline__ int kdelta<uint64_t>(const uint64_t* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = __ldg(k + i), b = __ldg(k + j);
+    if (a != b) return __clzll((long long)(a ^ b));
+    return __clzll((long long)(i ^ j)) + 64;
+}
+template <> __device__ __forceinline__ int kdelta<uint32_t>(const uint32_t* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = __ldg(k + i), b = __ldg(k + j);
+    if (a != b) return __clz((int)(a ^ b));
+    return __clz(i ^ j) + 32;
+}
+
+// Karras 2012 radix-tree emission (construct<T>, LBVHBuilderKernels.cu:11-63).
+// Interior node i covers [min(i,j), max(i,j)] and splits after gamma; a child
+// is a leaf (index + n-1) when its range has one reference.
+template <typename K>
+__global__ void __launch_bounds__(TB) k_karras(const K* __restrict__ keys, int n, int* parent,
+                                               int* left, int* right, int2* range) {
+    const int i = blockIdx.x * TB + threadIdx.x;
+    if (i == 0) parent[0] = -1;
+    if (i >= n - 1) return;
+    const int dr = kdelta(keys, n, i, i + 1), dl = kdelta(keys, n, i, i - 1);
+    const int d = (dr - dl > 0) - (dr - dl < 0);
+    const int dmin = kdelta(keys, n, i, i - d);
+    int lmax = 2;
+    while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = kdelta(keys, n, i, j);
+    int s = 0, k = 2, t;
+    do {
+        t = (l + k - 1) / k;
+        k <<= 1;
+        if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    int lc = gamma, rc = gamma + 1;
+    if (min(i, j) == gamma) lc += n - 1;
+    if (max(i, j) == gamma + 1) rc += n - 1;
+    left[i] = lc;
+    right[i] = rc;
+    parent[lc] = i;
+    parent[rc] = i;
+    range[i] = make_int2(min(i, j), max(i, j));
+}
+
+// One thread per sorted reference p (leaf node n-1+p): woopify its triangle,
+// store the leaf box, then climb. The second thread to reach a node merges
+// the children's boxes, sums sizes and evaluates the collapse rule of
+// computeNodeStatesAdaptive (BVHCollapserKernels.cu:58-136):
+//   leaf cost = ci*A, interior cost = ct*A + c(left) + c(right),
+//   state 0 (collapse into a leaf) iff ci*A*size < interior cost;
+// or, without adaptive leaves, computeNodeStates (:138-184): size <= maxLeafSize.
+// Node boxes keep the cost in min.w and the size (as int bits) in max.w.
+__global__ void __launch_bounds__(TB) k_climb(
+    int n, const int32_t* __restrict__ sorted_tri, const float* __restrict__ verts, int64_t nv,
+    const int32_t* __restrict__ tris, const int* __restrict__ parent, const int* __restrict__ left,
+    const int* __restrict__ right, const int2* __restrict__ range, float4* nbmin, float4* nbmax,
+    float4* __restrict__ woop, int* counters, int* max_hi, uint8_t* state, float ct, float ci,
+    int adaptive, int max_leaf, int* err) {
+    const int p = blockIdx.x * TB + threadIdx.x;
+    if (p >= n) return;
+    const int tri = sorted_tri[p];
+    tri_verts t = load_tri(verts, nv, tris, tri, err);
+    float4 w0, w1, w2;
+    hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
+    woop[3 * (int64_t)p + 0] = w0;
+    woop[3 * (int64_t)p + 1] = w1;
+    woop[3 * (int64_t)p + 2] = w2;
+    float ax = fminf(fminf(t.x0, t.x1), t.x2), ay = fminf(fminf(t.y0, t.y1), t.y2),
+          az = fminf(fminf(t.z0, t.z1), t.z2);
+    float bx = fmaxf(fmaxf(t.x0, t.x1), t.x2), by = fmaxf(fmaxf(t.y0, t.y1), t.y2),
+          bz = fmaxf(fmaxf(t.z0, t.z1), t.z2);
+    float cost = adaptive ? __fmul_rn(ci, hp_area(ax, ay, az, bx, by, bz)) : 0.0f;
+    const int leaf = n - 1 + p;
+    nbmin[leaf] = make_float4(ax, ay, az, cost);
+    nbmax[leaf] = make_float4(bx, by, bz, __int_as_float(1));
+    int node = parent[leaf];
+    int guard = 0;
+    while (node >= 0) {
+        if (node >= n - 1 || ++guard > n) {  // a valid tree reaches the root within n steps
+            hp_report(err, HP_DEV_BAD_INDEX, node);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(&counters[node], 1) == 0) return;
+        __threadfence();
+        const int l = left[node], r = right[node];
+        if ((unsigned)l >= (unsigned)(2 * n - 1) || (unsigned)r >= (unsigned)(2 * n - 1)) {
+            hp_report(err, HP_DEV_BAD_INDEX, node);
+            return;
+        }
+        const float4 lmn = __ldcg(nbmin + l), lmx = __ldcg(nbmax + l);
+        const float4 rmn = __ldcg(nbmin + r), rmx = __ldcg(nbmax + r);
+        const float mnx = fminf(lmn.x, rmn.x), mny = fminf(lmn.y, rmn.y), mnz = fminf(lmn.z, rmn.z);
+        const float mxx = fmaxf(lmx.x, rmx.x), mxy = fmaxf(lmx.y, rmx.y), mxz = fmaxf(lmx.z, rmx.z);
+        const int size = __float_as_int(lmx.w) + __float_as_int(rmx.w);
+        int st;
+        float c;
+        if (adaptive) {
+            const float area = hp_area(mnx, mny, mnz, mxx, mxy, mxz);
+            const float c_int = __fadd_rn(__fmaf_rn(ct, area, lmn.w), rmn.w);
+            const float c_leaf = __fmul_rn(__fmul_rn(ci, area), (float)size);
+            st = (c_leaf < c_int) ? 0 : 1;
+            c = st ? c_int : c_leaf;
+        } else {
+            st = (size <= max_leaf) ? 0 : 1;
+            c = 0.0f;
+        }
+        __stcg(nbmin + node, make_float4(mnx, mny, mnz, c));
+        __stcg(nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
+        state[node] = (uint8_t)st;
+        if (st == 0 && node != 0) {
+            const int2 rg = range[node];
+            atomicMax(&max_hi[rg.x], rg.y);
+        }
+        node = parent[node];
+    }
+}
+
+__device__ __forceinline__ int split_of(const int* left, int n, int i) {
+    int l = left[i];
+    return l >= n - 1 ? l - (n - 1) : l;
+}
+
+// Collapse flags: interior split gamma survives as an interior node; sorted
+// position p starts a leaf of the collapsed tree.
+__global__ void __launch_bounds__(TB) k_collapse_flags(int n, const int* __restrict__ left,
+                                                       const int2* __restrict__ range,
+                                                       const uint8_t* __restrict__ state,
+                                                       const int* __restrict__ max_hi,
+                                                       const int* __restrict__ reach,
+                                                       int* flag_int, int* flag_leaf) {
+    const int t = blockIdx.x * TB + threadIdx.x;
+    if (t < n - 1) {
+        const int2 rg = range[t];
+        const bool alive = (t == 0) || !(reach[rg.x] >= rg.y || max_hi[rg.x] > rg.y);
+        flag_int[split_of(left, n, t)] = (alive && (t == 0 || state[t] == 1)) ? 1 : 0;
+    } else if (t < 2 * n - 1) {
+        const int p = t - (n - 1);
+        flag_leaf[p] = (reach[p] < p) ? 1 : 0;
+    }
+}
+
+struct emit_ctx {
+    int n;
+    const int* left;
+    const int* right;
+    const int* parent;
+    const int2* range;
+    const uint8_t* state;
+    const int* rank_int;
+    const int* rank_leaf;
+    const float4* nbmin;
+    const float4* nbmax;
+    int root_rank;
+    int num_int;
+};
+
+__device__ __forceinline__ int new_interior(const emit_ctx& e, int i) {
+    if (i == 0) return 0;
+    int r = e.rank_int[split_of(e.left, e.n, i)];
+    return r < e.root_rank ? r + 1 : r;
+}
+
+// Encoded child reference of a surviving interior node: interior index, or
+// ~(leaf node index) for a leaf child.
+__device__ __forceinline__ int child_ref(const emit_ctx& e, int c) {
+    if (c >= e.n - 1) return ~(e.num_int + e.rank_leaf[c - (e.n - 1)]);
+    if (e.state[c] == 0) return ~(e.num_int + e.rank_leaf[e.range[c].x]);
+    return new_interior(e, c);
+}
+
+__device__ __forceinline__ void put_node(hp_node_bin* nodes, int idx, int max_nodes,
+                                         const hp_node_bin& nd, int* err) {
+    if ((unsigned)idx < (unsigned)max_nodes) nodes[idx] = nd;
+    else hp_report(err, HP_DEV_BAD_INDEX, idx);
+}
+
+__global__ void __launch_bounds__(TB) k_emit(emit_ctx e, const int* __restrict__ max_hi,
+                                             const int* __restrict__ reach, hp_bvh_info* info,
+                                             hp_node_bin* __restrict__ nodes, int max_nodes, int* err) {
+    const int t = blockIdx.x * TB + threadIdx.x;
+    const int n = e.n;
+    if (t >= 2 * n - 1) return;
+    e.root_rank = e.rank_int[split_of(e.left, n, 0)];
+    e.num_int = info->num_interior;
+    if (t < n - 1) {
+        const int2 rg = e.range[t];
+        const bool alive = (t == 0) || !(reach[rg.x] >= rg.y || max_hi[rg.x] > rg.y);
+        if (!alive) return;
+        const int par = (t == 0) ? -1 : new_interior(e, e.parent[t]);
+        const float4 mn = e.nbmin[t], mx = e.nbmax[t];
+        const int size = __float_as_int(mx.w);
+        if (t == 0 || e.state[t] == 1) {
+            const int l = e.left[t], r = e.right[t];
+            put_node(nodes, new_interior(e, t), max_nodes,
+                     hp_make_node(e.nbmin[l], e.nbmax[l], e.nbmin[r], e.nbmax[r], child_ref(e, l),
+                                  child_ref(e, r), size, par), err);
+        } else {
+            put_node(nodes, e.num_int + e.rank_leaf[rg.x], max_nodes,
+                     hp_make_node(mn, mx, mn, mx, rg.x, rg.y + 1, ~size, par), err);
+        }
+    } else {
+        const int p = t - (n - 1);
+        if (!(reach[p] < p && max_hi[p] < p)) return;
+        const float4 mn = e.nbmin[t], mx = e.nbmax[t];
+        const int par = new_interior(e, e.parent[t]);
+        put_node(nodes, e.num_int + e.rank_leaf[p], max_nodes,
+                 hp_make_node(mn, mx, mn, mx, p, p + 1, ~1, par), err);
+    }
+}
+
+// A single triangle: root interior node whose second child is an empty leaf.
+__global__ void k_single(const float* verts, int64_t nv, const int32_t* tris, hp_node_bin* nodes,
+                         float4* woop, int32_t* tri_idx, hp_bvh_info* info, int* err) {
+    if (threadIdx.x != 0) return;
+    tri_verts t = load_tri(verts, nv, tris, 0, err);
+    float4 w0, w1, w2;
+    hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
+    woop[0] = w0; woop[1] = w1; woop[2] = w2;
+    tri_idx[0] = 0;
+    float4 mn = make_float4(fminf(fminf(t.x0, t.x1), t.x2), fminf(fminf(t.y0, t.y1), t.y2),
+                            fminf(fminf(t.z0, t.z1), t.z2), 0.0f);
+    float4 mx = make_float4(fmaxf(fmaxf(t.x0, t.x1), t.x2), fmaxf(fmaxf(t.y0, t.y1), t.y2),
+                            fmaxf(fmaxf(t.z0, t.z1), t.z2), 0.0f);
+    float4 emn = make_float4(HP_MAX_FLOAT, HP_MAX_FLOAT, HP_MAX_FLOAT, 0.0f);
+    float4 emx = make_float4(-HP_MAX_FLOAT, -HP_MAX_FLOAT, -HP_MAX_FLOAT, 0.0f);
+    nodes[0] = hp_make_node(mn, mx, emn, emx, ~1, ~2, 1, -1);
+    nodes[1] = hp_make_node(mn, mx, mn, mx, 0, 1, ~1, 0);
+    nodes[2] = hp_make_node(emn, emx, emn, emx, 1, 1, ~0, 0);
+    for (int k = 0; k < 3; ++k) {
+        info->box_ord[k] = hp_f2ord((&mn.x)[k]);
+        info->box_ord[3 + k] = hp_f2ord((&mx.x)[k]);
+    }
+    info->num_interior = 1;
+    info->num_leaf = 2;
+}
+
+// ---- taps (intermediate results for parity tests) ----------------------------------
+template <typename K>
+__global__ void k_tap_keys(const K* in, uint64_t* out, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (uint64_t)in[i];
+}
+__global__ void k_tap_tree(int n, const int* parent, const int* left, const int* right,
+                           const float4* nbmin, const float4* nbmax, int* tp, int* tl, int* tr,
+                           float4* tmn, float4* tmx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * n - 1) return;
+    if (tp) tp[i] = parent[i];
+    if (tl) tl[i] = (i < n - 1) ? left[i] : i - (n - 1);
+    if (tr) tr[i] = (i < n - 1) ? right[i] : i - (n - 1) + 1;
+    float4 a = nbmin[i], b = nbmax[i];
+    if (tmn) tmn[i] = make_float4(a.x, a.y, a.z, 0.0f);
+    if (tmx) tmx[i] = make_float4(b.x, b.y, b.z, 0.0f);
+}
+__global__ void k_tap_box(const hp_bvh_info* info, float* out) {
+    int k = threadIdx.x;
+    if (k < 6) out[k] = hp_ord2f(info->box_ord[k]);
+}
+
+template <typename K>
+hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
+                 const hp_build_taps* taps, cudaStream_t s) {
+    const int64_t n = m->num_triangles;
+    const int bits = p->morton_bits;
+    const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits);
+    const int64_t nn = 2 * n - 1;
+    size_t need = 0;
+    need += 2 * hp_carve::pad(n * 16);                  // triangle boxes
+    need += 2 * hp_carve::pad(n * sizeof(K));           // keys, sorted keys
+    need += hp_carve::pad(plan.scratch_bytes);
+    need += hp_carve::pad(hp_sort_hist_bytes(plan.passes));
+    need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
+    need += 2 * hp_carve::pad(nn * 16);                 // node boxes
+    need += hp_carve::pad(n * 4) * 7 + hp_carve::pad(n);  // counters, maxhi, reach, flags, ranks, state
+    need += 2 * hp_scan2_scratch_bytes(n + 1);
+    HP_TRY(hp_ctx_reserve(ctx, need, s));
+    hp_carve cv(ctx->arena);
+    float4* tbmin = cv.take<float4>(n);
+    float4* tbmax = cv.take<float4>(n);
+    K* keys = cv.take<K>(n);
+    K* skeys = cv.take<K>(n);
+    void* sort_scratch = cv.take<char>(plan.scratch_bytes);
+    uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    int* parent = cv.take<int>(nn);
+    int* left = cv.take<int>(n);
+    int* right = cv.take<int>(n);
+    int2* range = cv.take<int2>(n);
+    float4* nbmin = cv.take<float4>(nn);
+    float4* nbmax = cv.take<float4>(nn);
+    int* counters = cv.take<int>(n);
+    int* max_hi = cv.take<int>(n);
+    int* reach = cv.take<int>(n);
+    int* flag_int = cv.take<int>(n);
+    int* flag_leaf = cv.take<int>(n);
+    int* rank_int = cv.take<int>(n);
+    int* rank_leaf = cv.take<int>(n);
+    uint8_t* state = cv.take<uint8_t>(n);
+    void* scan_a = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
+    void* scan_b = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
+    int* err = ctx->d_status;
+    hp_bvh_info* info = out->info;
+    const int grid_n = hp_div_up(n, TB);
+    const int grid_red = (int)std::min<int64_t>(grid_n, (int64_t)ctx->sm_count * 8);
+
+    k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
+    HP_CUDA(cudaMemsetAsync(counters, 0, n * 4, s));
+    HP_CUDA(cudaMemsetAsync(max_hi, 0xff, n * 4, s));
+    k_tri_boxes<<<grid_red, TB, 0, s>>>(m->vertices, m->num_vertices, m->triangles, n, tbmin, tbmax,
+                                        info->box_ord, err);
+    hp_count_launch(2);
+    hp_mark(ctx, s, "boxes");
+    k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_mark(ctx, s, "morton");
+    hp_sort_args sa{keys, nullptr, skeys, out->tri_idx, sort_scratch, hist, true, err, ctx};
+    HP_TRY(hp_sort_run(plan, sa, s));
+    k_karras<K><<<grid_n, TB, 0, s>>>(skeys, (int)n, parent, left, right, range);
+    hp_count_launch();
+    hp_mark(ctx, s, "karras");
+    k_climb<<<grid_n, TB, 0, s>>>((int)n, out->tri_idx, m->vertices, m->num_vertices, m->triangles,
+                                  parent, left, right, range, nbmin, nbmax, out->woop, counters,
+                                  max_hi, state, p->ct, p->ci, p->adaptive_leaf, p->max_leaf_size, err);
+    hp_count_launch();
+    hp_mark(ctx, s, "climb");
+    hp_scan_max_excl(max_hi, n, reach, scan_a, err, s);
+    k_collapse_flags<<<hp_div_up(nn, TB), TB, 0, s>>>((int)n, left, range, state, max_hi, reach,
+                                                     flag_int, flag_leaf);
+    hp_scan2_sum(flag_int, n - 1, flag_leaf, n, rank_int, rank_leaf, &info->num_interior, scan_b, err, s);
+    emit_ctx e{(int)n, left, right, parent, range, state, rank_int, rank_leaf, nbmin, nbmax, 0, 0};
+    k_emit<<<hp_div_up(nn, TB), TB, 0, s>>>(e, max_hi, reach, info, out->nodes,
+                                            (int)std::max<int64_t>(2 * out->capacity - 1, 3), err);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch(2);
+    hp_mark(ctx, s, "collapse");
+
+    if (taps) {
+        if (taps->morton_keys)
+            k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
+        if (taps->sorted_keys)
+            k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
+        if (taps->sorted_refs)
+            HP_CUDA(cudaMemcpyAsync(taps->sorted_refs, out->tri_idx, n * 4, cudaMemcpyDeviceToDevice, s));
+        if (taps->node_parent || taps->node_left || taps->node_right || taps->node_box_min ||
+            taps->node_box_max)
+            k_tap_tree<<<hp_div_up(nn, TB), TB, 0, s>>>((int)n, parent, left, right, nbmin, nbmax,
+                                                       taps->node_parent, taps->node_left,
+                                                       taps->node_right, (float4*)taps->node_box_min,
+                                                       (float4*)taps->node_box_max);
+        if (taps->scene_box) k_tap_box<<<1, 32, 0, s>>>(info, taps->scene_box);
+        HP_CUDA(cudaGetLastError());
+    }
+    return HP_OK;
+}
+
+}  // namespace
+
+hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
+                        const hp_build_taps* taps, cudaStream_t s) {
+    const int64_t n = m->num_triangles;
+    if (n == 1) {
+        k_single<<<1, 32, 0, s>>>(m->vertices, m->num_vertices, m->triangles, out->nodes, out->woop,
+                                  out->tri_idx, out->info, ctx->d_status);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        hp_mark(ctx, s, "single");
+        return HP_OK;
+    }
+    if (p->morton_bits <= 32) return lbvh_t<uint32_t>(ctx, m, p, out, taps, s);
+    return lbvh_t<uint64_t>(ctx, m, p, out, taps, s);
+}

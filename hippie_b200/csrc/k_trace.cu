@@ -1,0 +1,257 @@
+// Persistent-warp closest-hit / any-hit traversal of the 64-byte binary BVH.
+//
+// Reference: HipTracer::trace (rt/tracer/HipTracer.cpp:13-52) and the Aila-Laine
+// while-while kernel `trace` / `traceStats` (rt/tracer/HipTracerBinKernels.cu:19-286,
+// 290-568): persistent warps that take rays from a global counter, near child
+// first, a per-ray stack with a sentinel bottom entry, slab tests against both
+// children of a node, Woop triangle tests, and a refill of finished lanes when
+// fewer than 20 lanes of a warp still traverse.
+//
+// Differences by design:
+//   * the traversal stack is split: its first 16 entries live in shared memory
+//     (bank-conflict-free, one column per thread), deeper entries in local memory;
+//   * every lane handles its leaves as soon as it reaches them (no speculative
+//     postponing), so the sequence of node and triangle tests of a ray does not
+//     depend on the other lanes of its warp; with the explicit fma / IEEE
+//     reciprocal arithmetic below a CPU restatement reproduces every result bit;
+//   * closest-hit ties in t are resolved to the lower triangle id.
+#include <cuda_runtime.h>
+#include "hp_device.cuh"
+#include "hp_internal.h"
+
+namespace {
+
+constexpr int TRACE_BLOCK = 128;
+constexpr int SSTACK = 16;        // shared-memory stack entries per thread
+constexpr int LSTACK = 48;        // local-memory overflow entries per thread
+constexpr int SENTINEL = 0x76543210;
+constexpr int FETCH_THRESHOLD = 20;
+constexpr int TRAVERSAL_LIMIT = 1 << 22;  // visits per ray before the ray is abandoned with an error
+
+struct ray_state {
+    float ox, oy, oz, tmin, dx, dy, dz;
+    float idx_, idy, idz, oodx, oody, oodz;
+    float hit_t, hit_u, hit_v;
+    int hit;       // woop / leaf-ordered reference index of the closest hit, -1 if none
+    int nodes, tris;
+};
+
+__device__ __forceinline__ float safe_rcp(float d) {
+    // idir = 1 / (|d| > 2^-80 ? d : copysign(2^-80, d)) (HipTracerBinKernels.cu:83-86)
+    const float ooeps = 8.2718061255302767e-25f;  // 2^-80
+    return __frcp_rn(fabsf(d) > ooeps ? d : copysignf(ooeps, d));
+}
+
+template <bool ANY_HIT, bool STATS>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
+    const float4* __restrict__ rays, int64_t num_rays, int4* __restrict__ results,
+    int2* __restrict__ stats, const float4* __restrict__ nodes, const float4* __restrict__ woop,
+    const int32_t* __restrict__ tri_idx, int max_nodes, int num_refs,
+    unsigned long long* ray_counter, int* err) {
+    __shared__ int s_stack[SSTACK * TRACE_BLOCK];
+    int* sstack = s_stack + threadIdx.x;
+    int lstack[LSTACK];
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    ray_state r;
+    int64_t ray = -1;
+    int node = SENTINEL;
+    int sp = 0;
+    int steps = 0;  // node + leaf visits of the current ray (bounded)
+    bool exhausted = false;
+
+    while (true) {
+        // Refill lanes whose ray is finished (one atomic per warp).
+        const bool need = (node == SENTINEL) && !exhausted;
+        const unsigned need_mask = __ballot_sync(HP_FULL_MASK, need);
+        if (need_mask) {
+            const int leader = __ffs(need_mask) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(ray_counter, (unsigned long long)__popc(need_mask));
+            base = __shfl_sync(HP_FULL_MASK, base, leader);
+            if (need) {
+                const int64_t id = (int64_t)base + __popc(need_mask & lt_mask);
+                if (id < num_rays) {
+                    ray = id;
+                    const float4 o = __ldg(rays + 2 * id), d = __ldg(rays + 2 * id + 1);
+                    r.ox = o.x; r.oy = o.y; r.oz = o.z; r.tmin = o.w;
+                    r.dx = d.x; r.dy = d.y; r.dz = d.z; r.hit_t = d.w;
+                    r.idx_ = safe_rcp(d.x); r.idy = safe_rcp(d.y); r.idz = safe_rcp(d.z);
+                    r.oodx = __fmul_rn(o.x, r.idx_);
+                    r.oody = __fmul_rn(o.y, r.idy);
+                    r.oodz = __fmul_rn(o.z, r.idz);
+                    r.hit = -1;
+                    r.hit_u = r.hit_v = 0.0f;
+                    r.nodes = r.tris = 0;
+                    sp = 0;
+                    steps = 0;
+                    node = 0;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (__all_sync(HP_FULL_MASK, node == SENTINEL)) break;
+
+        while (node != SENTINEL) {
+            // Interior nodes until this lane reaches a leaf or finishes.
+            while ((unsigned)node < (unsigned)SENTINEL) {
+                if (node >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
+                    hp_report(err, HP_DEV_BAD_INDEX, node);
+                    node = SENTINEL;
+                    break;
+                }
+                if (STATS) ++r.nodes;
+                const float4* np = nodes + 4 * (int64_t)node;
+                const float4 n0 = __ldg(np), n1 = __ldg(np + 1), nz = __ldg(np + 2);
+                const float4 nm = __ldg(np + 3);
+                const float c0lox = __fmaf_rn(n0.x, r.idx_, -r.oodx);
+                const float c0hix = __fmaf_rn(n0.y, r.idx_, -r.oodx);
+                const float c0loy = __fmaf_rn(n0.z, r.idy, -r.oody);
+                const float c0hiy = __fmaf_rn(n0.w, r.idy, -r.oody);
+                const float c0loz = __fmaf_rn(nz.x, r.idz, -r.oodz);
+                const float c0hiz = __fmaf_rn(nz.y, r.idz, -r.oodz);
+                const float c1loz = __fmaf_rn(nz.z, r.idz, -r.oodz);
+                const float c1hiz = __fmaf_rn(nz.w, r.idz, -r.oodz);
+                const float c1lox = __fmaf_rn(n1.x, r.idx_, -r.oodx);
+                const float c1hix = __fmaf_rn(n1.y, r.idx_, -r.oodx);
+                const float c1loy = __fmaf_rn(n1.z, r.idy, -r.oody);
+                const float c1hiy = __fmaf_rn(n1.w, r.idy, -r.oody);
+                const float c0min = fmaxf(fmaxf(fminf(c0lox, c0hix), fminf(c0loy, c0hiy)),
+                                          fmaxf(fminf(c0loz, c0hiz), r.tmin));
+                const float c0max = fminf(fminf(fmaxf(c0lox, c0hix), fmaxf(c0loy, c0hiy)),
+                                          fminf(fmaxf(c0loz, c0hiz), r.hit_t));
+                const float c1min = fmaxf(fmaxf(fminf(c1lox, c1hix), fminf(c1loy, c1hiy)),
+                                          fmaxf(fminf(c1loz, c1hiz), r.tmin));
+                const float c1max = fminf(fminf(fmaxf(c1lox, c1hix), fmaxf(c1loy, c1hiy)),
+                                          fminf(fmaxf(c1loz, c1hiz), r.hit_t));
+                const bool t0 = c0max >= c0min, t1 = c1max >= c1min;
+                int c0 = __float_as_int(nm.x), c1 = __float_as_int(nm.y);
+                if (!t0 && !t1) {
+                    if (sp == 0) node = SENTINEL;
+                    else { --sp; node = sp < SSTACK ? sstack[sp * TRACE_BLOCK] : lstack[sp - SSTACK]; }
+                } else {
+                    node = t0 ? c0 : c1;
+                    if (t0 && t1) {
+                        int far = c1;
+                        if (c1min < c0min) { node = c1; far = c0; }
+                        if (sp < SSTACK) sstack[sp * TRACE_BLOCK] = far;
+                        else if (sp < SSTACK + LSTACK) lstack[sp - SSTACK] = far;
+                        else { hp_report(err, HP_DEV_STACK_OVERFLOW, (int)ray); --sp; }
+                        ++sp;
+                    }
+                }
+            }
+            // Leaves: test every triangle, then continue with the stack.
+            while (node < 0) {
+                if (~node >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
+                    hp_report(err, HP_DEV_BAD_INDEX, node);
+                    node = SENTINEL;
+                    break;
+                }
+                const float4 lm = __ldg(nodes + 4 * (int64_t)(~node) + 3);
+                int begin = __float_as_int(lm.x), end = __float_as_int(lm.y);
+                if (begin < 0 || end > num_refs || begin > end) {
+                    hp_report(err, HP_DEV_BAD_INDEX, begin);
+                    begin = end = 0;
+                }
+                for (int tri = begin; tri < end; ++tri) {
+                    if (STATS) ++r.tris;
+                    const float4 v0 = __ldg(woop + 3 * (int64_t)tri);
+                    const float oz = __fmaf_rn(-r.oz, v0.z, __fmaf_rn(-r.oy, v0.y, __fmaf_rn(-r.ox, v0.x, v0.w)));
+                    const float den = __fmaf_rn(r.dz, v0.z, __fmaf_rn(r.dy, v0.y, __fmul_rn(r.dx, v0.x)));
+                    const float t = __fmul_rn(oz, __frcp_rn(den));
+                    bool closer = t < r.hit_t;
+                    if (!closer && t == r.hit_t && r.hit >= 0)
+                        closer = __ldg(tri_idx + tri) < __ldg(tri_idx + r.hit);
+                    if (t > r.tmin && closer) {
+                        const float4 v1 = __ldg(woop + 3 * (int64_t)tri + 1);
+                        const float ox = __fmaf_rn(r.oz, v1.z, __fmaf_rn(r.oy, v1.y, __fmaf_rn(r.ox, v1.x, v1.w)));
+                        const float dx = __fmaf_rn(r.dz, v1.z, __fmaf_rn(r.dy, v1.y, __fmul_rn(r.dx, v1.x)));
+                        const float u = __fmaf_rn(t, dx, ox);
+                        if (u >= 0.0f) {
+                            const float4 v2 = __ldg(woop + 3 * (int64_t)tri + 2);
+                            const float oy = __fmaf_rn(r.oz, v2.z, __fmaf_rn(r.oy, v2.y, __fmaf_rn(r.ox, v2.x, v2.w)));
+                            const float dy = __fmaf_rn(r.dz, v2.z, __fmaf_rn(r.dy, v2.y, __fmul_rn(r.dx, v2.x)));
+                            const float v = __fmaf_rn(t, dy, oy);
+                            if (v >= 0.0f && __fadd_rn(u, v) <= 1.0f) {
+                                r.hit_t = t;
+                                r.hit = tri;
+                                r.hit_u = u;
+                                r.hit_v = v;
+                                if (ANY_HIT) { sp = 0; break; }
+                            }
+                        }
+                    }
+                }
+                if (ANY_HIT && r.hit >= 0) { node = SENTINEL; break; }
+                if (sp == 0) node = SENTINEL;
+                else { --sp; node = sp < SSTACK ? sstack[sp * TRACE_BLOCK] : lstack[sp - SSTACK]; }
+            }
+            if (node == SENTINEL) {
+                if (r.hit < 0) {
+                    reinterpret_cast<int2*>(results)[2 * ray] = make_int2(-1, __float_as_int(r.hit_t));
+                    if (STATS) stats[ray] = make_int2(0, 0);
+                } else {
+                    results[ray] = make_int4(__ldg(tri_idx + r.hit), __float_as_int(r.hit_t),
+                                             __float_as_int(r.hit_u), __float_as_int(r.hit_v));
+                    if (STATS) stats[ray] = make_int2(r.nodes, r.tris);
+                }
+                break;
+            }
+            if (__popc(__activemask()) < FETCH_THRESHOLD) break;
+        }
+    }
+}
+
+// Empty BVH: every ray misses.
+__global__ void k_trace_empty(const float4* rays, int64_t num_rays, int4* results, int2* stats) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= num_rays) return;
+    reinterpret_cast<int2*>(results)[2 * i] = make_int2(-1, __float_as_int(rays[2 * i + 1].w));
+    if (stats) stats[i] = make_int2(0, 0);
+}
+
+template <bool A, bool S>
+hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                   int64_t num_rays, int32_t* results, int32_t* stats, unsigned long long* counter,
+                   cudaStream_t s) {
+    int per_sm = 0;
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S>, TRACE_BLOCK, 0));
+    int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
+    grid = std::min<int64_t>(grid, (num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
+    const int max_nodes = (int)std::max<int64_t>(2 * b->capacity - 1, 3);
+    k_trace<A, S><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
+        reinterpret_cast<const float4*>(rays), num_rays, reinterpret_cast<int4*>(results),
+        reinterpret_cast<int2*>(stats), reinterpret_cast<const float4*>(b->nodes), b->woop, b->tri_idx,
+        max_nodes, (int)n_refs, counter, ctx->d_status);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_mark(ctx, s, "trace");
+    return HP_OK;
+}
+
+}  // namespace
+
+hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                          int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
+                          cudaStream_t s) {
+    if (num_rays <= 0) return HP_OK;
+    if (n_refs <= 0) {
+        k_trace_empty<<<hp_div_up(num_rays, 256), 256, 0, s>>>(
+            reinterpret_cast<const float4*>(rays), num_rays, reinterpret_cast<int4*>(results),
+            reinterpret_cast<int2*>(stats));
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        return HP_OK;
+    }
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
+    HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    hp_mark(ctx, s, "trace_begin");
+    const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && stats;
+    if (any && st) return launch_t<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
+    if (any) return launch_t<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
+    if (st) return launch_t<false, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
+    return launch_t<false, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
+}

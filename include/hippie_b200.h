@@ -1,0 +1,241 @@
+/*
+ * hippie_b200.h — C ABI of the B200-native build-and-trace hot path.
+ *
+ * This is the boundary a host program binds to (cgo / ctypes / JNI style):
+ * plain pointers, 64-bit sizes and status codes, no CUDA or C++ types.
+ * Streams are passed as `void*` (a cudaStream_t; NULL = legacy default stream).
+ *
+ * The entry points replace these reference interfaces (meistdan/hippie,
+ * paths relative to src/hippie/):
+ *   hp_build            BVHBuilder::build / rebuild           rt/bvh/BVHBuilder.h:16-68,
+ *                       LBVHBuilder::build                    rt/bvh/LBVHBuilder.cpp:183-241,
+ *                       PLOCBuilder::build                    rt/bvh/PLOCBuilder.cpp:161-208
+ *   hp_bvh_*            HipBVH (nodes, woop, triangle idx)    rt/bvh/HipBVH.h:19-106
+ *   hp_bvh_cost         HipBVH::getCost                       rt/bvh/HipBVH.cpp:346-370
+ *   hp_bvh_validate     HipBVH::validate                      rt/bvh/HipBVH.cpp:157-307
+ *   hp_refit            HipBVH::update (woopify + refit)      rt/bvh/HipBVH.cpp:472-477
+ *   hp_trace            HipTracer::trace / traceStats         rt/tracer/HipTracer.cpp:13-52
+ *   hp_radix_sort       RadixSort::sort                       radix_sort/RadixSort.cpp:181-238
+ *   hp_env_*            Environment / AppEnvironment          environment/Environment.cpp:290-466,
+ *                                                             environment/AppEnvironment.cpp:10-91
+ * and add the batched and adjoint entry points the reference does not have.
+ *
+ * Every function returns hp_status and never exits the process; the text of
+ * the last error on the calling thread is available from hp_last_error().
+ * All device work is stream-ordered and asynchronous unless stated.
+ */
+#ifndef HIPPIE_B200_H_
+#define HIPPIE_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HP_ABI_VERSION 1
+
+typedef enum hp_status {
+    HP_OK = 0,
+    HP_ERR_CUDA = 1,          /* a CUDA runtime call failed */
+    HP_ERR_ARG = 2,           /* invalid argument (null pointer, size out of range, ...) */
+    HP_ERR_OOM = 3,           /* device or host allocation failed */
+    HP_ERR_TIMEOUT = 4,       /* a host-side wait exceeded its limit */
+    HP_ERR_DEVICE_STATUS = 5, /* a kernel reported an error word (bounded spin gave up, bad index) */
+    HP_ERR_UNSUPPORTED = 6,   /* option not supported by this build */
+    HP_ERR_PARSE = 7          /* environment file could not be parsed */
+} hp_status;
+
+typedef enum hp_method {
+    HP_METHOD_LBVH = 0,       /* Bvh.method lbvh */
+    HP_METHOD_PLOC = 1,       /* Bvh.method ploc */
+    HP_METHOD_ATR = 2         /* Bvh.method atr  (LBVH + agglomerative treelet restructuring) */
+} hp_method;
+
+/* Trace flags (HipTracer: `anyHit` kernel argument and the traceStats variant). */
+#define HP_TRACE_ANY_HIT 1u
+#define HP_TRACE_STATS   2u
+
+/* Triangle mesh in device memory: vertices are 3 floats each, triangles are
+ * 3 int vertex indices each (the Scene vertex / vertIndices buffers). */
+typedef struct hp_mesh {
+    const float* vertices;
+    const int32_t* triangles;
+    int64_t num_vertices;
+    int64_t num_triangles;
+} hp_mesh;
+
+/* Build options: the Bvh.* environment keys of the reference
+ * (environment/AppEnvironment.cpp:52-75) plus Bvh.atrTreeletSize. */
+typedef struct hp_build_params {
+    int32_t method;           /* hp_method                     Bvh.method          */
+    int32_t morton_bits;      /* [6,60]                        Bvh.{lbvh,ploc,atr}MortonCodeBits */
+    int32_t ploc_radius;      /* [1,ploc_max_radius]           Bvh.plocRadius      */
+    int32_t ploc_max_radius;  /* >= 1                          Bvh.plocMaxRadius   */
+    int32_t ploc_adaptive;    /* 0/1                           Bvh.plocAdaptive    */
+    int32_t atr_iterations;   /* [0,25]                        Bvh.atrIterations   */
+    int32_t atr_treelet;      /* [4,30]                        Bvh.atrTreeletSize  */
+    float ct;                 /* > 0                           Bvh.ct              */
+    float ci;                 /* > 0                           Bvh.ci              */
+    int32_t max_leaf_size;    /* (0,1024]                      Bvh.maxLeafSize     */
+    int32_t adaptive_leaf;    /* 0/1                           Bvh.adaptiveLeafSize */
+    int32_t reserved[5];
+} hp_build_params;
+
+/* A built BVH. Device pointers are owned by the library; release with
+ * hp_bvh_free. The node buffer uses the reference's 64-byte binary node
+ * layout (rt/bvh/HipBVHNode.h:116-218):
+ *   int[16]: [0..3] child0 {lo.x, hi.x, lo.y, hi.y}, [4..7] child1 same,
+ *            [8..11] {c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z},
+ *            [12],[13] child indices (a leaf child is ~nodeIndex) or, in a leaf
+ *            node, the triangle range [begin, end), [14] size (~size in a
+ *            leaf), [15] parent index (-1 at the root).
+ * Interior nodes occupy [0, num_interior) with the root at 0; leaf nodes
+ * occupy [num_interior, num_interior + num_leaf).
+ * woop holds 3 float4 per leaf-ordered reference (rt/bvh/HipBVHKernels.cu:35-65),
+ * tri_indices maps a leaf-ordered reference to its scene triangle. */
+typedef struct hp_bvh {
+    void* nodes;
+    void* woop;
+    int32_t* tri_indices;
+    int64_t num_refs;         /* number of references (= triangles)           */
+    int64_t capacity_refs;    /* allocation size in references                */
+    int32_t num_interior;     /* filled by hp_bvh_sync                        */
+    int32_t num_leaf;         /* filled by hp_bvh_sync                        */
+    float scene_box[6];       /* filled by hp_bvh_sync: min xyz, max xyz      */
+    float morton_scale[3];    /* filled by hp_bvh_sync: scale used for keys   */
+    int32_t method;
+    float ct, ci;
+    void* impl;               /* library private                              */
+} hp_bvh;
+
+/* Optional device buffers that receive intermediate results of an LBVH build
+ * (for parity tests). Any pointer may be NULL. Sizes: n = num_triangles. */
+typedef struct hp_build_taps {
+    uint64_t* morton_keys;    /* [n] keys before sorting (always 64-bit)            */
+    uint64_t* sorted_keys;    /* [n] keys after sorting                             */
+    int32_t* sorted_refs;     /* [n] reference index per sorted position            */
+    int32_t* node_parent;     /* [2n-1] binary radix tree before collapse           */
+    int32_t* node_left;       /* [2n-1] left child (leaf node j: j-(n-1))           */
+    int32_t* node_right;      /* [2n-1] right child (leaf node j: j-(n-1)+1)        */
+    float* node_box_min;      /* [2n-1][4] refitted boxes before collapse (w = 0)   */
+    float* node_box_max;      /* [2n-1][4]                                           */
+    float* scene_box;         /* [6]                                                 */
+} hp_build_taps;
+
+typedef struct hp_ctx hp_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+hp_status hp_ctx_create(hp_ctx** out, int32_t device);
+hp_status hp_ctx_destroy(hp_ctx* ctx);
+/* Wait for all work of the context's device; returns HP_ERR_DEVICE_STATUS if a
+ * kernel reported an error word since the last check (and clears it). */
+hp_status hp_ctx_check(hp_ctx* ctx, void* stream);
+const char* hp_last_error(void);
+int32_t hp_abi_version(void);
+/* Phase timing, the counterpart of HipKernel::launchTimed's per-kernel event
+ * times (gpu/HipKernel.cpp:296-325) without host synchronisation: when enabled,
+ * build and trace record a CUDA event after every phase on the stream.
+ * hp_profile_count / hp_profile_get read the phases of the last enabled call
+ * sequence (they synchronise); hp_profile_reset clears them. */
+hp_status hp_profile_enable(hp_ctx* ctx, int32_t on);
+hp_status hp_profile_reset(hp_ctx* ctx);
+int32_t hp_profile_count(hp_ctx* ctx);
+hp_status hp_profile_get(hp_ctx* ctx, int32_t i, char* name, int64_t name_size, float* ms);
+/* Number of kernels this library has launched from the calling thread. */
+int64_t hp_launch_count(void);
+
+/* ---- build (BVHBuilder) --------------------------------------------------- */
+void hp_build_params_default(hp_build_params* p);
+/* Build a BVH over mesh m into *out (allocates on first use; reuses the
+ * allocation on later builds of the same or smaller size, like
+ * BVHBuilder::rebuild). No host synchronisation; capturable in a CUDA graph
+ * once out has capacity for the mesh. taps may be NULL. */
+hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
+                   hp_bvh* out, const hp_build_taps* taps, void* stream);
+/* Synchronise the stream and fill num_interior, num_leaf, scene_box, morton_scale. */
+hp_status hp_bvh_sync(hp_ctx* ctx, hp_bvh* bvh, void* stream);
+/* Copy the BVH to host memory (any pointer may be NULL): nodes_host receives
+ * (num_interior + num_leaf) * 64 bytes, woop_host num_refs * 48 bytes,
+ * tri_host num_refs int32. Synchronous; calls hp_bvh_sync first. */
+hp_status hp_bvh_download(hp_ctx* ctx, hp_bvh* bvh, void* nodes_host, void* woop_host,
+                          int32_t* tri_host, void* stream);
+hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh);
+/* SAH cost as HipBVH::getCost (sum over nodes of ct|ci*size times node area
+ * over scene area); summed in a fixed order in double precision. Synchronous. */
+hp_status hp_bvh_cost(hp_ctx* ctx, const hp_bvh* bvh, double* cost, void* stream);
+/* Structural validation as HipBVH::validate; *valid = 1 if consistent.
+ * Synchronous (copies the BVH to the host). */
+hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m,
+                          int32_t* valid, void* stream);
+/* Refit-only update after vertex moves (HipBVH::update): re-woopify and
+ * recompute every node box bottom-up from the mesh's current vertices. */
+hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream);
+
+/* ---- trace (HipTracer) ---------------------------------------------------- */
+/* rays: 8 floats per ray {ox, oy, oz, tmin, dx, dy, dz, tmax} (Ray, rt/ray/Ray.h:16-27);
+ * results: 4 int32 per ray {triangle id, t bits, u bits, v bits} (RayResult);
+ * on a miss only {-1, tmax bits} are written. stats (or NULL): 2 int32 per ray
+ * {traversed nodes, tested triangles}. Closest hits break ties in t by the
+ * lower triangle id. */
+hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays,
+                   int32_t* results, int32_t* stats, uint32_t flags, void* stream);
+
+/* ---- adjoint ------------------------------------------------------------ */
+/* Scatter dL/d(t,u,v) (3 floats per ray) of closest hits into dL/dvertices
+ * (3 floats per vertex, accumulated: the caller zeroes it). results must come
+ * from hp_trace on the same bvh, rays and mesh. Misses contribute nothing. */
+hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays,
+                           const int32_t* results, const float* dl_dtuv, int64_t num_rays,
+                           float* dl_dvertices, void* stream);
+
+/* ---- primitives ------------------------------------------------------------ */
+/* Stable LSD radix sort of (key, value) pairs by key bits [0, bits). key_bytes
+ * is 4 or 8. vals_in may be NULL (values are then 0..n-1). Output in keys_out /
+ * vals_out (may not alias the inputs). Uses the context's scratch arena. */
+hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in,
+                        void* keys_out, int32_t* vals_out, int64_t n,
+                        int32_t key_bytes, int32_t bits, void* stream);
+
+/* ---- environment files (Environment / AppEnvironment) ------------------- */
+typedef struct hp_env hp_env;
+hp_status hp_env_create(hp_env** out);      /* registers the reference's options */
+hp_status hp_env_destroy(hp_env* env);
+/* Parse a block-structured env file; unknown keys and malformed values make
+ * the parse fail (HP_ERR_PARSE) like Environment::readEnvFile. */
+hp_status hp_env_read_file(hp_env* env, const char* path);
+hp_status hp_env_read_string(hp_env* env, const char* text);
+/* First value of an option (or its default); HP_ERR_ARG if unknown or unset. */
+hp_status hp_env_get_int(const hp_env* env, const char* name, int32_t* value);
+hp_status hp_env_get_float(const hp_env* env, const char* name, float* value);
+hp_status hp_env_get_bool(const hp_env* env, const char* name, int32_t* value);
+hp_status hp_env_get_string(const hp_env* env, const char* name, char* buf, int64_t buf_size);
+/* Fill build parameters from the Bvh.* keys with the builders' range checks
+ * (out-of-range values keep the default, as the reference setters do). */
+hp_status hp_env_build_params(const hp_env* env, hp_build_params* p);
+
+/* ---- synthetic inputs (host memory, deterministic, thread-count independent) */
+/* Uniform triangle soup: centre ~ U[0,1]^3, vertex = centre + U[-h,h]^3. */
+hp_status hp_gen_uniform_mesh(uint64_t seed, int64_t n, float half_extent,
+                              float* vertices, int32_t* triangles);
+/* Clustered soup: n_clusters centres ~ U[0,1]^3, triangle i in cluster i % n_clusters,
+ * centre = cluster centre + N(0, sigma^2)^3, vertex = centre + U[-h,h]^3. */
+hp_status hp_gen_clustered_mesh(uint64_t seed, int64_t n, int32_t n_clusters, float sigma,
+                                float half_extent, float* vertices, int32_t* triangles);
+/* Heightfield nx*ny vertices on [0,1]x[0,ny/(nx)] ... see implementation notes:
+ * domain [0,sx]x[0,sy], z = sum of n_waves sinusoids; 2 triangles per cell. */
+hp_status hp_gen_heightfield(uint64_t seed, int32_t nx, int32_t ny, float sx, float sy,
+                             int32_t n_waves, float* vertices, int32_t* triangles);
+/* Rays aimed at targets: origin ~ U[lo,hi]^3, target ~ U[0,1]^3, tmin 0, tmax inf. */
+hp_status hp_gen_rays_targeted(uint64_t seed, int64_t n, float lo, float hi, float* rays);
+/* Rays with origin ~ U(box) and direction uniform on the sphere. */
+hp_status hp_gen_rays_sphere(uint64_t seed, int64_t n, const float* box6, float* rays);
+/* Downward rays on a jittered nx*ny grid over [0,sx]x[0,sy], origin z = z0. */
+hp_status hp_gen_rays_grid_down(uint64_t seed, int32_t nx, int32_t ny, float sx, float sy,
+                                float z0, float* rays);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIPPIE_B200_H_ */

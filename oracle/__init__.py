@@ -1,0 +1,157 @@
+"""CPU oracle — test infrastructure only (see oracle.cpp).
+
+ctypes access to liboracle.so, a C++/OpenMP restatement of the reference's
+build-and-trace path. Only the tests, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py use it; the shipped library never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_lib = None
+
+_P = C.c_void_p
+_SIGS = {
+    "or_tri_boxes": (None, [_P, _P, C.c_int64, _P, _P, _P]),
+    "or_morton": (None, [C.c_int64, _P, _P, _P, _P, C.c_int, _P, _P]),
+    "or_sort": (None, [C.c_int64, _P, C.c_int, _P, _P]),
+    "or_karras": (None, [C.c_int, _P, _P, _P, _P]),
+    "or_refit": (None, [C.c_int, _P, _P, _P, _P, _P, _P, C.c_float, C.c_float, C.c_int, C.c_int,
+                        _P, _P, _P, _P, _P]),
+    "or_collapse": (C.c_int64, [C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "or_woopify": (None, [C.c_int64, _P, _P, _P, _P]),
+    "or_build_lbvh": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
+                                  _P, _P, _P, _P, _P, _P, _P]),
+    "or_cost": (C.c_double, [_P, C.c_int64, _P, C.c_float, C.c_float]),
+    "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
+    "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
+    "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
+    "or_adjoint64": (None, [_P, _P, _P, _P, _P, C.c_int64, _P]),
+}
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    src = HERE / "oracle.cpp"
+    if not LIB.exists() or (src.exists() and src.stat().st_mtime > LIB.stat().st_mtime):
+        subprocess.run(["make", "-C", str(HERE), "liboracle.so"], check=True, capture_output=True)
+    lib = C.CDLL(str(LIB))
+    for k, (res, args) in _SIGS.items():
+        f = getattr(lib, k)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def tri_boxes(verts, tris):
+    n = tris.shape[0]
+    bmin = np.zeros((n, 4), np.float32)
+    bmax = np.zeros((n, 4), np.float32)
+    box = np.zeros(6, np.float32)
+    load().or_tri_boxes(_p(verts), _p(tris), n, _p(bmin), _p(bmax), _p(box))
+    return bmin, bmax, box
+
+
+def morton(bmin, bmax, scene_box, bits, scale=None):
+    n = bmin.shape[0]
+    keys = np.zeros(n, np.uint64)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    load().or_morton(n, _p(bmin), _p(bmax), _p(np.ascontiguousarray(scene_box, np.float32)), _p(s_in), bits,
+                     _p(keys), _p(sc))
+    return keys, sc
+
+
+def sort(keys, bits):
+    n = keys.shape[0]
+    sk = np.zeros(n, np.uint64)
+    sr = np.zeros(n, np.int32)
+    load().or_sort(n, _p(np.ascontiguousarray(keys, np.uint64)), bits, _p(sk), _p(sr))
+    return sk, sr
+
+
+def karras(skeys):
+    n = skeys.shape[0]
+    nn = 2 * n - 1
+    parent = np.zeros(nn, np.int32)
+    left = np.zeros(nn, np.int32)
+    right = np.zeros(nn, np.int32)
+    load().or_karras(n, _p(skeys), _p(parent), _p(left), _p(right))
+    return parent, left, right
+
+
+def refit(verts, tris, sorted_tri, parent, left, right, ct=3.0, ci=2.0, adaptive=1, max_leaf=8):
+    n = sorted_tri.shape[0]
+    nn = 2 * n - 1
+    bmin = np.zeros((nn, 4), np.float32)
+    bmax = np.zeros((nn, 4), np.float32)
+    size = np.zeros(nn, np.int32)
+    cost = np.zeros(nn, np.float32)
+    state = np.zeros(nn, np.int32)
+    load().or_refit(n, _p(verts), _p(tris), _p(sorted_tri), _p(parent), _p(left), _p(right), ct, ci, adaptive,
+                    max_leaf, _p(bmin), _p(bmax), _p(size), _p(cost), _p(state))
+    return bmin, bmax, size, cost, state
+
+
+def build_lbvh(verts, tris, bits=60, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+    """Full LBVH build; returns dict with nodes (N,16) int32, woop (n,12), tri_idx, counts, box, scale."""
+    n = tris.shape[0]
+    cap = max(2 * n - 1, 3)
+    nodes = np.zeros((cap, 16), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    cnt = load().or_build_lbvh(_p(verts), _p(tris), n, bits, ct, ci, adaptive, max_leaf, _p(s_in), _p(nodes),
+                               _p(woop), _p(tri), _p(counts), _p(box), _p(sc))
+    return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
+
+
+def cost(nodes, scene_box, ct=3.0, ci=2.0):
+    return load().or_cost(_p(np.ascontiguousarray(nodes)), nodes.shape[0],
+                          _p(np.ascontiguousarray(scene_box, np.float32)), ct, ci)
+
+
+def trace(nodes, woop, tri_idx, rays, any_hit=False, stats=False):
+    r = rays.shape[0]
+    res = np.zeros((r, 4), np.int32)
+    st = np.zeros((r, 2), np.int32) if stats else None
+    load().or_trace(_p(np.ascontiguousarray(nodes)), _p(np.ascontiguousarray(woop)),
+                    _p(np.ascontiguousarray(tri_idx)), tri_idx.shape[0], _p(np.ascontiguousarray(rays)), r,
+                    _p(res), _p(st), int(any_hit))
+    return (res, st) if stats else res
+
+
+def brute64(verts, tris, rays):
+    out = np.zeros((rays.shape[0], 4), np.float64)
+    load().or_brute64(_p(verts), _p(tris), tris.shape[0], _p(np.ascontiguousarray(rays)), rays.shape[0], _p(out))
+    return out
+
+
+def adjoint64(verts, tris, rays, results, dl):
+    out = np.zeros(verts.shape, np.float64)
+    load().or_adjoint64(_p(verts), _p(tris), _p(np.ascontiguousarray(rays)), _p(np.ascontiguousarray(results)),
+                        _p(np.ascontiguousarray(dl, np.float32)), rays.shape[0], _p(out))
+    return out
+
+
+def intersect64(v0, v1, v2, o, d, tmin=0.0):
+    tuv = np.zeros(3, np.float64)
+    a = [np.ascontiguousarray(x, np.float64) for x in (v0, v1, v2, o, d)]
+    hit = load().or_intersect64(*[_p(x) for x in a], tmin, _p(tuv))
+    return bool(hit), tuv

@@ -1,0 +1,700 @@
+// CPU ORACLE — test infrastructure only.
+//
+// A plain C++/OpenMP restatement of the reference's build-and-trace path
+// (meistdan/hippie, paths relative to src/hippie/). It is the checker the
+// parity tests compare the CUDA library against, and the CPU baseline the
+// benchmark times; nothing in the shipped library calls it.
+//
+// Each function cites the reference code it restates. Floating-point
+// expressions are written with the same explicit fmaf calls the CUDA kernels
+// use (this file is compiled with -ffp-contract=off), so oracle and GPU agree
+// bit for bit. Two places differ from the reference's fast-math JIT build and
+// are handled explicitly:
+//   * the Morton scale 1/diagonal is an approximate quotient on the GPU; the
+//     oracle takes that value as an input (or uses the IEEE quotient when run
+//     alone);
+//   * reciprocals in woopify and traversal use IEEE 1/x on both sides.
+// Parity pin: the reference ships no tests, fixtures or golden vectors (its
+// test/ folder holds benchmark sweep scripts only), so this restatement is
+// pinned by known-answer vectors derived by hand from the reference formulas
+// (tests/golden/) and by structural invariants; see the tests.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+const float MAXF = 3.402823466e+38f;
+
+// cvt.rzi.u32.f32: truncate toward zero, saturate, NaN -> 0.
+inline uint32_t f2u_rz_sat(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967296.0f) return 0xffffffffu;
+    return (uint32_t)x;
+}
+
+// rt/HipUtil.h:35-49
+inline uint32_t spread10(uint32_t x) {
+    x = (x | (x << 16)) & 0x030000FFu;
+    x = (x | (x << 8)) & 0x0300F00Fu;
+    x = (x | (x << 4)) & 0x030C30C3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+inline uint32_t morton30(uint32_t x, uint32_t y, uint32_t z) {
+    return spread10(x) | (spread10(y) << 1) | (spread10(z) << 2);
+}
+// rt/HipUtil.h:72-82
+inline uint64_t morton60(uint32_t x, uint32_t y, uint32_t z) {
+    uint64_t lo = morton30(x & 1023u, y & 1023u, z & 1023u);
+    uint64_t hi = morton30(x >> 10, y >> 10, z >> 10);
+    return (hi << 30) | lo;
+}
+
+// util/AABB.h:33 with the fast-math contraction 2*fma(dz,dx,fma(dx,dy,dy*dz)).
+inline float area6(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
+    if (!(mnx <= mxx && mny <= mxy && mnz <= mxz)) return 0.0f;
+    float dx = mxx - mnx, dy = mxy - mny, dz = mxz - mnz;
+    return 2.0f * std::fmaf(dz, dx, std::fmaf(dx, dy, dy * dz));
+}
+
+// detImpl<3> (util/Math.h:326-330), terms in reference order, one fma per term.
+inline float det3(const float* a) {
+#define A(r, c) a[(r) + 3 * (c)]
+    float acc = (A(0, 0) * A(1, 1)) * A(2, 2);
+    acc = std::fmaf(-(A(0, 0) * A(1, 2)), A(2, 1), acc);
+    acc = std::fmaf(A(1, 0) * A(2, 1), A(0, 2), acc);
+    acc = std::fmaf(-(A(1, 0) * A(2, 2)), A(0, 1), acc);
+    acc = std::fmaf(A(2, 0) * A(0, 1), A(1, 2), acc);
+    acc = std::fmaf(-(A(2, 0) * A(0, 2)), A(1, 1), acc);
+#undef A
+    return acc;
+}
+
+// woopifyTriangle (rt/bvh/HipBVHKernels.cu:12-33) with inverse() (util/Math.h:350-367).
+void woop(const float* v0, const float* v1, const float* v2, float* w /*12*/) {
+    float ax = v0[0] - v2[0], ay = v0[1] - v2[1], az = v0[2] - v2[2];
+    float bx = v1[0] - v2[0], by = v1[1] - v2[1], bz = v1[2] - v2[2];
+    float nx = std::fmaf(ay, bz, -(az * by));
+    float ny = std::fmaf(az, bx, -(ax * bz));
+    float nz = std::fmaf(ax, by, -(ay * bx));
+    float M[16] = {ax, ay, az, 0.0f, bx, by, bz, 0.0f, nx, ny, nz, 0.0f, v2[0], v2[1], v2[2], 1.0f};
+    float R[16];
+    float d = 0.0f, si = 1.0f;
+    for (int i = 0; i < 4; ++i) {
+        float sj = si;
+        for (int j = 0; j < 4; ++j) {
+            float sub[9];
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l)
+                    sub[k + 3 * l] = M[((k < j) ? k : k + 1) + 4 * ((l < i) ? l : l + 1)];
+            float dd = det3(sub) * sj;
+            R[i + 4 * j] = dd;
+            d = std::fmaf(dd, M[j + 4 * i], d);
+            sj = -sj;
+        }
+        si = -si;
+    }
+    float rd = (d != 0.0f) ? 1.0f / d : 0.0f;
+    for (int k = 0; k < 16; ++k) R[k] = (R[k] * rd) * 4.0f;
+#define IM(c, r) R[(r) + 4 * (c)]
+    w[0] = IM(0, 2); w[1] = IM(1, 2); w[2] = IM(2, 2); w[3] = -IM(3, 2);
+    w[4] = IM(0, 0); w[5] = IM(1, 0); w[6] = IM(2, 0); w[7] = IM(3, 0);
+    w[8] = IM(0, 1); w[9] = IM(1, 1); w[10] = IM(2, 1); w[11] = IM(3, 1);
+#undef IM
+}
+
+template <typename K> inline int clz_k(K x);
+template <> inline int clz_k<uint64_t>(uint64_t x) { return x ? __builtin_clzll(x) : 64; }
+
+// delta<unsigned long long> (rt/bvh/HipBVHUtil.h:17-25).
+inline int delta(const uint64_t* k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint64_t a = k[i], b = k[j];
+    if (a != b) return clz_k<uint64_t>(a ^ b);
+    return clz_k<uint64_t>((uint64_t)(int64_t)(i ^ j)) + 64;
+}
+
+inline void tri_box(const float* verts, const int32_t* tris, int64_t t, float* mn, float* mx) {
+    for (int a = 0; a < 3; ++a) { mn[a] = MAXF; mx[a] = -MAXF; }
+    for (int k = 0; k < 3; ++k) {
+        const float* p = verts + 3 * (int64_t)tris[3 * t + k];
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(mn[a], p[a]);
+            mx[a] = std::max(mx[a], p[a]);
+        }
+    }
+}
+
+struct bin_node {
+    float f[12];
+    int32_t c0, c1, size, parent;
+};
+static_assert(sizeof(bin_node) == 64, "node");
+
+void make_node(bin_node& n, const float* amn, const float* amx, const float* bmn, const float* bmx,
+               int c0, int c1, int size, int parent) {
+    n.f[0] = amn[0]; n.f[1] = amx[0]; n.f[2] = amn[1]; n.f[3] = amx[1];
+    n.f[4] = bmn[0]; n.f[5] = bmx[0]; n.f[6] = bmn[1]; n.f[7] = bmx[1];
+    n.f[8] = amn[2]; n.f[9] = amx[2]; n.f[10] = bmn[2]; n.f[11] = bmx[2];
+    n.c0 = c0; n.c1 = c1; n.size = size; n.parent = parent;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- A1/A2: setupBoxes (rt/bvh/LBVHBuilderKernels.cu:65-98) + scene box ----------
+void or_tri_boxes(const float* verts, const int32_t* tris, int64_t n, float* bmin4, float* bmax4,
+                  float* scene_box) {
+    float smn[3] = {MAXF, MAXF, MAXF}, smx[3] = {-MAXF, -MAXF, -MAXF};
+    for (int64_t i = 0; i < n; ++i) {
+        float mn[3], mx[3];
+        tri_box(verts, tris, i, mn, mx);
+        for (int a = 0; a < 3; ++a) {
+            bmin4[4 * i + a] = mn[a];
+            bmax4[4 * i + a] = mx[a];
+            smn[a] = std::min(smn[a], mn[a]);
+            smx[a] = std::max(smx[a], mx[a]);
+        }
+        bmin4[4 * i + 3] = 0.0f;
+        bmax4[4 * i + 3] = 0.0f;
+    }
+    for (int a = 0; a < 3; ++a) { scene_box[a] = smn[a]; scene_box[3 + a] = smx[a]; }
+}
+
+// ---- A3: computeMortonCodes60 (rt/bvh/LBVHBuilderKernels.cu:131-160) --------------
+// scale: the per-axis 1/diagonal to use; if null, the IEEE quotient.
+void or_morton(int64_t n, const float* bmin4, const float* bmax4, const float* scene_box,
+               const float* scale_in, int bits, uint64_t* keys, float* scale_out) {
+    float scale[3];
+    for (int a = 0; a < 3; ++a)
+        scale[a] = scale_in ? scale_in[a] : 1.0f / (scene_box[3 + a] - scene_box[a]);
+    if (scale_out) for (int a = 0; a < 3; ++a) scale_out[a] = scale[a];
+    const float q20 = 1048575.0f;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        uint32_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            float c = (bmin4[4 * i + a] + bmax4[4 * i + a]) * 0.5f;
+            q[a] = f2u_rz_sat(((c - scene_box[a]) * scale[a]) * q20);
+        }
+        keys[i] = morton60(q[0], q[1], q[2]) >> (60 - bits);
+    }
+}
+
+// ---- A4: stable sort (RadixSort::sort, radix_sort/RadixSort.cpp:181-238) -----------
+// Stable LSD radix sort by key bits [0, bits), 8-bit digits, OpenMP histograms.
+// sorted_refs receives the original index of every sorted position.
+void or_sort(int64_t n, const uint64_t* keys, int bits, uint64_t* sorted_keys, int32_t* sorted_refs) {
+    std::vector<uint64_t> ka(keys, keys + n), kb(n);
+    std::vector<int32_t> va(n), vb(n);
+    for (int64_t i = 0; i < n; ++i) va[i] = (int32_t)i;
+    const int passes = (bits + 7) / 8;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        int nt = 1;
+#ifdef _OPENMP
+        nt = omp_get_max_threads();
+#endif
+        std::vector<int64_t> hist((size_t)nt * 256, 0);
+        const int64_t chunk = (n + nt - 1) / nt;
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            int64_t b = std::min(n, t * chunk), e = std::min(n, b + chunk);
+            int64_t* h = &hist[(size_t)t * 256];
+            for (int64_t i = b; i < e; ++i) h[(ka[i] >> shift) & 255]++;
+        }
+        int64_t run = 0;
+        for (int d = 0; d < 256; ++d)
+            for (int t = 0; t < nt; ++t) {
+                int64_t c = hist[(size_t)t * 256 + d];
+                hist[(size_t)t * 256 + d] = run;
+                run += c;
+            }
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            int64_t b = std::min(n, t * chunk), e = std::min(n, b + chunk);
+            int64_t* h = &hist[(size_t)t * 256];
+            for (int64_t i = b; i < e; ++i) {
+                int64_t pos = h[(ka[i] >> shift) & 255]++;
+                kb[pos] = ka[i];
+                vb[pos] = va[i];
+            }
+        }
+        ka.swap(kb);
+        va.swap(vb);
+    }
+    std::memcpy(sorted_keys, ka.data(), n * 8);
+    std::memcpy(sorted_refs, va.data(), n * 4);
+}
+
+// ---- A6: construct<T> (rt/bvh/LBVHBuilderKernels.cu:11-63) ----------------------------
+void or_karras(int n, const uint64_t* keys, int32_t* parent, int32_t* left, int32_t* right) {
+    if (n >= 1) parent[0] = -1;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n - 1; ++i) {
+        const int dr = delta(keys, n, i, i + 1), dl = delta(keys, n, i, i - 1);
+        const int d = (dr - dl > 0) - (dr - dl < 0);
+        const int dmin = delta(keys, n, i, i - d);
+        int lmax = 2;
+        while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = delta(keys, n, i, j);
+        int s = 0, k = 2, t;
+        do {
+            t = (l + k - 1) / k;
+            k <<= 1;
+            if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        } while (t > 1);
+        const int gamma = i + s * d + std::min(d, 0);
+        int lc = gamma, rc = gamma + 1;
+        if (std::min(i, j) == gamma) lc += n - 1;
+        if (std::max(i, j) == gamma + 1) rc += n - 1;
+        left[i] = lc;
+        right[i] = rc;
+        parent[lc] = i;
+        parent[rc] = i;
+    }
+    // leaf nodes (setupLeaves, LBVHBuilderKernels.cu:162-195): left = i, right = i + 1
+    for (int i = 0; i < n; ++i) {
+        left[n - 1 + i] = i;
+        right[n - 1 + i] = i + 1;
+    }
+}
+
+// ---- A5/A7 + collapse DP: refit (LBVHBuilderKernels.cu:254-305),
+// computeSizes (BVHCollapserKernels.cu:11-56), computeNodeStatesAdaptive (:58-136),
+// computeNodeStates (:138-184). Post-order over the tree from the root.
+// Outputs per node (2n-1): box min/max (4 floats, w = 0), size, cost, state.
+void or_refit(int n, const float* verts, const int32_t* tris, const int32_t* sorted_tri,
+              const int32_t* parent, const int32_t* left, const int32_t* right, float ct, float ci,
+              int adaptive, int max_leaf, float* bmin4, float* bmax4, int32_t* size, float* cost,
+              int32_t* state) {
+    (void)parent;
+    const int nn = 2 * n - 1;
+    for (int p = 0; p < n; ++p) {
+        const int j = n - 1 + p;
+        float mn[3], mx[3];
+        tri_box(verts, tris, sorted_tri[p], mn, mx);
+        for (int a = 0; a < 3; ++a) { bmin4[4 * j + a] = mn[a]; bmax4[4 * j + a] = mx[a]; }
+        bmin4[4 * j + 3] = bmax4[4 * j + 3] = 0.0f;
+        size[j] = 1;
+        cost[j] = adaptive ? ci * area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) : 0.0f;
+        state[j] = 0;
+    }
+    if (n < 2) return;
+    // iterative post-order
+    std::vector<int> stack;
+    std::vector<char> expanded(nn, 0);
+    stack.push_back(0);
+    while (!stack.empty()) {
+        int v = stack.back();
+        if (v >= n - 1) { stack.pop_back(); continue; }
+        if (!expanded[v]) {
+            expanded[v] = 1;
+            stack.push_back(right[v]);
+            stack.push_back(left[v]);
+            continue;
+        }
+        stack.pop_back();
+        const int l = left[v], r = right[v];
+        float mn[3], mx[3];
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(bmin4[4 * l + a], bmin4[4 * r + a]);
+            mx[a] = std::max(bmax4[4 * l + a], bmax4[4 * r + a]);
+            bmin4[4 * v + a] = mn[a];
+            bmax4[4 * v + a] = mx[a];
+        }
+        bmin4[4 * v + 3] = bmax4[4 * v + 3] = 0.0f;
+        size[v] = size[l] + size[r];
+        if (adaptive) {
+            const float A = area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]);
+            const float c_int = std::fmaf(ct, A, cost[l]) + cost[r];
+            const float c_leaf = (ci * A) * (float)size[v];
+            state[v] = (c_leaf < c_int) ? 0 : 1;
+            cost[v] = state[v] ? c_int : c_leaf;
+        } else {
+            state[v] = (size[v] <= max_leaf) ? 0 : 1;
+            cost[v] = 0.0f;
+        }
+    }
+}
+
+// ---- A9/A10: collapse into 64-byte binary nodes ----------------------------------------
+// Leaf assignment as computeLeafIndices (BVHCollapserKernels.cu:186-217): the
+// leaf of a reference is its topmost state-0 ancestor below the root (the
+// root is always interior). Node numbering is the canonical order for trees
+// over contiguous reference ranges: interior nodes by split position with the
+// root moved to 0, leaves by their first reference; triangles stay in sorted
+// order. Returns the node count; counts[0] = interior, counts[1] = leaves.
+int64_t or_collapse(int n, const int32_t* parent, const int32_t* left, const int32_t* right,
+                    const float* bmin4, const float* bmax4, const int32_t* size, const int32_t* state,
+                    void* nodes_out, int32_t* counts) {
+    bin_node* out = reinterpret_cast<bin_node*>(nodes_out);
+    if (n < 2) { counts[0] = counts[1] = 0; return 0; }
+    const int nn = 2 * n - 1;
+    // lo/hi range of every node
+    std::vector<int> lo(nn), hi(nn);
+    for (int p = 0; p < n; ++p) lo[n - 1 + p] = hi[n - 1 + p] = p;
+    {
+        std::vector<int> st{0};
+        std::vector<char> ex(nn, 0);
+        while (!st.empty()) {
+            int v = st.back();
+            if (v >= n - 1) { st.pop_back(); continue; }
+            if (!ex[v]) { ex[v] = 1; st.push_back(right[v]); st.push_back(left[v]); continue; }
+            st.pop_back();
+            lo[v] = lo[left[v]];
+            hi[v] = hi[right[v]];
+        }
+    }
+    // leaf index of every reference (walk to the root)
+    std::vector<int> leaf_of(n);
+    for (int p = 0; p < n; ++p) {
+        int node = n - 1 + p, leaf = node, par = parent[node];
+        while (par > 0) {
+            if (state[par] == 0) leaf = par;
+            node = par;
+            par = parent[node];
+        }
+        leaf_of[p] = leaf;
+    }
+    std::vector<char> is_leaf(nn, 0), alive(nn, 0);
+    for (int p = 0; p < n; ++p) is_leaf[leaf_of[p]] = 1;
+    // surviving interior nodes: ancestors of collapsed leaves
+    for (int v = 0; v < nn; ++v)
+        if (is_leaf[v]) {
+            alive[v] = 1;
+            for (int a = parent[v]; a >= 0 && !alive[a]; a = parent[a]) alive[a] = 1;
+        }
+    // numbering
+    std::vector<int> split_rank(n - 1, -1);  // by split position gamma
+    int num_int = 0;
+    std::vector<int> gamma_of(n - 1);
+    for (int v = 0; v < n - 1; ++v) gamma_of[v] = hi[left[v]];
+    std::vector<int> int_at(n - 1, -1);
+    for (int v = 0; v < n - 1; ++v)
+        if (alive[v] && !is_leaf[v]) int_at[gamma_of[v]] = v;
+    std::vector<int> new_int(nn, -1);
+    for (int g = 0; g < n - 1; ++g)
+        if (int_at[g] >= 0) split_rank[g] = num_int++;
+    const int root_rank = split_rank[gamma_of[0]];
+    for (int v = 0; v < n - 1; ++v)
+        if (alive[v] && !is_leaf[v]) {
+            int r = split_rank[gamma_of[v]];
+            new_int[v] = (v == 0) ? 0 : (r < root_rank ? r + 1 : r);
+        }
+    std::vector<int> leaf_rank(n, -1);
+    int num_leaf = 0;
+    std::vector<int> leaf_at(n, -1);
+    for (int v = 0; v < nn; ++v)
+        if (is_leaf[v]) leaf_at[lo[v]] = v;
+    for (int p = 0; p < n; ++p)
+        if (leaf_at[p] >= 0) leaf_rank[p] = num_leaf++;
+    auto ref_of = [&](int v) -> int {
+        if (is_leaf[v]) return ~(num_int + leaf_rank[lo[v]]);
+        return new_int[v];
+    };
+    auto box = [&](int v, float* mn, float* mx) {
+        for (int a = 0; a < 3; ++a) { mn[a] = bmin4[4 * v + a]; mx[a] = bmax4[4 * v + a]; }
+    };
+    for (int v = 0; v < nn; ++v) {
+        if (!alive[v]) continue;
+        const int par = (v == 0) ? -1 : new_int[parent[v]];
+        if (is_leaf[v]) {
+            float mn[3], mx[3];
+            box(v, mn, mx);
+            make_node(out[num_int + leaf_rank[lo[v]]], mn, mx, mn, mx, lo[v], hi[v] + 1, ~size[v], par);
+        } else {
+            float amn[3], amx[3], bmn[3], bmx[3];
+            box(left[v], amn, amx);
+            box(right[v], bmn, bmx);
+            make_node(out[new_int[v]], amn, amx, bmn, bmx, ref_of(left[v]), ref_of(right[v]), size[v], par);
+        }
+    }
+    counts[0] = num_int;
+    counts[1] = num_leaf;
+    return (int64_t)num_int + num_leaf;
+}
+
+// ---- A11: woopifyTriangles (rt/bvh/HipBVHKernels.cu:35-65) ---------------------------------
+void or_woopify(int64_t n, const float* verts, const int32_t* tris, const int32_t* tri_idx, float* woop4) {
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < n; ++r) {
+        const int32_t* t = tris + 3 * (int64_t)tri_idx[r];
+        woop(verts + 3 * (int64_t)t[0], verts + 3 * (int64_t)t[1], verts + 3 * (int64_t)t[2], woop4 + 12 * r);
+    }
+}
+
+// Single-triangle BVH: root with the triangle's leaf and an empty leaf.
+int64_t or_single(const float* verts, const int32_t* tris, void* nodes_out, int32_t* counts) {
+    bin_node* out = reinterpret_cast<bin_node*>(nodes_out);
+    float mn[3], mx[3], emn[3] = {MAXF, MAXF, MAXF}, emx[3] = {-MAXF, -MAXF, -MAXF};
+    tri_box(verts, tris, 0, mn, mx);
+    make_node(out[0], mn, mx, emn, emx, ~1, ~2, 1, -1);
+    make_node(out[1], mn, mx, mn, mx, 0, 1, ~1, 0);
+    make_node(out[2], emn, emx, emn, emx, 1, 1, ~0, 0);
+    counts[0] = 1;
+    counts[1] = 2;
+    return 3;
+}
+
+// ---- whole LBVH build (LBVHBuilder::build, rt/bvh/LBVHBuilder.cpp:183-241) -----------------
+// nodes_out: (2n-1 or 3) * 64 bytes; woop4: 12 floats per reference.
+int64_t or_build_lbvh(const float* verts, const int32_t* tris, int64_t n64, int bits, float ct, float ci,
+                      int adaptive, int max_leaf, const float* scale_in, void* nodes_out, float* woop4,
+                      int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    if (n == 0) { counts[0] = counts[1] = 0; return 0; }
+    if (n == 1) {
+        tri_idx[0] = 0;
+        or_woopify(1, verts, tris, tri_idx, woop4);
+        float mn[3], mx[3];
+        tri_box(verts, tris, 0, mn, mx);
+        for (int a = 0; a < 3; ++a) { scene_box[a] = mn[a]; scene_box[3 + a] = mx[a]; }
+        return or_single(verts, tris, nodes_out, counts);
+    }
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    or_sort(n, keys.data(), bits, skeys.data(), tri_idx);
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), left(nn), right(nn), size(nn), state(nn);
+    or_karras(n, skeys.data(), parent.data(), left.data(), right.data());
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn), cost(nn);
+    or_refit(n, verts, tris, tri_idx, parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    or_woopify(n, verts, tris, tri_idx, woop4);
+    return or_collapse(n, parent.data(), left.data(), right.data(), nbmin.data(), nbmax.data(), size.data(),
+                       state.data(), nodes_out, counts);
+}
+
+// ---- A12: HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370, HipBVHKernels.cu:184-238) ----------
+double or_cost(const void* nodes_in, int64_t count, const float* scene_box, float ct, float ci) {
+    const bin_node* nd = reinterpret_cast<const bin_node*>(nodes_in);
+    const double sa = area6(scene_box[0], scene_box[1], scene_box[2], scene_box[3], scene_box[4], scene_box[5]);
+    double c = 0.0;
+    for (int64_t i = 0; i < count; ++i) {
+        const float* f = nd[i].f;
+        float mn[3] = {std::min(f[0], f[4]), std::min(f[2], f[6]), std::min(f[8], f[10])};
+        float mx[3] = {std::max(f[1], f[5]), std::max(f[3], f[7]), std::max(f[9], f[11])};
+        double a = area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) / sa;
+        if (nd[i].size < 0) c += (double)ci * a * (double)(~nd[i].size);
+        else c += (double)ct * a;
+    }
+    return c;
+}
+
+// ---- A13: closest-hit traversal (rt/tracer/HipTracerBinKernels.cu:19-286) ------------------
+// Per ray: near child first, far child pushed; leaves handled as they are reached;
+// Woop test with the kernel's fma order; ties in t go to the lower triangle id.
+void or_trace(const void* nodes_in, const float* woop4, const int32_t* tri_idx, int64_t num_refs,
+              const float* rays, int64_t num_rays, int32_t* results, int32_t* stats, int any_hit) {
+    const bin_node* nodes = reinterpret_cast<const bin_node*>(nodes_in);
+    const float ooeps = 8.2718061255302767e-25f;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t ri = 0; ri < num_rays; ++ri) {
+        const float* ry = rays + 8 * ri;
+        const float ox = ry[0], oy = ry[1], oz = ry[2], tmin = ry[3];
+        const float dx = ry[4], dy = ry[5], dz = ry[6];
+        float hit_t = ry[7], hit_u = 0.0f, hit_v = 0.0f;
+        int hit = -1, n_nodes = 0, n_tris = 0;
+        auto srcp = [&](float d) { return 1.0f / (std::fabs(d) > ooeps ? d : std::copysign(ooeps, d)); };
+        const float idx = srcp(dx), idy = srcp(dy), idz = srcp(dz);
+        const float oodx = ox * idx, oody = oy * idy, oodz = oz * idz;
+        int stack[64];
+        int sp = 0;
+        int node = num_refs > 0 ? 0 : -0x7fffffff;
+        bool done = num_refs <= 0;
+        while (!done) {
+            if (node >= 0) {
+                ++n_nodes;
+                const float* f = nodes[node].f;
+                auto slab = [&](float b, float id, float ood) { return std::fmaf(b, id, -ood); };
+                const float c0lox = slab(f[0], idx, oodx), c0hix = slab(f[1], idx, oodx);
+                const float c0loy = slab(f[2], idy, oody), c0hiy = slab(f[3], idy, oody);
+                const float c0loz = slab(f[8], idz, oodz), c0hiz = slab(f[9], idz, oodz);
+                const float c1lox = slab(f[4], idx, oodx), c1hix = slab(f[5], idx, oodx);
+                const float c1loy = slab(f[6], idy, oody), c1hiy = slab(f[7], idy, oody);
+                const float c1loz = slab(f[10], idz, oodz), c1hiz = slab(f[11], idz, oodz);
+                const float c0min = std::max(std::max(std::min(c0lox, c0hix), std::min(c0loy, c0hiy)),
+                                             std::max(std::min(c0loz, c0hiz), tmin));
+                const float c0max = std::min(std::min(std::max(c0lox, c0hix), std::max(c0loy, c0hiy)),
+                                             std::min(std::max(c0loz, c0hiz), hit_t));
+                const float c1min = std::max(std::max(std::min(c1lox, c1hix), std::min(c1loy, c1hiy)),
+                                             std::max(std::min(c1loz, c1hiz), tmin));
+                const float c1max = std::min(std::min(std::max(c1lox, c1hix), std::max(c1loy, c1hiy)),
+                                             std::min(std::max(c1loz, c1hiz), hit_t));
+                const bool t0 = c0max >= c0min, t1 = c1max >= c1min;
+                const int c0 = nodes[node].c0, c1 = nodes[node].c1;
+                if (!t0 && !t1) {
+                    if (sp == 0) { done = true; continue; }
+                    node = stack[--sp];
+                } else {
+                    node = t0 ? c0 : c1;
+                    if (t0 && t1) {
+                        int far = c1;
+                        if (c1min < c0min) { node = c1; far = c0; }
+                        if (sp < 64) stack[sp++] = far;
+                    }
+                }
+            } else {
+                const bin_node& lf = nodes[~node];
+                for (int tri = lf.c0; tri < lf.c1; ++tri) {
+                    ++n_tris;
+                    const float* v0 = woop4 + 12 * (int64_t)tri;
+                    const float* v1 = v0 + 4;
+                    const float* v2 = v0 + 8;
+                    const float Oz = std::fmaf(-oz, v0[2], std::fmaf(-oy, v0[1], std::fmaf(-ox, v0[0], v0[3])));
+                    const float den = std::fmaf(dz, v0[2], std::fmaf(dy, v0[1], dx * v0[0]));
+                    const float t = Oz * (1.0f / den);
+                    bool closer = t < hit_t;
+                    if (!closer && t == hit_t && hit >= 0) closer = tri_idx[tri] < tri_idx[hit];
+                    if (t > tmin && closer) {
+                        const float Ox = std::fmaf(oz, v1[2], std::fmaf(oy, v1[1], std::fmaf(ox, v1[0], v1[3])));
+                        const float Dx = std::fmaf(dz, v1[2], std::fmaf(dy, v1[1], dx * v1[0]));
+                        const float u = std::fmaf(t, Dx, Ox);
+                        if (u >= 0.0f) {
+                            const float Oy = std::fmaf(oz, v2[2], std::fmaf(oy, v2[1], std::fmaf(ox, v2[0], v2[3])));
+                            const float Dy = std::fmaf(dz, v2[2], std::fmaf(dy, v2[1], dx * v2[0]));
+                            const float v = std::fmaf(t, Dy, Oy);
+                            if (v >= 0.0f && u + v <= 1.0f) {
+                                hit_t = t; hit = tri; hit_u = u; hit_v = v;
+                                if (any_hit) break;
+                            }
+                        }
+                    }
+                }
+                if (any_hit && hit >= 0) break;
+                if (sp == 0) break;
+                node = stack[--sp];
+            }
+        }
+        int32_t* res = results + 4 * ri;
+        if (hit < 0) {
+            res[0] = -1;
+            std::memcpy(&res[1], &hit_t, 4);
+            if (stats) { stats[2 * ri] = 0; stats[2 * ri + 1] = 0; }
+        } else {
+            res[0] = tri_idx[hit];
+            std::memcpy(&res[1], &hit_t, 4);
+            std::memcpy(&res[2], &hit_u, 4);
+            std::memcpy(&res[3], &hit_v, 4);
+            if (stats) { stats[2 * ri] = n_nodes; stats[2 * ri + 1] = n_tris; }
+        }
+    }
+}
+
+// Double-precision intersection of one ray with one triangle, in the
+// reference's barycentric convention (u weights v0, v weights v1). Returns 1
+// on a hit with t > tmin.
+int or_intersect64(const double* v0, const double* v1, const double* v2, const double* o, const double* d,
+                   double tmin, double* tuv) {
+    double a[3], b[3], c[3], rhs[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = v0[k] - v2[k];
+        b[k] = v1[k] - v2[k];
+        c[k] = -d[k];
+        rhs[k] = o[k] - v2[k];
+    }
+    auto cross = [](const double* x, const double* y, double* r) {
+        r[0] = x[1] * y[2] - x[2] * y[1];
+        r[1] = x[2] * y[0] - x[0] * y[2];
+        r[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    double bc[3], ca[3], ab[3];
+    cross(b, c, bc); cross(c, a, ca); cross(a, b, ab);
+    double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+    if (det == 0.0) return 0;
+    double u = (rhs[0] * bc[0] + rhs[1] * bc[1] + rhs[2] * bc[2]) / det;
+    double v = (rhs[0] * ca[0] + rhs[1] * ca[1] + rhs[2] * ca[2]) / det;
+    double t = (rhs[0] * ab[0] + rhs[1] * ab[1] + rhs[2] * ab[2]) / det;
+    tuv[0] = t; tuv[1] = u; tuv[2] = v;
+    return (t > tmin && u >= 0.0 && v >= 0.0 && u + v <= 1.0) ? 1 : 0;
+}
+
+// Brute-force closest hit in double precision (small cases): results as
+// (triangle id, t, u, v) in doubles; id -1 on a miss. Ties go to the lower id.
+void or_brute64(const float* verts, const int32_t* tris, int64_t n, const float* rays, int64_t num_rays,
+                double* out) {
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t ri = 0; ri < num_rays; ++ri) {
+        const float* ry = rays + 8 * ri;
+        double o[3] = {ry[0], ry[1], ry[2]}, d[3] = {ry[4], ry[5], ry[6]};
+        double best_t = ry[7], bu = 0, bv = 0;
+        int64_t best = -1;
+        for (int64_t i = 0; i < n; ++i) {
+            double p[3][3];
+            for (int k = 0; k < 3; ++k)
+                for (int a = 0; a < 3; ++a) p[k][a] = verts[3 * (int64_t)tris[3 * i + k] + a];
+            double tuv[3];
+            if (or_intersect64(p[0], p[1], p[2], o, d, ry[3], tuv) && tuv[0] < best_t) {
+                best_t = tuv[0]; bu = tuv[1]; bv = tuv[2]; best = i;
+            }
+        }
+        out[4 * ri] = (double)best;
+        out[4 * ri + 1] = best_t;
+        out[4 * ri + 2] = bu;
+        out[4 * ri + 3] = bv;
+    }
+}
+
+// Adjoint in double precision: dL/dvertices of sum_r (g_t t + g_u u + g_v v) for
+// the hit triangles of `results` (ids), with (t, u, v) recomputed in double.
+void or_adjoint64(const float* verts, const int32_t* tris, const float* rays, const int32_t* results,
+                  const float* dl, int64_t num_rays, double* dverts) {
+    for (int64_t ri = 0; ri < num_rays; ++ri) {
+        const int tri = results[4 * ri];
+        if (tri < 0) continue;
+        const float* ry = rays + 8 * ri;
+        double p[3][3];
+        int vid[3];
+        for (int k = 0; k < 3; ++k) {
+            vid[k] = tris[3 * (int64_t)tri + k];
+            for (int a = 0; a < 3; ++a) p[k][a] = verts[3 * (int64_t)vid[k] + a];
+        }
+        double a[3], b[3], c[3], rhs[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = p[0][k] - p[2][k]; b[k] = p[1][k] - p[2][k]; c[k] = -(double)ry[4 + k];
+            rhs[k] = (double)ry[k] - p[2][k];
+        }
+        auto cross = [](const double* x, const double* y, double* r) {
+            r[0] = x[1] * y[2] - x[2] * y[1];
+            r[1] = x[2] * y[0] - x[0] * y[2];
+            r[2] = x[0] * y[1] - x[1] * y[0];
+        };
+        double bc[3], ca[3], ab[3];
+        cross(b, c, bc); cross(c, a, ca); cross(a, b, ab);
+        double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+        if (det == 0.0) continue;
+        double u = (rhs[0] * bc[0] + rhs[1] * bc[1] + rhs[2] * bc[2]) / det;
+        double v = (rhs[0] * ca[0] + rhs[1] * ca[1] + rhs[2] * ca[2]) / det;
+        const double gt = dl[3 * ri], gu = dl[3 * ri + 1], gv = dl[3 * ri + 2];
+        double q[3];
+        for (int k = 0; k < 3; ++k) q[k] = (gu * bc[k] + gv * ca[k] + gt * ab[k]) / det;
+        const double w[3] = {u, v, 1.0 - u - v};
+        for (int k = 0; k < 3; ++k)
+            for (int x = 0; x < 3; ++x) dverts[3 * (int64_t)vid[k] + x] -= w[k] * q[x];
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,145 @@
+"""Closest-hit adjoint and refit-only update on a heightfield (sm_100a).
+
+The adjoint is checked against the FP64 closed-form gradient (oracle) and
+against FP64 central finite differences; the refit against boxes recomputed
+from the moved vertices over the same topology.
+"""
+import numpy as np
+import pytest
+import torch
+
+import hippie_b200 as hp
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _scene(nx=64, ny=128, rx=256, ry=512, seed=3):
+    v, t = hp.gen.heightfield(seed, nx, ny)
+    rays = hp.gen.rays_grid_down(seed + 1, rx, ry)
+    return v, t, rays
+
+
+def test_adjoint_vs_fp64(ctx):
+    v, t, rays = _scene()
+    V, T, R = dev(v), dev(t), dev(rays)
+    bvh = ctx.build(V, T, hp.BuildParams(morton_bits=60))
+    res = ctx.trace(bvh, R)
+    rng = np.random.default_rng(0)
+    dl = rng.standard_normal((rays.shape[0], 3)).astype(np.float32)
+    g = ctx.adjoint(V, T, R, res, dev(dl)).cpu().numpy().astype(np.float64)
+    ctx.check()
+    res_np = res.cpu().numpy()
+    assert (res_np[:, 0] >= 0).mean() > 0.99
+    ref = oracle.adjoint64(v, t, rays, res_np, dl)
+    scale = np.abs(ref).max()
+    err = np.abs(g - ref)
+    assert err.max() <= 1e-3 * scale
+    rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+    assert rel < 1e-4
+
+
+def test_adjoint_vs_finite_differences(ctx):
+    v, t, rays = _scene(nx=32, ny=64, rx=128, ry=256, seed=7)
+    V, T, R = dev(v), dev(t), dev(rays)
+    bvh = ctx.build(V, T, hp.BuildParams(morton_bits=60))
+    res = ctx.trace(bvh, R).cpu().numpy()
+    rng = np.random.default_rng(1)
+    dl = rng.standard_normal((rays.shape[0], 3)).astype(np.float32)
+    g = ctx.adjoint(V, T, R, dev(res), dev(dl)).cpu().numpy().astype(np.float64)
+    hit = res[:, 0]
+    # rays per triangle
+    by_tri = {}
+    for r in np.nonzero(hit >= 0)[0]:
+        by_tri.setdefault(int(hit[r]), []).append(int(r))
+    tri_of_vertex = {}
+    for ti, tri in enumerate(t):
+        for k in tri:
+            tri_of_vertex.setdefault(int(k), []).append(ti)
+    h = 1e-5
+    checked = 0
+    interior = [i for i in range(v.shape[0]) if 0 < i % 32 < 31 and 0 < i // 32 < 63]
+    for vid in rng.choice(interior, 200, replace=False):
+        rs = [(r, ti) for ti in tri_of_vertex[int(vid)] for r in by_tri.get(ti, [])]
+        if not rs:
+            continue
+        for axis in range(3):
+            fd = 0.0
+            stable = True
+            for sgn in (+1, -1):
+                vv = v.astype(np.float64).copy()
+                vv[vid, axis] += sgn * h
+                loss = 0.0
+                for r, ti in rs:
+                    p = vv[t[ti]]
+                    ok, tuv = oracle.intersect64(p[0], p[1], p[2], rays[r, :3].astype(np.float64),
+                                                 rays[r, 4:7].astype(np.float64))
+                    if not ok:
+                        stable = False
+                        break
+                    loss += dl[r, 0] * tuv[0] + dl[r, 1] * tuv[1] + dl[r, 2] * tuv[2]
+                if not stable:
+                    break
+                fd += sgn * loss
+            if not stable:
+                continue
+            fd /= 2 * h
+            an = g[vid, axis]
+            assert abs(an - fd) <= 1e-3 * max(abs(fd), 1e-2), (vid, axis, an, fd)
+            checked += 1
+        if checked >= 512:
+            break
+    assert checked >= 100
+
+
+def test_refit_after_vertex_step(ctx):
+    v, t, rays = _scene(nx=64, ny=128, rx=128, ry=256, seed=11)
+    V, T, R = dev(v), dev(t), dev(rays)
+    bvh = ctx.build(V, T, hp.BuildParams(morton_bits=60))
+    before = bvh.download()[0]
+    rng = np.random.default_rng(5)
+    v2 = v.copy()
+    v2[:, 2] += rng.uniform(-0.01, 0.01, v.shape[0]).astype(np.float32)
+    V2 = dev(v2)
+    ctx.refit(bvh, V2, T)
+    ctx.check()
+    nodes, woop, tri = bvh.download()
+    # topology unchanged
+    np.testing.assert_array_equal(nodes[:, 12:], before[:, 12:])
+    # woop equals a fresh woopify of the moved triangles
+    ref_woop = np.zeros_like(woop)
+    oracle.load().or_woopify(tri.shape[0], v2.ctypes.data, t.ctypes.data, tri.ctypes.data, ref_woop.ctypes.data)
+    np.testing.assert_array_equal(woop.view(np.int32), ref_woop.view(np.int32))
+    # every node's child boxes are the exact boxes of the moved geometry below them
+    n_int = bvh.c.num_interior
+    f = nodes[:, :12].view(np.float32)
+
+    def node_box(i):
+        if nodes[i, 14] < 0:
+            b, e = nodes[i, 12], nodes[i, 13]
+            p = v2[t[tri[b:e]]].reshape(-1, 3)
+            return p.min(0), p.max(0)
+        (a0, a1), (b0, b1) = node_box(child(i, 0)), node_box(child(i, 1))
+        return np.minimum(a0, b0), np.maximum(a1, b1)
+
+    def child(i, k):
+        c = nodes[i, 12 + k]
+        return ~c if c < 0 else c
+
+    import sys
+    sys.setrecursionlimit(10000)
+    for i in rng.choice(n_int, 200, replace=False):
+        for k in range(2):
+            mn, mx = node_box(child(i, k))
+            got_mn = np.array([f[i, 4 * k + 0], f[i, 4 * k + 2], f[i, 8 + 2 * k]])
+            got_mx = np.array([f[i, 4 * k + 1], f[i, 4 * k + 3], f[i, 9 + 2 * k]])
+            np.testing.assert_array_equal(got_mn, mn)
+            np.testing.assert_array_equal(got_mx, mx)
+    assert bvh.validate(V2, T)
+    # tracing the refitted BVH equals the oracle on the refitted data
+    got = ctx.trace(bvh, R, results=torch.zeros((rays.shape[0], 4), dtype=torch.int32, device="cuda"))
+    np.testing.assert_array_equal(got.cpu().numpy(), oracle.trace(nodes, woop, tri, rays))
