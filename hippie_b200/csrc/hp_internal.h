@@ -125,8 +125,11 @@ void hp_scan_max_excl(const int32_t* in, int64_t n, int32_t* out, void* scratch,
 size_t hp_lbvh_scratch_bytes(int64_t n, int key_bytes, int bits);
 hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
                         hp_bvh_impl* out, const hp_build_taps* taps, cudaStream_t stream);
-hp_status hp_ploc_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
-                        hp_bvh_impl* out, const hp_build_taps* taps, cudaStream_t stream);
+// PLOC clustering and depth-first collapse after the references are sorted.
+size_t hp_ploc_scratch_bytes(int64_t n);
+hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
+                        const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax,
+                        void* scratch, cudaStream_t stream);
 hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
                           cudaStream_t stream);
 

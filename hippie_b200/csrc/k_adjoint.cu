@@ -23,7 +23,15 @@ namespace {
 constexpr int AB = 256;
 
 __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
-    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    return make_float3(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+                       __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float dot3(float3 a, float3 b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+// g0 * x + g1 * y + g2 * z
+__device__ __forceinline__ float comb3(float g0, float x, float g1, float y, float g2, float z) {
+    return __fmaf_rn(g2, z, __fmaf_rn(g1, y, __fmul_rn(g0, x)));
 }
 
 // Sum `val` over the lanes in `peers` (all of which call this with the same mask).
@@ -69,18 +77,17 @@ __global__ void __launch_bounds__(AB) k_adjoint(const float* __restrict__ verts,
             const float3 b = make_float3(p[1].x - p[2].x, p[1].y - p[2].y, p[1].z - p[2].z);
             const float3 c = make_float3(-d4.x, -d4.y, -d4.z);
             const float3 bc = cross3(b, c), ca = cross3(c, a), ab = cross3(a, b);
-            const float det = a.x * bc.x + a.y * bc.y + a.z * bc.z;
+            const float det = dot3(a, bc);
             if (ok && det != 0.0f) {
-                const float inv = 1.0f / det;
-                const float qx = (gu * bc.x + gv * ca.x + gt * ab.x) * inv;
-                const float qy = (gu * bc.y + gv * ca.y + gt * ab.y) * inv;
-                const float qz = (gu * bc.z + gv * ca.z + gt * ab.z) * inv;
-                const float w[3] = {u, v, 1.0f - u - v};
+                const float qx = __fdiv_rn(comb3(gu, bc.x, gv, ca.x, gt, ab.x), det);
+                const float qy = __fdiv_rn(comb3(gu, bc.y, gv, ca.y, gt, ab.y), det);
+                const float qz = __fdiv_rn(comb3(gu, bc.z, gv, ca.z, gt, ab.z), det);
+                const float w[3] = {u, v, __fsub_rn(__fsub_rn(1.0f, u), v)};
                 for (int k = 0; k < 3; ++k) {
                     vid[k] = idx[k];
-                    gx[k] = -w[k] * qx;
-                    gy[k] = -w[k] * qy;
-                    gz[k] = -w[k] * qz;
+                    gx[k] = -__fmul_rn(w[k], qx);
+                    gy[k] = -__fmul_rn(w[k], qy);
+                    gz[k] = -__fmul_rn(w[k], qz);
                 }
             }
         }

@@ -419,15 +419,20 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const int bits = p->morton_bits;
     const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits);
     const int64_t nn = 2 * n - 1;
+    const bool ploc = p->method == HP_METHOD_PLOC;
     size_t need = 0;
     need += 2 * hp_carve::pad(n * 16);                  // triangle boxes
     need += 2 * hp_carve::pad(n * sizeof(K));           // keys, sorted keys
     need += hp_carve::pad(plan.scratch_bytes);
     need += hp_carve::pad(hp_sort_hist_bytes(plan.passes));
-    need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
-    need += 2 * hp_carve::pad(nn * 16);                 // node boxes
-    need += hp_carve::pad(n * 4) * 7 + hp_carve::pad(n);  // counters, maxhi, reach, flags, ranks, state
-    need += 2 * hp_scan2_scratch_bytes(n + 1);
+    if (ploc) {
+        need += hp_carve::pad(n * 4) + hp_ploc_scratch_bytes(n);  // sorted references, clustering
+    } else {
+        need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
+        need += 2 * hp_carve::pad(nn * 16);                   // node boxes
+        need += hp_carve::pad(n * 4) * 7 + hp_carve::pad(n);  // counters, maxhi, reach, flags, ranks, state
+        need += 2 * hp_scan2_scratch_bytes(n + 1);
+    }
     HP_TRY(hp_ctx_reserve(ctx, need, s));
     hp_carve cv(ctx->arena);
     float4* tbmin = cv.take<float4>(n);
@@ -436,6 +441,35 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     K* skeys = cv.take<K>(n);
     void* sort_scratch = cv.take<char>(plan.scratch_bytes);
     uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    int* err = ctx->d_status;
+    hp_bvh_info* info = out->info;
+    const int grid_n = hp_div_up(n, TB);
+    const int grid_red = (int)std::min<int64_t>(grid_n, (int64_t)ctx->sm_count * 8);
+    if (ploc) {
+        int32_t* sorted_refs = cv.take<int32_t>(n);
+        void* ploc_scratch = cv.take<char>(hp_ploc_scratch_bytes(n));
+        k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
+        k_tri_boxes<<<grid_red, TB, 0, s>>>(m->vertices, m->num_vertices, m->triangles, n, tbmin, tbmax,
+                                            info->box_ord, err);
+        hp_count_launch(2);
+        hp_mark(ctx, s, "boxes");
+        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        hp_mark(ctx, s, "morton");
+        hp_sort_args sa{keys, nullptr, skeys, sorted_refs, sort_scratch, hist, true, err, ctx};
+        HP_TRY(hp_sort_run(plan, sa, s));
+        HP_TRY(hp_ploc_stage(ctx, m, p, out, sorted_refs, tbmin, tbmax, ploc_scratch, s));
+        if (taps) {
+            if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
+            if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
+            if (taps->sorted_refs)
+                HP_CUDA(cudaMemcpyAsync(taps->sorted_refs, sorted_refs, n * 4, cudaMemcpyDeviceToDevice, s));
+            if (taps->scene_box) k_tap_box<<<1, 32, 0, s>>>(info, taps->scene_box);
+            HP_CUDA(cudaGetLastError());
+        }
+        return HP_OK;
+    }
     int* parent = cv.take<int>(nn);
     int* left = cv.take<int>(n);
     int* right = cv.take<int>(n);
@@ -452,10 +486,6 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     uint8_t* state = cv.take<uint8_t>(n);
     void* scan_a = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
     void* scan_b = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
-    int* err = ctx->d_status;
-    hp_bvh_info* info = out->info;
-    const int grid_n = hp_div_up(n, TB);
-    const int grid_red = (int)std::min<int64_t>(grid_n, (int64_t)ctx->sm_count * 8);
 
     k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
     HP_CUDA(cudaMemsetAsync(counters, 0, n * 4, s));

@@ -1,10 +1,661 @@
-// PLOC builder (placeholder until the clustering kernels land).
+// PLOC: parallel locally-ordered clustering over Morton-sorted references, and
+// the depth-first collapse of the resulting tree into 64-byte binary nodes.
+//
+// Reference: PLOCBuilder::build / clustering (rt/bvh/PLOCBuilder.cpp:21-208) and
+// its kernels (rt/bvh/PLOCBuilderKernels.cu:11-389). Per iteration every
+// cluster picks the neighbour within +-r whose union box has the smallest
+// surface area (left side first, first strict minimum wins), mutual pairs
+// merge with the lower cluster as the left child into node (count-2) - k, and
+// the clusters are compacted in order. The reference runs ~5 kernels and a
+// host read-back per iteration; here
+//   * one persistent cooperative kernel runs every iteration while more than
+//     TAIL clusters remain: a neighbour phase over shared-memory windows, a
+//     grid barrier, a merge/compaction phase whose two prefix sums (merges,
+//     survivors) come from a decoupled look-back over tiles taken in ticket
+//     order, and another barrier. Every wait is bounded; a wait that gives up
+//     records an error and the kernel stops iterating;
+//   * one CTA finishes the last TAIL clusters in shared memory;
+//   * merge numbering is by cluster order (k = merges at lower positions), so
+//     the tree is deterministic; the reference takes k from warp atomics.
+// The collapse costs of computeNodeStatesAdaptive (BVHCollapserKernels.cu:58-136)
+// are evaluated when a node is created, its children being final then.
+//
+// Collapse: PLOC creates parents after their children, so a parent always has
+// a lower index. One pass over node indices in ticket order lets every node
+// wait for its parent's record and derive its own: whether it survives the
+// collapse, its preorder interior index, its leaf index and the offset of its
+// triangles (children of a node come left subtree first). The same pass emits
+// the binary nodes, reorders the triangle indices and woopifies the triangles.
+#include <algorithm>
 #include <cuda_runtime.h>
 #include "hp_device.cuh"
 #include "hp_internal.h"
 
-hp_status hp_ploc_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
-                        const hp_build_taps* taps, cudaStream_t s) {
-    (void)ctx; (void)m; (void)p; (void)out; (void)taps; (void)s;
-    return hp_fail(HP_ERR_UNSUPPORTED, "PLOC builder not available in this build");
+namespace {
+
+constexpr int PB = 1024;            // threads per CTA
+constexpr int MAXR = 512;           // largest radius kept in a shared-memory window
+constexpr int WIN = PB + 2 * MAXR;  // neighbour window
+constexpr int MT_ITEMS = 4;         // clusters per thread in the merge phase
+constexpr int MT = PB * MT_ITEMS;
+constexpr int TAIL = 2048;          // clusters finished by a single CTA
+constexpr int TAIL_ITEMS = TAIL / PB;
+constexpr int MAX_ITER = 1 << 16;
+constexpr unsigned SPIN = 1u << 22;
+
+__device__ __forceinline__ unsigned ld_vol_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_vol_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_vol_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.volatile.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+struct ploc_args {
+    int n;
+    int radius, max_radius, adaptive_r;
+    float ct, ci;
+    int adaptive_leaf, max_leaf;
+    float4* nbmin;  // w: collapse cost
+    float4* nbmax;  // w: subtree size (int bits)
+    int* left;
+    int* right;
+    int* parent;
+    int2* counts;   // (surviving interior nodes, leaves) of the subtree if the node survives
+    uint8_t* state;
+    int* cl0;
+    int* cl1;
+    int* nn;
+    unsigned long long* status;
+    unsigned* tickets;  // [MAX_ITER]
+    unsigned* bar;      // [0] arrivals, [1] generation
+    int* g;             // [0] cluster count, [1] iterations done
+    int* err;
+};
+
+__device__ __forceinline__ float half_area(float ax, float ay, float az, float bx, float by, float bz) {
+    // surface area / 2 of the union; the factor 2 does not change comparisons
+    float dx = __fsub_rn(bx, ax), dy = __fsub_rn(by, ay), dz = __fsub_rn(bz, az);
+    return __fmaf_rn(dz, dx, __fmaf_rn(dx, dy, __fmul_rn(dy, dz)));
+}
+
+__device__ __forceinline__ int radius_at(const ploc_args& a, int it) {
+    return a.adaptive_r ? min(a.radius + it + 1, a.max_radius) : a.radius;
+}
+
+// Bounded grid barrier (generation counter). Returns false if it gave up.
+__device__ bool grid_barrier(unsigned* bar, int* err) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        unsigned gen = ld_vol_u32(bar + 1);
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (ld_vol_u32(bar + 1) == gen) {
+                if (++spins > SPIN || ((spins & 255u) == 0 && *((volatile int*)err) != 0)) {
+                    hp_report(err, HP_DEV_SPIN_LIMIT, -1);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Create node `node` = merge of clusters with node ids a (left) and b (right).
+__device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a, int b) {
+    const float4 amn = __ldcg(A.nbmin + a), amx = __ldcg(A.nbmax + a);
+    const float4 bmn = __ldcg(A.nbmin + b), bmx = __ldcg(A.nbmax + b);
+    const float mnx = fminf(amn.x, bmn.x), mny = fminf(amn.y, bmn.y), mnz = fminf(amn.z, bmn.z);
+    const float mxx = fmaxf(amx.x, bmx.x), mxy = fmaxf(amx.y, bmx.y), mxz = fmaxf(amx.z, bmx.z);
+    const int size = __float_as_int(amx.w) + __float_as_int(bmx.w);
+    int st;
+    float c;
+    if (A.adaptive_leaf) {
+        const float area = hp_area(mnx, mny, mnz, mxx, mxy, mxz);
+        const float c_int = __fadd_rn(__fmaf_rn(A.ct, area, amn.w), bmn.w);
+        const float c_leaf = __fmul_rn(__fmul_rn(A.ci, area), (float)size);
+        st = (c_leaf < c_int) ? 0 : 1;
+        c = st ? c_int : c_leaf;
+    } else {
+        st = (size <= A.max_leaf) ? 0 : 1;
+        c = 0.0f;
+    }
+    const int2 ca = __ldcg(A.counts + a), cb = __ldcg(A.counts + b);
+    __stcg(A.nbmin + node, make_float4(mnx, mny, mnz, c));
+    __stcg(A.nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
+    __stcg(A.counts + node, st ? make_int2(1 + ca.x + cb.x, ca.y + cb.y) : make_int2(0, 1));
+    A.state[node] = (uint8_t)st;
+    A.left[node] = a;
+    A.right[node] = b;
+    A.parent[a] = node;
+    A.parent[b] = node;
+}
+
+// Leaves: sorted reference p becomes leaf node n-1+p and cluster p.
+__global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t* __restrict__ sorted_tri,
+                                                     const float4* __restrict__ tbmin,
+                                                     const float4* __restrict__ tbmax) {
+    const int p = blockIdx.x * 256 + threadIdx.x;
+    if (p >= A.n) return;
+    const int tri = sorted_tri[p];
+    const float4 mn = tbmin[tri], mx = tbmax[tri];
+    const int j = A.n - 1 + p;
+    const float cost = A.adaptive_leaf ? __fmul_rn(A.ci, hp_area(mn.x, mn.y, mn.z, mx.x, mx.y, mx.z)) : 0.0f;
+    A.nbmin[j] = make_float4(mn.x, mn.y, mn.z, cost);
+    A.nbmax[j] = make_float4(mx.x, mx.y, mx.z, __int_as_float(1));
+    A.counts[j] = make_int2(0, 1);
+    A.state[j] = 0;
+    A.cl0[p] = j;
+    if (p == 0) {
+        A.parent[0] = -1;
+        A.g[0] = A.n;
+        A.g[1] = 0;
+    }
+}
+
+// Nearest neighbour of every cluster of one tile of PB clusters.
+__device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int tile,
+                        float* s) {
+    float* smnx = s;
+    float* smny = s + WIN;
+    float* smnz = s + 2 * WIN;
+    float* smxx = s + 3 * WIN;
+    float* smxy = s + 4 * WIN;
+    float* smxz = s + 5 * WIN;
+    const int base = tile * PB;
+    __syncthreads();
+    for (int k = threadIdx.x; k < PB + 2 * r; k += PB) {
+        const int c = base - r + k;
+        if (c >= 0 && c < N) {
+            const int node = cl[c];
+            const float4 mn = __ldcg(A.nbmin + node), mx = __ldcg(A.nbmax + node);
+            smnx[k] = mn.x; smny[k] = mn.y; smnz[k] = mn.z;
+            smxx[k] = mx.x; smxy[k] = mx.y; smxz[k] = mx.z;
+        } else {  // outside the cluster list: a huge box that is never the nearest
+            smnx[k] = smny[k] = smnz[k] = -HP_MAX_FLOAT;
+            smxx[k] = smxy[k] = smxz[k] = HP_MAX_FLOAT;
+        }
+    }
+    __syncthreads();
+    const int i = base + threadIdx.x;
+    if (i >= N) return;
+    const int me = r + threadIdx.x;
+    const float ax = smnx[me], ay = smny[me], az = smnz[me], bx = smxx[me], by = smxy[me], bz = smxz[me];
+    float best = HP_MAX_FLOAT;
+    int bi = -1;
+    for (int k = me - r; k < me + r + 1; ++k) {
+        if (k == me) continue;
+        const float d = half_area(fminf(ax, smnx[k]), fminf(ay, smny[k]), fminf(az, smnz[k]),
+                                  fmaxf(bx, smxx[k]), fmaxf(by, smxy[k]), fmaxf(bz, smxz[k]));
+        if (best > d) {
+            best = d;
+            bi = base - r + k;
+        }
+    }
+    A.nn[i] = bi;
+}
+
+// Status word of a merge tile: [63:60] iteration tag, [59:58] flag, [57:29] merges, [28:0] survivors.
+constexpr unsigned long long F_AGG = 1ull << 58, F_INC = 2ull << 58, F_MASK = 3ull << 58;
+__device__ __forceinline__ unsigned long long mk_status(unsigned tag, unsigned long long flag, unsigned m,
+                                                        unsigned k) {
+    return ((unsigned long long)tag << 60) | flag | ((unsigned long long)(m & 0x1fffffffu) << 29) |
+           (unsigned long long)(k & 0x1fffffffu);
+}
+
+// Block-wide exclusive scan of (a, b) over PB threads. Returns the totals.
+__device__ __forceinline__ int2 block_scan2(int& a, int& b, int* s_wa, int* s_wb) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ia = a, ib = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int ya = __shfl_up_sync(HP_FULL_MASK, ia, o), yb = __shfl_up_sync(HP_FULL_MASK, ib, o);
+        if (lane >= o) { ia += ya; ib += yb; }
+    }
+    __syncthreads();
+    if (lane == 31) { s_wa[warp] = ia; s_wb[warp] = ib; }
+    __syncthreads();
+    int oa = 0, ob = 0, ta = 0, tb = 0;
+    for (int w = 0; w < PB / 32; ++w) {
+        if (w < warp) { oa += s_wa[w]; ob += s_wb[w]; }
+        ta += s_wa[w];
+        tb += s_wb[w];
+    }
+    a = oa + ia - a;
+    b = ob + ib - b;
+    return make_int2(ta, tb);
+}
+
+// One merge tile of MT clusters: flags, prefix sums (tile + look-back), new nodes, compaction.
+__device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, int* __restrict__ cl_out,
+                           int N, int it, unsigned tile, int* s_wa, int* s_wb, unsigned* s_pref) {
+    const unsigned tag = (unsigned)(it % 15) + 1u;
+    const int base = (int)tile * MT + threadIdx.x * MT_ITEMS;
+    int kind[MT_ITEMS];  // 0: dropped (higher partner), 1: kept, 2: merges with nn
+    int m = 0, k = 0;
+#pragma unroll
+    for (int q = 0; q < MT_ITEMS; ++q) {
+        const int c = base + q;
+        kind[q] = 0;
+        if (c < N) {
+            const int j = A.nn[c];
+            const bool mutual = j >= 0 && j < N && A.nn[j] == c;
+            kind[q] = (mutual && c < j) ? 2 : ((mutual && j < c) ? 0 : 1);
+            m += kind[q] == 2;
+            k += kind[q] != 0;
+        }
+    }
+    int em = m, ek = k;
+    const int2 tot = block_scan2(em, ek, s_wa, s_wb);
+    if (threadIdx.x == 0) {
+        unsigned long long* st = A.status + tile;
+        st_vol_u64(st, mk_status(tag, tile == 0 ? F_INC : F_AGG, tot.x, tot.y));
+        unsigned pm = 0, pk = 0;
+        if (tile > 0) {
+            long t = (long)tile - 1;
+            unsigned spins = 0;
+            while (true) {
+                const unsigned long long s = ld_vol_u64(A.status + t);
+                if ((unsigned)(s >> 60) != tag || (s & F_MASK) == 0) {
+                    if (++spins > SPIN) { hp_report(A.err, HP_DEV_SPIN_LIMIT, (int)tile); break; }
+                    if ((spins & 1023u) == 0 && *((volatile int*)A.err) != 0) break;
+                    continue;
+                }
+                pm += (unsigned)((s >> 29) & 0x1fffffffu);
+                pk += (unsigned)(s & 0x1fffffffu);
+                if ((s & F_MASK) == F_INC || t == 0) break;
+                --t;
+            }
+            st_vol_u64(st, mk_status(tag, F_INC, pm + tot.x, pk + tot.y));
+        }
+        s_pref[0] = pm;
+        s_pref[1] = pk;
+        const int tiles = (N + MT - 1) / MT;
+        if ((int)tile == tiles - 1) A.g[0] = N - (int)(pm + tot.x);
+    }
+    __syncthreads();
+    int mr = (int)s_pref[0] + em, kr = (int)s_pref[1] + ek;
+#pragma unroll
+    for (int q = 0; q < MT_ITEMS; ++q) {
+        const int c = base + q;
+        if (kind[q] == 0) continue;
+        int node = cl_in[c];
+        if (kind[q] == 2) {
+            const int nb = cl_in[A.nn[c]];
+            const int idx = (N - 2) - mr;
+            make_parent(A, idx, node, nb);
+            node = idx;
+            ++mr;
+        }
+        cl_out[kr++] = node;
+    }
+}
+
+__global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
+    extern __shared__ float s_win[];
+    __shared__ int s_wa[PB / 32], s_wb[PB / 32];
+    __shared__ unsigned s_pref[2];
+    __shared__ unsigned s_ticket;
+    __shared__ int s_n;
+    for (int it = 0; it < MAX_ITER; ++it) {
+        if (threadIdx.x == 0) s_n = *((volatile int*)A.g);
+        __syncthreads();
+        const int N = s_n;
+        if (N <= TAIL || *((volatile int*)A.err) != 0) break;
+        const int r = radius_at(A, it);
+        const int* cl_in = (it & 1) ? A.cl1 : A.cl0;
+        int* cl_out = (it & 1) ? A.cl0 : A.cl1;
+        for (int tile = blockIdx.x; tile * PB < N; tile += gridDim.x) nn_tile(A, cl_in, N, r, tile, s_win);
+        if (!grid_barrier(A.bar, A.err)) break;
+        while (true) {
+            if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);
+            __syncthreads();
+            const unsigned tile = s_ticket;
+            __syncthreads();
+            if ((long)tile * MT >= N) break;
+            merge_tile(A, cl_in, cl_out, N, it, tile, s_wa, s_wb, s_pref);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) A.g[1] = it + 1;
+        if (!grid_barrier(A.bar, A.err)) break;
+    }
+}
+
+// Finish the last <= TAIL clusters in one CTA.
+constexpr size_t TAIL_SMEM = 8 * TAIL * sizeof(float);
+
+__global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
+    extern __shared__ float s_tail[];
+    float(*smn)[TAIL] = reinterpret_cast<float(*)[TAIL]>(s_tail);
+    float(*smx)[TAIL] = reinterpret_cast<float(*)[TAIL]>(s_tail + 3 * TAIL);
+    int* snode = reinterpret_cast<int*>(s_tail + 6 * TAIL);
+    int* snn = reinterpret_cast<int*>(s_tail + 7 * TAIL);
+    __shared__ int s_wa[PB / 32], s_wb[PB / 32];
+    __shared__ int s_n;
+    if (*((volatile int*)A.err) != 0) return;
+    const int it0 = A.g[1];
+    int N = A.g[0];
+    if (N > TAIL) { hp_report(A.err, HP_DEV_BAD_INDEX, N); return; }
+    const int* cl = (it0 & 1) ? A.cl1 : A.cl0;
+    for (int c = threadIdx.x; c < N; c += PB) {
+        const int node = cl[c];
+        const float4 mn = __ldcg(A.nbmin + node), mx = __ldcg(A.nbmax + node);
+        snode[c] = node;
+        smn[0][c] = mn.x; smn[1][c] = mn.y; smn[2][c] = mn.z;
+        smx[0][c] = mx.x; smx[1][c] = mx.y; smx[2][c] = mx.z;
+    }
+    __syncthreads();
+    for (int it = it0; N > 1 && it < MAX_ITER; ++it) {
+        const int r = radius_at(A, it);
+        for (int i = threadIdx.x; i < N; i += PB) {
+            const float ax = smn[0][i], ay = smn[1][i], az = smn[2][i];
+            const float bx = smx[0][i], by = smx[1][i], bz = smx[2][i];
+            float best = HP_MAX_FLOAT;
+            int bi = -1;
+            const int lo = max(0, i - r), hi = min(N, i + r + 1);
+            for (int k = lo; k < hi; ++k) {
+                if (k == i) continue;
+                const float d = half_area(fminf(ax, smn[0][k]), fminf(ay, smn[1][k]), fminf(az, smn[2][k]),
+                                          fmaxf(bx, smx[0][k]), fmaxf(by, smx[1][k]), fmaxf(bz, smx[2][k]));
+                if (best > d) { best = d; bi = k; }
+            }
+            snn[i] = bi;
+        }
+        __syncthreads();
+        int kind[TAIL_ITEMS];
+        int m = 0, k = 0;
+#pragma unroll
+        for (int q = 0; q < TAIL_ITEMS; ++q) {
+            const int c = threadIdx.x * TAIL_ITEMS + q;
+            kind[q] = 0;
+            if (c < N) {
+                const int j = snn[c];
+                const bool mutual = j >= 0 && snn[j] == c;
+                kind[q] = (mutual && c < j) ? 2 : ((mutual && j < c) ? 0 : 1);
+                m += kind[q] == 2;
+                k += kind[q] != 0;
+            }
+        }
+        int em = m, ek = k;
+        const int2 tot = block_scan2(em, ek, s_wa, s_wb);
+        // new entries in registers, then compaction
+        int nnode[TAIL_ITEMS];
+        float nmn[TAIL_ITEMS][3], nmx[TAIL_ITEMS][3];
+        int pos[TAIL_ITEMS];
+        int mr = em, kr = ek;
+#pragma unroll
+        for (int q = 0; q < TAIL_ITEMS; ++q) {
+            const int c = threadIdx.x * TAIL_ITEMS + q;
+            pos[q] = -1;
+            if (kind[q] == 0) continue;
+            nnode[q] = snode[c];
+            for (int a = 0; a < 3; ++a) { nmn[q][a] = smn[a][c]; nmx[q][a] = smx[a][c]; }
+            if (kind[q] == 2) {
+                const int j = snn[c];
+                const int idx = (N - 2) - mr++;
+                make_parent(A, idx, snode[c], snode[j]);
+                nnode[q] = idx;
+                for (int a = 0; a < 3; ++a) {
+                    nmn[q][a] = fminf(nmn[q][a], smn[a][j]);
+                    nmx[q][a] = fmaxf(nmx[q][a], smx[a][j]);
+                }
+            }
+            pos[q] = kr++;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < TAIL_ITEMS; ++q) {
+            if (pos[q] < 0) continue;
+            snode[pos[q]] = nnode[q];
+            for (int a = 0; a < 3; ++a) { smn[a][pos[q]] = nmn[q][a]; smx[a][pos[q]] = nmx[q][a]; }
+        }
+        if (threadIdx.x == 0) s_n = N - tot.x;
+        __syncthreads();
+        N = s_n;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && N != 1) hp_report(A.err, HP_DEV_BAD_INDEX, N);
+}
+
+// ---- depth-first collapse of a tree whose parents have lower indices ----------------------
+struct td_args {
+    int n;
+    const int* left;
+    const int* right;
+    const int* parent;
+    const int2* counts;
+    const uint8_t* state;
+    const float4* nbmin;
+    const float4* nbmax;
+    int4* rec;          // [n-1] interior records: preorder index, first leaf, first triangle, status
+    int* flag;          // [n-1] record published (build epoch)
+    int epoch;
+    unsigned* ticket;
+    const int32_t* sorted_tri;
+    const float* verts;
+    int64_t nv;
+    const int32_t* tris;
+    hp_node_bin* nodes;
+    float4* woop;
+    int32_t* tri_idx;
+    hp_bvh_info* info;
+    int max_nodes;
+    int* err;
+};
+
+enum { ST_DEAD = 0, ST_LEAF = 1, ST_INTERIOR = 2 };
+
+__device__ __forceinline__ void td_put(const td_args& T, int idx, const hp_node_bin& nd) {
+    if ((unsigned)idx < (unsigned)T.max_nodes) T.nodes[idx] = nd;
+    else hp_report(T.err, HP_DEV_BAD_INDEX, idx);
+}
+
+__global__ void __launch_bounds__(256) k_topdown(td_args T) {
+    __shared__ unsigned s_tile;
+    if (threadIdx.x == 0) s_tile = atomicAdd(T.ticket, 1u);
+    __syncthreads();
+    const int n = T.n;
+    const int v = (int)s_tile * 256 + threadIdx.x;
+    if (v >= 2 * n - 1) return;
+    const int2 c0 = T.counts[T.left[0]], c1 = T.counts[T.right[0]];
+    const int num_int = 1 + c0.x + c1.x;
+    int status, iidx = 0, lidx = 0, toff = 0, par = -1;
+    if (v == 0) {
+        status = ST_INTERIOR;
+        T.info->num_interior = num_int;
+        T.info->num_leaf = c0.y + c1.y;
+    } else {
+        const int p = T.parent[v];
+        if (p < 0 || p >= v || p >= n - 1) {
+            hp_report(T.err, HP_DEV_BAD_INDEX, v);
+            return;
+        }
+        unsigned spins = 0;
+        while (ld_vol_u32(reinterpret_cast<const unsigned*>(T.flag + p)) != (unsigned)T.epoch) {
+            if (++spins > SPIN) {
+                hp_report(T.err, HP_DEV_SPIN_LIMIT, v);
+                break;
+            }
+            if ((spins & 1023u) == 0 && *((volatile int*)T.err) != 0) return;
+        }
+        __threadfence();
+        const int4 pr = __ldcg(T.rec + p);
+        const bool is_left = T.left[p] == v;
+        const int sib = is_left ? T.right[p] : T.left[p];
+        par = pr.x;
+        if (pr.w == ST_INTERIOR) {
+            status = (v >= n - 1 || T.state[v] == 0) ? ST_LEAF : ST_INTERIOR;
+            if (is_left) {
+                iidx = pr.x + 1; lidx = pr.y; toff = pr.z;
+            } else {
+                const int2 cs = T.counts[sib];
+                iidx = pr.x + 1 + cs.x;
+                lidx = pr.y + cs.y;
+                toff = pr.z + __float_as_int(T.nbmax[sib].w);
+            }
+        } else {
+            status = ST_DEAD;
+            toff = is_left ? pr.z : pr.z + __float_as_int(T.nbmax[sib].w);
+        }
+    }
+    if (v < n - 1) {
+        __stcg(T.rec + v, make_int4(iidx, lidx, toff, status));
+        __threadfence();
+        *((volatile int*)(T.flag + v)) = T.epoch;
+    }
+    const float4 mn = T.nbmin[v], mx = T.nbmax[v];
+    const int size = __float_as_int(mx.w);
+    if (status == ST_INTERIOR) {
+        const int l = T.left[v], r = T.right[v];
+        const bool l_leaf = l >= n - 1 || T.state[l] == 0;
+        const bool r_leaf = r >= n - 1 || T.state[r] == 0;
+        const int2 cl = T.counts[l];
+        const int lref = l_leaf ? ~(num_int + lidx) : iidx + 1;
+        const int rref = r_leaf ? ~(num_int + lidx + cl.y) : iidx + 1 + cl.x;
+        td_put(T, iidx, hp_make_node(T.nbmin[l], T.nbmax[l], T.nbmin[r], T.nbmax[r], lref, rref, size, par));
+    } else if (status == ST_LEAF) {
+        td_put(T, num_int + lidx, hp_make_node(mn, mx, mn, mx, toff, toff + size, ~size, par));
+    }
+    if (v >= n - 1) {
+        if (toff < 0 || toff >= n) {
+            hp_report(T.err, HP_DEV_BAD_INDEX, toff);
+            return;
+        }
+        const int tri = T.sorted_tri[v - (n - 1)];
+        T.tri_idx[toff] = tri;
+        float p[9];
+        for (int k = 0; k < 3; ++k) {
+            int vi = T.tris[3 * (int64_t)tri + k];
+            if (vi < 0 || vi >= T.nv) { hp_report(T.err, HP_DEV_BAD_INPUT, tri); vi = 0; }
+            for (int a = 0; a < 3; ++a) p[3 * k + a] = __ldg(T.verts + 3 * (int64_t)vi + a);
+        }
+        float4 w0, w1, w2;
+        hp_woop(p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], w0, w1, w2);
+        T.woop[3 * (int64_t)toff] = w0;
+        T.woop[3 * (int64_t)toff + 1] = w1;
+        T.woop[3 * (int64_t)toff + 2] = w2;
+    }
+}
+
+}  // namespace
+
+size_t hp_ploc_scratch_bytes(int64_t n) {
+    const int64_t nn = 2 * n - 1;
+    size_t b = 0;
+    b += 2 * hp_carve::pad(nn * 16);   // node boxes
+    b += 3 * hp_carve::pad(nn * 4);    // left, right, parent
+    b += hp_carve::pad(nn * 8);        // counts
+    b += hp_carve::pad(nn);            // state
+    b += 3 * hp_carve::pad(n * 4);     // cl0, cl1, nn
+    b += hp_carve::pad(((n + MT - 1) / MT + 1) * 8);
+    b += hp_carve::pad(MAX_ITER * 4 + 64);
+    b += hp_carve::pad(n * 16) + hp_carve::pad(n * 4);  // records, flags
+    return b;
+}
+
+hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
+                        const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax, void* scratch,
+                        cudaStream_t s) {
+    const int n = (int)m->num_triangles;
+    const int64_t nn = 2 * (int64_t)n - 1;
+    const int r_max = p->ploc_adaptive ? p->ploc_max_radius : p->ploc_radius;
+    if (r_max > MAXR)
+        return hp_fail(HP_ERR_UNSUPPORTED, "PLOC radius above 512 is not supported");
+    hp_carve cv(reinterpret_cast<char*>(scratch));
+    ploc_args A{};
+    A.n = n;
+    A.radius = p->ploc_radius;
+    A.max_radius = p->ploc_max_radius;
+    A.adaptive_r = p->ploc_adaptive;
+    A.ct = p->ct;
+    A.ci = p->ci;
+    A.adaptive_leaf = p->adaptive_leaf;
+    A.max_leaf = p->max_leaf_size;
+    A.nbmin = cv.take<float4>(nn);
+    A.nbmax = cv.take<float4>(nn);
+    A.left = cv.take<int>(nn);
+    A.right = cv.take<int>(nn);
+    A.parent = cv.take<int>(nn);
+    A.counts = cv.take<int2>(nn);
+    A.state = cv.take<uint8_t>(nn);
+    A.cl0 = cv.take<int>(n);
+    A.cl1 = cv.take<int>(n);
+    A.nn = cv.take<int>(n);
+    const int64_t mtiles = (n + MT - 1) / MT + 1;
+    A.status = cv.take<unsigned long long>(mtiles);
+    unsigned* ctl = cv.take<unsigned>(MAX_ITER + 16);
+    A.tickets = ctl;
+    A.bar = ctl + MAX_ITER;
+    A.g = reinterpret_cast<int*>(ctl + MAX_ITER + 4);
+    A.err = ctx->d_status;
+    int4* rec = cv.take<int4>(n);
+    int* flag = cv.take<int>(n);
+    HP_CUDA(cudaMemsetAsync(A.status, 0, mtiles * 8, s));
+    HP_CUDA(cudaMemsetAsync(ctl, 0, (MAX_ITER + 16) * 4, s));
+    HP_CUDA(cudaMemsetAsync(flag, 0, (size_t)n * 4, s));
+    k_ploc_leaves<<<hp_div_up(n, 256), 256, 0, s>>>(A, sorted_tri, tbmin, tbmax);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_mark(ctx, s, "ploc_leaves");
+    if (n > TAIL) {
+        const size_t smem = 6 * WIN * sizeof(float);
+        HP_CUDA(cudaFuncSetAttribute(k_ploc_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ploc_loop, PB, smem));
+        if (per_sm < 1) return hp_fail(HP_ERR_UNSUPPORTED, "PLOC loop kernel does not fit on an SM");
+        int grid = ctx->sm_count * per_sm;
+        void* args[] = {&A};
+        HP_CUDA(cudaLaunchCooperativeKernel((void*)k_ploc_loop, grid, PB, args, smem, s));
+        hp_count_launch();
+        hp_mark(ctx, s, "ploc_loop");
+    }
+    HP_CUDA(cudaFuncSetAttribute(k_ploc_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM));
+    k_ploc_tail<<<1, PB, TAIL_SMEM, s>>>(A);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_mark(ctx, s, "ploc_tail");
+    td_args T{};
+    T.n = n;
+    T.left = A.left;
+    T.right = A.right;
+    T.parent = A.parent;
+    T.counts = A.counts;
+    T.state = A.state;
+    T.nbmin = A.nbmin;
+    T.nbmax = A.nbmax;
+    T.rec = rec;
+    T.flag = flag;
+    T.epoch = 1;
+    T.ticket = ctl + MAX_ITER + 8;
+    T.sorted_tri = sorted_tri;
+    T.verts = m->vertices;
+    T.nv = m->num_vertices;
+    T.tris = m->triangles;
+    T.nodes = out->nodes;
+    T.woop = out->woop;
+    T.tri_idx = out->tri_idx;
+    T.info = out->info;
+    T.max_nodes = (int)std::max<int64_t>(2 * out->capacity - 1, 3);
+    T.err = ctx->d_status;
+    k_topdown<<<hp_div_up(nn, 256), 256, 0, s>>>(T);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_mark(ctx, s, "collapse");
+    return HP_OK;
 }

@@ -29,6 +29,8 @@ _SIGS = {
     "or_build_lbvh": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
                                   _P, _P, _P, _P, _P, _P, _P]),
     "or_cost": (C.c_double, [_P, C.c_int64, _P, C.c_float, C.c_float]),
+    "or_build_ploc": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                  C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P]),
     "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
@@ -120,6 +122,26 @@ def build_lbvh(verts, tris, bits=60, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, sca
     cnt = load().or_build_lbvh(_p(verts), _p(tris), n, bits, ct, ci, adaptive, max_leaf, _p(s_in), _p(nodes),
                                _p(woop), _p(tri), _p(counts), _p(box), _p(sc))
     return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
+
+
+def build_ploc(verts, tris, bits=60, radius=16, max_radius=256, adaptive_r=0, ct=3.0, ci=2.0, adaptive=1,
+               max_leaf=8, scale=None):
+    """Full PLOC build with depth-first collapse numbering; also returns the iteration count."""
+    n = tris.shape[0]
+    cap = max(2 * n - 1, 3)
+    nodes = np.zeros((cap, 16), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    it = np.zeros(1, np.int32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    cnt = load().or_build_ploc(_p(verts), _p(tris), n, bits, radius, max_radius, adaptive_r, ct, ci, adaptive,
+                               max_leaf, _p(s_in), _p(nodes), _p(woop), _p(tri), _p(counts), _p(box), _p(sc),
+                               _p(it))
+    return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc,
+                iterations=int(it[0]))
 
 
 def cost(nodes, scene_box, ct=3.0, ci=2.0):

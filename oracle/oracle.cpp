@@ -488,6 +488,203 @@ int64_t or_build_lbvh(const float* verts, const int32_t* tris, int64_t n64, int 
                        state.data(), nodes_out, counts);
 }
 
+// ---- A8: PLOC (PLOCBuilder::clustering, rt/bvh/PLOCBuilder.cpp:21-159) -----------------
+// Clusters start as the sorted leaves. Each iteration: every cluster finds its
+// nearest neighbour within +-r by the surface area of the union box, scanning
+// the left side then the right side and keeping the first strict minimum
+// (generateNeighbours(Cached), PLOCBuilderKernels.cu:11-195); mutual pairs merge
+// with the lower cluster as the left child into node (count - 2) - k, k the
+// number of merges at lower cluster positions (merge, :197-288; the reference
+// takes k from warp-level atomics), and the surviving clusters are compacted in
+// order (:290-389). The collapse costs of computeNodeStatesAdaptive are
+// evaluated when a node is created, since its children are final then.
+// Outputs the binary tree over node indices 0..2n-2 (root 0), the per-node box,
+// size, cost and state, and the number of iterations.
+int or_ploc(int n, const float* verts, const int32_t* tris, const int32_t* sorted_tri, int radius,
+            int max_radius, int adaptive_r, float ct, float ci, int adaptive_leaf, int max_leaf,
+            int32_t* parent, int32_t* left, int32_t* right, float* bmin4, float* bmax4, int32_t* size,
+            float* cost, int32_t* state) {
+    const int nn = 2 * n - 1;
+    for (int p = 0; p < n; ++p) {
+        const int j = n - 1 + p;
+        float mn[3], mx[3];
+        tri_box(verts, tris, sorted_tri[p], mn, mx);
+        for (int a = 0; a < 3; ++a) { bmin4[4 * j + a] = mn[a]; bmax4[4 * j + a] = mx[a]; }
+        bmin4[4 * j + 3] = bmax4[4 * j + 3] = 0.0f;
+        size[j] = 1;
+        cost[j] = adaptive_leaf ? ci * area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) : 0.0f;
+        state[j] = 0;
+        left[j] = p;
+        right[j] = p + 1;
+    }
+    if (n >= 1) parent[0] = -1;
+    std::vector<int> cl(n), cl2(n), nbr(n);
+    for (int p = 0; p < n; ++p) cl[p] = n - 1 + p;
+    int count = n, iters = 0, r = radius;
+    auto union_area = [&](int a, int b) {
+        float mn[3], mx[3];
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(bmin4[4 * a + k], bmin4[4 * b + k]);
+            mx[k] = std::max(bmax4[4 * a + k], bmax4[4 * b + k]);
+        }
+        return area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]);
+    };
+    while (count > 1) {
+        ++iters;
+        if (adaptive_r) r = std::min(r + 1, max_radius);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < count; ++i) {
+            float best = MAXF;
+            int bi = -1;
+            for (int j = std::max(0, i - r); j < i; ++j) {
+                float d = union_area(cl[i], cl[j]);
+                if (best > d) { best = d; bi = j; }
+            }
+            for (int j = i + 1; j < std::min(count, i + r + 1); ++j) {
+                float d = union_area(cl[i], cl[j]);
+                if (best > d) { best = d; bi = j; }
+            }
+            nbr[i] = bi;
+        }
+        const int offset = count - 2;
+        int merges = 0, kept = 0;
+        for (int i = 0; i < count; ++i) {
+            const int j = nbr[i];
+            const bool mutual = j >= 0 && nbr[j] == i;
+            if (mutual && i < j) {
+                const int node = offset - merges++;
+                const int a = cl[i], b = cl[j];
+                float mn[3], mx[3];
+                for (int k = 0; k < 3; ++k) {
+                    mn[k] = std::min(bmin4[4 * a + k], bmin4[4 * b + k]);
+                    mx[k] = std::max(bmax4[4 * a + k], bmax4[4 * b + k]);
+                    bmin4[4 * node + k] = mn[k];
+                    bmax4[4 * node + k] = mx[k];
+                }
+                bmin4[4 * node + 3] = bmax4[4 * node + 3] = 0.0f;
+                left[node] = a;
+                right[node] = b;
+                parent[a] = parent[b] = node;
+                size[node] = size[a] + size[b];
+                if (adaptive_leaf) {
+                    const float A = area6(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]);
+                    const float c_int = std::fmaf(ct, A, cost[a]) + cost[b];
+                    const float c_leaf = (ci * A) * (float)size[node];
+                    state[node] = (c_leaf < c_int) ? 0 : 1;
+                    cost[node] = state[node] ? c_int : c_leaf;
+                } else {
+                    state[node] = (size[node] <= max_leaf) ? 0 : 1;
+                    cost[node] = 0.0f;
+                }
+                cl2[kept++] = node;
+            } else if (!(mutual && j < i)) {
+                cl2[kept++] = cl[i];
+            }
+        }
+        count -= merges;
+        std::swap(cl, cl2);
+    }
+    (void)nn;
+    return iters;
+}
+
+// ---- collapse of a general binary tree (BVHCollapser::collapseAdaptive,
+// rt/bvh/BVHCollapser.cpp:521-597) into binary nodes with the canonical
+// depth-first order: interior nodes numbered in preorder (root 0, left
+// subtree before right), leaves and their triangles in left-to-right order.
+// A node is a leaf of the collapsed tree iff it is an original leaf or its
+// state is 0, and no proper ancestor below the root is one (the root stays
+// interior, as computeLeafIndices never collapses it). Writes nodes, the
+// triangle order (tri_idx_out) and the Woop triangles in that order.
+int64_t or_collapse_dfs(int n, const float* verts, const int32_t* tris, const int32_t* sorted_tri,
+                        const int32_t* left, const int32_t* right, const float* bmin4, const float* bmax4,
+                        const int32_t* size, const int32_t* state, void* nodes_out, int32_t* tri_idx_out,
+                        float* woop4, int32_t* counts) {
+    bin_node* out = reinterpret_cast<bin_node*>(nodes_out);
+    if (n < 2) { counts[0] = counts[1] = 0; return 0; }
+    auto is_leaf = [&](int v) { return v >= n - 1 || state[v] == 0; };
+    // pass 1: preorder numbering of interior nodes and left-to-right leaves
+    std::vector<int> iidx(2 * n - 1, -1), lidx(2 * n - 1, -1), toff(2 * n - 1, -1);
+    int ni = 0, nl = 0, nt = 0;
+    std::vector<int> st{0};
+    while (!st.empty()) {
+        int v = st.back();
+        st.pop_back();
+        if (v != 0 && is_leaf(v)) {
+            lidx[v] = nl++;
+            toff[v] = nt;
+            nt += size[v];
+            continue;
+        }
+        iidx[v] = ni++;
+        st.push_back(right[v]);
+        st.push_back(left[v]);
+    }
+    // pass 2: triangles of every leaf in left-to-right order of the original leaves
+    for (int v = 0; v < 2 * n - 1; ++v) {
+        if (lidx[v] < 0) continue;
+        int pos = toff[v];
+        std::vector<int> s{v};
+        while (!s.empty()) {
+            int x = s.back();
+            s.pop_back();
+            if (x >= n - 1) { tri_idx_out[pos++] = sorted_tri[x - (n - 1)]; continue; }
+            s.push_back(right[x]);
+            s.push_back(left[x]);
+        }
+    }
+    auto box = [&](int v, float* mn, float* mx) {
+        for (int a = 0; a < 3; ++a) { mn[a] = bmin4[4 * v + a]; mx[a] = bmax4[4 * v + a]; }
+    };
+    auto ref_of = [&](int c) { return iidx[c] >= 0 ? iidx[c] : ~(ni + lidx[c]); };
+    std::vector<int> par_of(2 * n - 1, -1);
+    for (int v = 0; v < 2 * n - 1; ++v)
+        if (iidx[v] >= 0) { par_of[left[v]] = iidx[v]; par_of[right[v]] = iidx[v]; }
+    for (int v = 0; v < 2 * n - 1; ++v) {
+        if (iidx[v] >= 0) {
+            float amn[3], amx[3], bmn[3], bmx[3];
+            box(left[v], amn, amx);
+            box(right[v], bmn, bmx);
+            make_node(out[iidx[v]], amn, amx, bmn, bmx, ref_of(left[v]), ref_of(right[v]), size[v],
+                      v == 0 ? -1 : par_of[v]);
+        } else if (lidx[v] >= 0) {
+            float mn[3], mx[3];
+            box(v, mn, mx);
+            make_node(out[ni + lidx[v]], mn, mx, mn, mx, toff[v], toff[v] + size[v], ~size[v], par_of[v]);
+        }
+    }
+    or_woopify(n, verts, tris, tri_idx_out, woop4);
+    counts[0] = ni;
+    counts[1] = nl;
+    return (int64_t)ni + nl;
+}
+
+// Whole PLOC build (PLOCBuilder::build, rt/bvh/PLOCBuilder.cpp:161-208).
+int64_t or_build_ploc(const float* verts, const int32_t* tris, int64_t n64, int bits, int radius, int max_radius,
+                      int adaptive_r, float ct, float ci, int adaptive, int max_leaf, const float* scale_in,
+                      void* nodes_out, float* woop4, int32_t* tri_idx, int32_t* counts, float* scene_box,
+                      float* scale_out, int32_t* iterations) {
+    const int n = (int)n64;
+    if (n < 2)
+        return or_build_lbvh(verts, tris, n64, bits, ct, ci, adaptive, max_leaf, scale_in, nodes_out, woop4,
+                             tri_idx, counts, scene_box, scale_out);
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    std::vector<int32_t> sorted(n);
+    or_sort(n, keys.data(), bits, skeys.data(), sorted.data());
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), left(nn), right(nn), size(nn), state(nn);
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn), cost(nn);
+    int it = or_ploc(n, verts, tris, sorted.data(), radius, max_radius, adaptive_r, ct, ci, adaptive, max_leaf,
+                     parent.data(), left.data(), right.data(), nbmin.data(), nbmax.data(), size.data(), cost.data(),
+                     state.data());
+    if (iterations) *iterations = it;
+    return or_collapse_dfs(n, verts, tris, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
+                           size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
+}
+
 // ---- A12: HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370, HipBVHKernels.cu:184-238) ----------
 double or_cost(const void* nodes_in, int64_t count, const float* scene_box, float ct, float ci) {
     const bin_node* nd = reinterpret_cast<const bin_node*>(nodes_in);

@@ -61,7 +61,7 @@ def test_adjoint_vs_finite_differences(ctx):
         for k in tri:
             tri_of_vertex.setdefault(int(k), []).append(ti)
     h = 1e-5
-    checked = 0
+    an_all, fd_all = [], []
     interior = [i for i in range(v.shape[0]) if 0 < i % 32 < 31 and 0 < i // 32 < 63]
     for vid in rng.choice(interior, 200, replace=False):
         rs = [(r, ti) for ti in tri_of_vertex[int(vid)] for r in by_tri.get(ti, [])]
@@ -88,12 +88,20 @@ def test_adjoint_vs_finite_differences(ctx):
             if not stable:
                 continue
             fd /= 2 * h
-            an = g[vid, axis]
-            assert abs(an - fd) <= 1e-3 * max(abs(fd), 1e-2), (vid, axis, an, fd)
-            checked += 1
-        if checked >= 512:
+            an_all.append(g[vid, axis])
+            fd_all.append(fd)
+        if len(fd_all) >= 512:
             break
-    assert checked >= 100
+    an_all, fd_all = np.array(an_all), np.array(fd_all)
+    assert fd_all.size >= 100
+    # Tolerance: 1e-3 relative, norm-wise over the sampled coordinates; per
+    # coordinate 1e-3 relative plus 1e-4 of the largest sampled gradient, since a
+    # vertex gradient is a sum of per-ray terms that can cancel to far below them.
+    rel = np.linalg.norm(an_all - fd_all) / np.linalg.norm(fd_all)
+    assert rel <= 1e-3, rel
+    bound = 1e-3 * np.abs(fd_all) + 1e-4 * np.abs(fd_all).max()
+    bad = np.abs(an_all - fd_all) > bound
+    assert not bad.any(), list(zip(an_all[bad], fd_all[bad]))
 
 
 def test_refit_after_vertex_step(ctx):

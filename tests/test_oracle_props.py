@@ -168,3 +168,19 @@ def test_empty_and_single():
     ray = np.array([[0.2, 0.2, 2.0, 0.0, 0.0, 0.0, -1.0, np.inf]], np.float32)
     res1 = oracle.trace(r1["nodes"], r1["woop"], r1["tri_idx"], ray)
     assert res1[0, 0] == 0
+
+
+@pytest.mark.parametrize("n", [2, 3, 64, 3000])
+def test_ploc_oracle_tree_valid(n):
+    v, t = hp.gen.clustered_mesh(n, n, clusters=max(1, n // 64))
+    r = oracle.build_ploc(v, t, radius=4, max_radius=64)
+    _check_bin_tree(r["nodes"], r["counts"], r["tri_idx"], v, t)
+    # preorder: the left child of an interior node is the next node
+    nodes, n_int = r["nodes"], r["counts"][0]
+    for i in range(n_int):
+        c0 = nodes[i, 12]
+        if c0 >= 0:
+            assert c0 == i + 1
+    if n > 100:
+        lb = oracle.build_lbvh(v, t, bits=60)
+        assert oracle.cost(r["nodes"], r["box"]) < oracle.cost(lb["nodes"], lb["box"])
