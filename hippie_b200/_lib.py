@@ -70,6 +70,7 @@ _SIGS = {
     "hp_trace": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, _P]),
     "hp_trace_adjoint": (C.c_int, [_P, C.POINTER(hp_mesh), _P, _P, _P, C.c_int64, _P, _P]),
     "hp_radix_sort": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P]),
+    "hp_radix_sort_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "hp_env_create": (C.c_int, [C.POINTER(C.c_void_p)]),
     "hp_env_destroy": (C.c_int, [_P]),
     "hp_env_read_file": (C.c_int, [_P, C.c_char_p]),

@@ -15,6 +15,8 @@
 // The result equals a stable sort by key: ties keep their input order, so
 // with values 0..n-1 ties are ordered by original index, as in the reference.
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <cuda_runtime.h>
 #include "hp_device.cuh"
 #include "hp_internal.h"
@@ -450,4 +452,71 @@ void hp_scan_max_excl(const int32_t* in, int64_t n, int32_t* out, void* scratch,
     k_scan_lb<true><<<(unsigned)tiles, SCAN_BLOCK, 0, stream>>>(in, n, nullptr, 0, out, nullptr,
                                                                 nullptr, st, counter, tiles, status);
     hp_count_launch();
+}
+
+// ---- sort without allocation --------------------------------------------------------------
+// Callers that may not allocate device memory (a plugin whose host application
+// owns the GPU memory budget, or a loop where cudaMalloc's implicit device
+// synchronisation is not acceptable) get the same sort with its scratch in
+// this file-scope device array. Host code never names the array as a pointer:
+// the symbol is a host-side stand-in, so its device address is looked up once
+// per device with cudaGetSymbolAddress and then passed to the kernels.
+namespace {
+
+constexpr size_t noalloc_pad(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t noalloc_sort_scratch(int64_t n, size_t key_bytes, int tile, int passes) {
+    return 2 * (noalloc_pad((size_t)n * key_bytes) + noalloc_pad((size_t)n * 4)) +
+           noalloc_pad(((size_t)passes * (size_t)((n + tile - 1) / tile) * 256 + 64) * 4);
+}
+constexpr size_t noalloc_max(size_t a, size_t b) { return a > b ? a : b; }
+// Largest sort scratch over both key widths, plus the digit histograms and an error word.
+constexpr size_t NOALLOC_BYTES =
+    noalloc_max(noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 8, 512 * 8, 8),
+                noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 4, 512 * 12, 4)) +
+    noalloc_pad(8 * 256 * 4) + 256;
+
+__device__ __align__(256) unsigned char g_noalloc_sort_scratch[NOALLOC_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
+
+}  // namespace
+
+extern "C" hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* vals_in, void* keys_out,
+                                           int32_t* vals_out, int64_t n, int32_t key_bytes, int32_t bits,
+                                           int32_t* device_status, void* stream) {
+    if (key_bytes != 4 && key_bytes != 8)
+        return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: key_bytes must be 4 or 8");
+    if (bits < 1 || bits > 8 * key_bytes) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: bits out of range");
+    if (n < 0) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: negative n");
+    if (n > HP_NOALLOC_SORT_MAX_KEYS)
+        return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: n = " + std::to_string(n) +
+                                       " exceeds the fixed scratch capacity of " +
+                                       std::to_string(HP_NOALLOC_SORT_MAX_KEYS) + " keys");
+    if (n == 0) return HP_OK;
+    if (!keys_in || !keys_out || !vals_out) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: null buffer");
+    int dev = 0;
+    HP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: device id too large");
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+            if (e != cudaSuccess) return hp_cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_sort_scratch)");
+            g_noalloc_base[dev] = p;
+        }
+        base = g_noalloc_base[dev];
+    }
+    const hp_sort_plan plan = hp_sort_make_plan(n, key_bytes, bits);
+    hp_carve cv(reinterpret_cast<char*>(base));
+    void* scratch = cv.take<char>(plan.scratch_bytes);
+    uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    int* own_status = cv.take<int>(64);
+    if (cv.off > NOALLOC_BYTES) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: scratch plan exceeds the fixed array");
+    hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false,
+                   device_status ? reinterpret_cast<int*>(device_status) : own_status, nullptr};
+    return hp_sort_run(plan, a, reinterpret_cast<cudaStream_t>(stream));
 }

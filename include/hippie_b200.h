@@ -197,6 +197,27 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
                         void* keys_out, int32_t* vals_out, int64_t n,
                         int32_t key_bytes, int32_t bits, void* stream);
 
+/* The same sort for callers that must not allocate GPU memory: no context, no
+ * cudaMalloc / cudaFree / allocating library call. This entry point has no
+ * counterpart in the reference. It serves code that runs where the device
+ * memory budget is owned by someone else (a plugin inside a host
+ * application that hands it only fixed buffers) or where an allocation's
+ * implicit device synchronisation is not allowed (a latency-critical frame
+ * loop). Its scratch is a fixed array in the library's device memory, loaded
+ * once on every GPU that uses the library and kept until the process exits:
+ * at most HP_NOALLOC_SORT_MAX_KEYS keys per call, larger n returns HP_ERR_ARG.
+ * The first call on a device looks up that array's device address, so make
+ * the first call on each device before any stream capture. All calls share
+ * the one array: calls whose GPU work overlaps (different streams, or
+ * several host threads) race; serialise them on one stream. Every call clears
+ * the scratch state it needs. device_status (optional, device memory, one
+ * int32) receives a nonzero code if a bounded wait inside the sort gave up. */
+#define HP_NOALLOC_SORT_MAX_KEYS 262144
+hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* vals_in,
+                                void* keys_out, int32_t* vals_out, int64_t n,
+                                int32_t key_bytes, int32_t bits, int32_t* device_status,
+                                void* stream);
+
 /* ---- environment files (Environment / AppEnvironment) ------------------- */
 typedef struct hp_env hp_env;
 hp_status hp_env_create(hp_env** out);      /* registers the reference's options */
