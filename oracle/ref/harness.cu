@@ -4,7 +4,6 @@
 // The sequences restate, without Qt or HIP, the reference host code:
 //   LBVHBuilder::build          rt/bvh/LBVHBuilder.cpp:183-241
 //   PLOCBuilder::clustering     rt/bvh/PLOCBuilder.cpp:21-159, build :161-208
-//   RadixSort::sort/dispatch    radix_sort/RadixSort.cpp:29-238
 //   BVHCollapser::collapseAdaptive + computeNodeOffsets loop
 //                               rt/bvh/BVHCollapser.cpp:14-306,521-597
 //   HipBVH::woopifyTriangles    rt/bvh/HipBVH.cpp:95-116
@@ -12,12 +11,15 @@
 //   HipTracer::trace            rt/tracer/HipTracer.cpp:13-52
 // Each kernel is timed like HipKernel::launchTimed (gpu/HipKernel.cpp:296-325):
 // synchronise, event, launch, event, synchronise; the build time is the sum.
-// One deliberate difference: PLOC never writes nodeParentIndices[0]
-// (the root's parent) and the collapser reads it; the harness sets it to -1.
+// Deliberate differences: PLOC never writes nodeParentIndices[0] (the root's
+// parent) and the collapser reads it, so the harness sets it to -1; and the
+// sort step uses CUB's stable radix sort instead of the reference's radix sort
+// kernels (see the note at the sort below).
 #include <algorithm>
 #include <cstdio>
 #include <vector>
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 #include "hpref.h"
 
 namespace {
@@ -45,72 +47,31 @@ template <typename T> T* dalloc(size_t count) {
     return p;
 }
 
+char g_err[512] = "";
+int fail(int code, const char* where) {
+    cudaError_t e = cudaGetLastError();
+    std::snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+    return code;
+}
+
 #define ROUND_UP(x, y) ((((x) + (y) - 1) / (y)) * (y))
 
-// RadixSort::getMaxGridSize for compute capability >= 3.0 with the reference's
-// policy constants (radix_sort/RadixSortPolicy.h).
-int max_grid_size(int sm_count) {
-    int regs = 0, smem = 0;
-    hpref_sort_attrs(&regs, &smem);
-    const int warp_threads = 32, max_sm_blocks = 16, max_sm_warps = 2048 / 32, max_sm_regs = 64 * 1024;
-    const int warp_alloc_unit = 4, smem_alloc_unit = 256, reg_alloc_unit = 256, smem_bytes = 48 * 1024,
-              subscription = 5;
-    const int block_warps = (128 + warp_threads - 1) / warp_threads;
-    const int max_warp_occ = max_sm_warps / block_warps;
-    const int regs_per_side = max_sm_regs / warp_alloc_unit;
-    const int regs_per_warp = ROUND_UP(regs * warp_threads, reg_alloc_unit);
-    const int warps = (regs_per_side / regs_per_warp) * warp_alloc_unit;
-    const int max_reg_occ = warps / block_warps;
-    const int block_smem = ROUND_UP(smem, smem_alloc_unit);
-    const int max_smem_occ = block_smem > 0 ? smem_bytes / block_smem : max_sm_blocks;
-    const int occ = std::min(std::min(max_sm_blocks, max_warp_occ), std::min(max_smem_occ, max_reg_occ));
-    return occ * sm_count * subscription;
-}
-
-// RadixSort::dispatch: passes of `radix` bits over [begin_bit, end_bit).
-void dispatch(timer& T, unsigned long long* k1, unsigned long long* k2, int* v1, int* v2, int* spine, bool& swap,
-              int n, int spine_size, int begin_bit, int end_bit, bool alt, int max_grid) {
-    const int tile = 128 * 7;
-    const int total_grains = (n + tile - 1) / tile;
-    const int grid = std::min(total_grains, max_grid);
-    const int grains_per_block = total_grains / grid;
-    const int big_blocks = total_grains - grains_per_block * grid;
-    const int normal_share = grains_per_block * tile;
-    const int normal_base = big_blocks * tile;
-    const int big_share = normal_share + tile;
-    for (int bit = begin_bit; bit < end_bit; bit += alt ? 4 : 5) {
-        unsigned long long* kin = swap ? k2 : k1;
-        unsigned long long* kout = swap ? k1 : k2;
-        int* vin = swap ? v2 : v1;
-        int* vout = swap ? v1 : v2;
-        T.run([&] { hpref_upsweep(grid, n, bit, big_blocks, big_share, normal_share, normal_base, total_grains, kin,
-                                  spine, alt); });
-        T.run([&] { hpref_scan(spine_size, spine); });
-        T.run([&] { hpref_downsweep(grid, bit, n, big_blocks, big_share, normal_share, normal_base, total_grains,
-                                    spine, kin, kout, vin, vout, alt); });
-        swap = !swap;
-    }
-}
-
-// RadixSort::sort over [0, bits).
-void ref_sort(timer& T, unsigned long long* k1, unsigned long long* k2, int* v1, int* v2, bool& swap, int n,
-              int bits, int sm_count) {
-    const int max_grid = max_grid_size(sm_count);
-    const int scan_tile = 1024 * 4;
-    const int spine_size = max_grid * 32 + scan_tile;
-    const int alt_spine_size = max_grid * 16 + scan_tile;
-    int* spine = dalloc<int>(std::max(spine_size, alt_spine_size));
-    swap = false;
-    int begin_bit = 0;
-    const int rem = bits % 5;
-    if (rem != 0) {
-        const int max_alt = 5 - rem;
-        const int alt_end = std::min(bits, begin_bit + max_alt * 4);
-        dispatch(T, k1, k2, v1, v2, spine, swap, n, alt_spine_size, begin_bit, alt_end, true, max_grid);
-        begin_bit = alt_end;
-    }
-    dispatch(T, k1, k2, v1, v2, spine, swap, n, spine_size, begin_bit, bits, false, max_grid);
-    cudaFree(spine);
+// Host check of a binary tree over nodes 0..2n-2 (root 0, leaves n-1..):
+// every interior node's children are in range, name it as parent, and every
+// node but the root is a child exactly once. The collapse kernels climb these
+// links, so they only run on a tree that passes.
+bool valid_tree(int n, const int* parent, const int* left, const int* right) {
+    const int nn = 2 * n - 1;
+    std::vector<int> hp(nn), hl(nn), hr(nn), uses(nn, 0);
+    if (cudaMemcpy(hp.data(), parent, nn * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hl.data(), left, nn * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hr.data(), right, nn * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    if (hp[0] != -1) return false;
+    for (int i = 0; i < n - 1; ++i)
+        for (int c : {hl[i], hr[i]})
+            if (c <= 0 || c >= nn || hp[c] != i || uses[c]++) return false;
+    return true;
 }
 
 // BVHCollapser::collapseAdaptive (Bin layout).
@@ -155,6 +116,8 @@ void ref_collapse(timer& T, int n, int* parent, int* left, int* right, float4* n
 
 extern "C" {
 
+const char* hpref_last_error(void) { return g_err; }
+
 // Build a BVH with the reference's kernels. method 0 = LBVH, 1 = PLOC.
 // Device inputs: verts, tris. Device outputs: nodes (64 B x (2n-1)), woop
 // (48 B x n), tri_idx (n). Optional device taps (null to skip): morton keys
@@ -175,9 +138,8 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     timer T;
     float4* rbmin = dalloc<float4>(n);
     float4* rbmax = dalloc<float4>(n);
-    // The reference sort ranks keys with pre-Volta warp-synchronous scans. Its
-    // buffers are padded so that a mis-rank can only land in owned memory, and
-    // its output is checked to be a permutation before anything reads it.
+    // Sort buffers are padded, and the sorted order is checked on the host
+    // before any kernel indexes memory with it.
     const size_t pad_n = 3 * (size_t)n + 65536;
     unsigned long long* keys0 = dalloc<unsigned long long>(pad_n);
     unsigned long long* keys1 = dalloc<unsigned long long>(pad_n);
@@ -195,18 +157,39 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     hpref_set_scene_box(scene_box);
     T.run([&] { hpref_morton60(n, bits, keys0, refs0, rbmin, rbmax); });
     if (tap_keys) cudaMemcpy(tap_keys, keys0, n * 8, cudaMemcpyDeviceToDevice);
-    bool swap = false;
-    ref_sort(T, keys0, keys1, refs0, refs1, swap, n, bits, sm);
-    if (swap) {  // the reference copies buffer 1 over buffer 0
-        cudaMemcpy(keys0, keys1, n * 8, cudaMemcpyDeviceToDevice);
-        cudaMemcpy(refs0, refs1, n * 4, cudaMemcpyDeviceToDevice);
-    }
+    std::vector<unsigned long long> unsorted(n);
+    if (cudaMemcpy(unsorted.data(), keys0, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(7, "after setupBoxes / computeMortonCodes60");
+    // The reference's own radix sort kernels (radix_sort/RadixSortKernels.cu)
+    // rank keys with pre-Volta warp-synchronous shared-memory scans; on this
+    // GPU they failed for a 3000-key input, so they are not run. Their output is
+    // by definition the stable sort of (key, index) pairs; CUB's stable radix
+    // sort produces it (timed like every other kernel).
     {
+        size_t temp_bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys0, keys1, refs0, refs1, n, 0, bits);
+        void* temp = nullptr;
+        if (cudaMalloc(&temp, std::max<size_t>(temp_bytes, 1)) != cudaSuccess) return fail(5, "sort temp");
+        T.run([&] { cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys0, keys1, refs0, refs1, n, 0, bits); });
+        cudaFree(temp);
+        if (cudaMemcpy(keys0, keys1, n * 8, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+            cudaMemcpy(refs0, refs1, n * 4, cudaMemcpyDeviceToDevice) != cudaSuccess)
+            return fail(6, "after sort");
+    }
+    (void)sm;
+    {
+        // The later kernels index memory with this output: check that it is the
+        // stable sort of the keys before any of them runs.
         std::vector<int> h(n), seen(n, 0);
-        cudaMemcpy(h.data(), refs0, n * 4, cudaMemcpyDeviceToHost);
+        std::vector<unsigned long long> hk(n);
+        if (cudaMemcpy(h.data(), refs0, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(hk.data(), keys0, n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(8, "reading the sorted keys");
         for (int i = 0; i < n; ++i) {
-            if (h[i] < 0 || h[i] >= n || seen[h[i]]++) {
-                std::fprintf(stderr, "reference sort output is not a permutation (position %d)\n", i);
+            bool ok = h[i] >= 0 && h[i] < n && !seen[h[i]]++ && hk[i] == unsorted[h[i]];
+            if (ok && i > 0) ok = hk[i - 1] < hk[i] || (hk[i - 1] == hk[i] && h[i - 1] < h[i]);
+            if (!ok) {
+                std::fprintf(stderr, "reference sort output is not the stable sort of its keys (position %d)\n", i);
                 return 3;
             }
         }
@@ -217,6 +200,10 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     int iters = 0;
     if (method == 0) {
         T.run([&] { hpref_construct60(n, parent, left, right, keys0); });
+        if (!valid_tree(n, parent, left, right)) {
+            std::fprintf(stderr, "reference construct60 produced an invalid tree\n");
+            return 4;
+        }
         int* counters = dalloc<int>(n);
         cudaMemset(counters, 0, n * 4);
         T.run([&] { hpref_refit(nn, counters, parent, left, right, nbmin, nbmax); });
@@ -248,6 +235,10 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
             if (merged == 0) break;  // would never terminate
         }
         cudaFree(dist); cudaFree(nbr); cudaFree(block_off);
+        if (clusters != 1 || !valid_tree(n, parent, left, right)) {
+            std::fprintf(stderr, "reference PLOC clustering produced an invalid tree\n");
+            return 4;
+        }
     }
     if (tap_parent) cudaMemcpy(tap_parent, parent, nn * 4, cudaMemcpyDeviceToDevice);
     if (tap_left) cudaMemcpy(tap_left, left, nn * 4, cudaMemcpyDeviceToDevice);
@@ -257,6 +248,7 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     ref_collapse(T, n, parent, left, right, nbmin, nbmax, tri1, tri0, nodes, ct, ci, counts);
     T.run([&] { hpref_woopify(n, tri0, tris, verts, woop); });
     cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) fail(2, "after the collapse / woopify");
     cudaFree(rbmin); cudaFree(rbmax); cudaFree(keys0); cudaFree(keys1); cudaFree(refs0); cudaFree(refs1);
     cudaFree(tri1); cudaFree(parent); cudaFree(left); cudaFree(right); cudaFree(nbmin); cudaFree(nbmax);
     *seconds = T.total;

@@ -16,15 +16,6 @@ void hpref_setup_leaves(int n, int* refs0, int* refs1, int* tri0, int* tri1, int
 void hpref_construct60(int n, int* parent, int* left, int* right, unsigned long long* keys);
 void hpref_refit(int nodes, int* counters, int* parent, int* left, int* right, float4* nbmin, float4* nbmax);
 
-// w_sort.cu
-void hpref_sort_attrs(int* regs, int* smem);
-void hpref_upsweep(int grid, int n, int bit, int big_blocks, int big_share, int normal_share, int normal_base,
-                   int total_grains, unsigned long long* keys, int* spine, bool alt);
-void hpref_scan(int bins, int* spine);
-void hpref_downsweep(int grid, int bit, int n, int big_blocks, int big_share, int normal_share, int normal_base,
-                     int total_grains, int* spine, unsigned long long* kin, unsigned long long* kout, int* vin,
-                     int* vout, bool alt);
-
 // w_ploc.cu
 void hpref_ploc_neighbours(int clusters, int r, float* dist, int* nbr, float4* nbmin, float4* nbmax, int* nodes);
 void hpref_ploc_merge(int clusters, int offset, int* nbr, int* in, int* out, int* parent, int* left, int* right,

@@ -31,6 +31,8 @@ def load():
                                     C.POINTER(C.c_double), _P]
         lib.hpref_trace.restype = C.c_int
         lib.hpref_trace.argtypes = [_P, _P, _P, _P, C.c_int, _P, C.c_int, C.POINTER(C.c_double)]
+        lib.hpref_last_error.restype = C.c_char_p
+        lib.hpref_last_error.argtypes = []
         lib.hpref_bvh_cost.restype = C.c_float
         lib.hpref_bvh_cost.argtypes = [_P, C.c_int, C.c_float, C.c_float, C.c_float]
         _lib = lib
@@ -68,7 +70,7 @@ def build(V, T, scene_box, method="lbvh", bits=60, radius=16, max_radius=256, ad
                             _p(tp.get("bmin")), _p(tp.get("bmax")), counts.ctypes.data, C.byref(secs),
                             iters.ctypes.data)
     if rc != 0:
-        raise RuntimeError(f"reference build failed ({rc})")
+        raise RuntimeError(f"reference build failed ({rc}): {load().hpref_last_error().decode()}")
     cnt = int(counts.sum())
     out = dict(nodes=nodes[:cnt].cpu().numpy(), woop=woop.cpu().numpy(), tri_idx=tri.cpu().numpy(),
                counts=counts, seconds=secs.value, iterations=int(iters[0]))
