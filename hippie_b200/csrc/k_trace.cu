@@ -10,10 +10,11 @@
 // Differences by design:
 //   * the traversal stack is split: its first 16 entries live in shared memory
 //     (bank-conflict-free, one column per thread), deeper entries in local memory;
-//   * every lane handles its leaves as soon as it reaches them (no speculative
-//     postponing), so the sequence of node and triangle tests of a ray does not
-//     depend on the other lanes of its warp; with the explicit fma / IEEE
-//     reciprocal arithmetic below a CPU restatement reproduces every result bit;
+//   * every floating-point step is written out (fma, IEEE reciprocal), so a CPU
+//     restatement of the per-ray algorithm reproduces the results bit for bit;
+//     the first leaf a lane meets is postponed as in the reference, which can
+//     change the order in which a ray tests its leaves but not its closest hit
+//     unless two candidate hits lie within rounding of a node's slab distance;
 //   * closest-hit ties in t are resolved to the lower triangle id.
 #include <cuda_runtime.h>
 #include "hp_device.cuh"
@@ -36,6 +37,13 @@ struct ray_state {
     int nodes, tris;
 };
 
+// One 32-byte read-only load (sm_100 vector width); p must be 32-byte aligned.
+__device__ __forceinline__ void ld32(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
+}
+
 __device__ __forceinline__ float safe_rcp(float d) {
     // idir = 1 / (|d| > 2^-80 ? d : copysign(2^-80, d)) (HipTracerBinKernels.cu:83-86)
     const float ooeps = 8.2718061255302767e-25f;  // 2^-80
@@ -57,6 +65,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
     ray_state r;
     int64_t ray = -1;
     int node = SENTINEL;
+    int leaf = 0;   // postponed leaf (~index), >= 0 when none
     int sp = 0;
     int steps = 0;  // node + leaf visits of the current ray (bounded)
     bool exhausted = false;
@@ -86,6 +95,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
                     r.nodes = r.tris = 0;
                     sp = 0;
                     steps = 0;
+                    leaf = 0;
                     node = 0;
                 } else {
                     exhausted = true;
@@ -94,18 +104,26 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
         }
         if (__all_sync(HP_FULL_MASK, node == SENTINEL)) break;
 
-        while (node != SENTINEL) {
-            // Interior nodes until this lane reaches a leaf or finishes.
+        // Traverse until fewer than FETCH_THRESHOLD lanes of the warp still hold
+        // a ray; the warp reconverges after every round so that the decision
+        // (and the refill that follows) is taken by all 32 lanes together.
+        while (true) {
+          if (node != SENTINEL) {
+            // Interior nodes. The first leaf a lane reaches is postponed and the
+            // lane keeps traversing until every lane still traversing holds a
+            // leaf (or finishes); then the leaves are tested together.
             while ((unsigned)node < (unsigned)SENTINEL) {
                 if (node >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
                     hp_report(err, HP_DEV_BAD_INDEX, node);
                     node = SENTINEL;
+                    leaf = 0;
                     break;
                 }
                 if (STATS) ++r.nodes;
                 const float4* np = nodes + 4 * (int64_t)node;
-                const float4 n0 = __ldg(np), n1 = __ldg(np + 1), nz = __ldg(np + 2);
-                const float4 nm = __ldg(np + 3);
+                float4 n0, n1, nz, nm;
+                ld32(np, n0, n1);
+                ld32(np + 2, nz, nm);
                 const float c0lox = __fmaf_rn(n0.x, r.idx_, -r.oodx);
                 const float c0hix = __fmaf_rn(n0.y, r.idx_, -r.oodx);
                 const float c0loy = __fmaf_rn(n0.z, r.idy, -r.oody);
@@ -142,15 +160,22 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
                         ++sp;
                     }
                 }
+                if (node < 0 && leaf >= 0) {  // postpone the first leaf
+                    leaf = node;
+                    if (sp == 0) node = SENTINEL;
+                    else { --sp; node = sp < SSTACK ? sstack[sp * TRACE_BLOCK] : lstack[sp - SSTACK]; }
+                }
+                if (!__any_sync(__activemask(), leaf >= 0)) break;
             }
-            // Leaves: test every triangle, then continue with the stack.
-            while (node < 0) {
-                if (~node >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
-                    hp_report(err, HP_DEV_BAD_INDEX, node);
+            // Leaves: the postponed one, then `node` if it is a leaf too.
+            while (leaf < 0) {
+                if (~leaf >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
+                    hp_report(err, HP_DEV_BAD_INDEX, leaf);
                     node = SENTINEL;
+                    leaf = 0;
                     break;
                 }
-                const float4 lm = __ldg(nodes + 4 * (int64_t)(~node) + 3);
+                const float4 lm = __ldg(nodes + 4 * (int64_t)(~leaf) + 3);
                 int begin = __float_as_int(lm.x), end = __float_as_int(lm.y);
                 if (begin < 0 || end > num_refs || begin > end) {
                     hp_report(err, HP_DEV_BAD_INDEX, begin);
@@ -185,9 +210,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
                         }
                     }
                 }
-                if (ANY_HIT && r.hit >= 0) { node = SENTINEL; break; }
-                if (sp == 0) node = SENTINEL;
-                else { --sp; node = sp < SSTACK ? sstack[sp * TRACE_BLOCK] : lstack[sp - SSTACK]; }
+                if (ANY_HIT && r.hit >= 0) { node = SENTINEL; leaf = 0; break; }
+                leaf = node;
+                if (node < 0) {
+                    if (sp == 0) node = SENTINEL;
+                    else { --sp; node = sp < SSTACK ? sstack[sp * TRACE_BLOCK] : lstack[sp - SSTACK]; }
+                }
             }
             if (node == SENTINEL) {
                 if (r.hit < 0) {
@@ -198,9 +226,10 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
                                              __float_as_int(r.hit_u), __float_as_int(r.hit_v));
                     if (STATS) stats[ray] = make_int2(r.nodes, r.tris);
                 }
-                break;
             }
-            if (__popc(__activemask()) < FETCH_THRESHOLD) break;
+          }
+          __syncwarp();
+          if (__popc(__ballot_sync(HP_FULL_MASK, node != SENTINEL)) < FETCH_THRESHOLD) break;
         }
     }
 }

@@ -40,7 +40,13 @@ def test_trace_bit_exact(ctx, kind, n, n_rays, bits):
     exp, est = oracle.trace(nodes, woop, tri, rays, stats=True)
     got = res.cpu().numpy()
     np.testing.assert_array_equal(got, exp)
-    np.testing.assert_array_equal(st.cpu().numpy(), est)
+    # Counters: postponed leaves make the GPU's visit order depend on the warp,
+    # so node / triangle counts are compared in aggregate, not per ray.
+    gst = st.cpu().numpy()
+    hit = exp[:, 0] >= 0
+    assert np.all(gst[~hit] == 0) and np.all(gst[hit] > 0)
+    for k in range(2):
+        assert abs(gst[hit, k].mean() / est[hit, k].mean() - 1.0) < 0.15
     hits = (got[:, 0] >= 0).mean()
     assert 0.05 < hits < 1.0
     # plain trace (no stats) gives the same results
@@ -74,8 +80,16 @@ def test_any_hit_and_limits(ctx):
     ctx.trace(bvh, R, results=anyh, any_hit=True)
     anyh = anyh.cpu().numpy()
     np.testing.assert_array_equal(anyh[:, 0] >= 0, closest[:, 0] >= 0)
+    # any hit: some intersected triangle, never closer than the closest one
+    h = anyh[:, 0] >= 0
+    assert np.all(anyh[h, 1].view(np.float32) >= closest[h, 1].view(np.float32))
+    bf = oracle.brute64(v, t, rays[h][:2000])
+    for i, row in enumerate(anyh[h][:2000]):
+        p = v[t[row[0]]].astype(np.float64)
+        ok, tuv = oracle.intersect64(p[0], p[1], p[2], rays[h][i, :3], rays[h][i, 4:7])
+        assert ok and abs(tuv[0] - row[1:2].view(np.float32)[0]) <= 1e-4 * max(1.0, tuv[0]), i
+    assert np.all(bf[:, 0] >= 0)
     nodes, woop, tri = bvh.download()
-    np.testing.assert_array_equal(anyh, oracle.trace(nodes, woop, tri, rays, any_hit=True))
     # tmin / tmax windows
     r2 = rays.copy()
     r2[:, 3] = 0.3
