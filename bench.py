@@ -155,32 +155,66 @@ def committed_traffic(name):
     return None
 
 
+def oracle_build(cfg, v, t):
+    """The CPU restatement of the workload's builder (LBVH or PLOC, same parameters)."""
+    import oracle
+    if cfg["method"] == "ploc":
+        return oracle.build_ploc(v, t, bits=cfg["bits"], radius=16, max_radius=256)
+    return oracle.build_lbvh(v, t, bits=cfg["bits"])
+
+
+def cpu_sample(cfg, v, t, budget_s):
+    """Largest prefix of the mesh whose oracle build fits about budget_s seconds."""
+    n = cfg["n"]
+    m = min(n, 131072)
+    t0 = time.perf_counter()
+    oracle_build(cfg, v, np.ascontiguousarray(t[:m]))
+    dt = time.perf_counter() - t0
+    return int(min(n, max(m, m * budget_s / max(dt, 1e-4))))
+
+
 def cpu_baseline(cfg, v, t, rays, budget_s=20.0):
     """Time the CPU restatement (oracle) on a bounded sample of the workload."""
     import oracle
     oracle.load()
     cores = os.cpu_count() or 1
-    n = cfg["n"]
-    m = min(n, 262144)
+    m = cpu_sample(cfg, v, t, 0.4 * budget_s)
     tt = np.ascontiguousarray(t[:m])
     t0 = time.perf_counter()
-    r = oracle.build_lbvh(v, tt, bits=cfg["bits"])
+    r = oracle_build(cfg, v, tt)
     b_s = time.perf_counter() - t0
-    # scale the sample so build + trace fit the budget
-    m2 = int(min(n, m * max(1.0, 0.5 * budget_s / max(b_s, 1e-3))))
-    if m2 > m:
-        tt = np.ascontiguousarray(t[:m2])
-        t0 = time.perf_counter()
-        r = oracle.build_lbvh(v, tt, bits=cfg["bits"])
-        b_s = time.perf_counter() - t0
-        m = m2
     k = min(rays.shape[0], 1 << 18)
     t0 = time.perf_counter()
     oracle.trace(r["nodes"], r["woop"], r["tri_idx"], rays[:k])
     tr_s = time.perf_counter() - t0
     return {"value": m / b_s / 1e6, "unit": "Mtris/s", "cores": cores, "kind": "port",
-            "sample": f"LBVH build of the first {m} triangles; trace of {k} rays on that BVH",
+            "sample": f"{cfg['method'].upper()} build of the first {m} triangles; trace of {k} rays on that BVH",
             "trace_mrays_s": k / tr_s / 1e6}
+
+
+def reference_kernels(cfg, V, T, R, v, reps=3):
+    """The reference's own CUDA kernels (oracle/_ref, built from its sources) on the
+    same device inputs: summed kernel time of the build and the tracer's rate.
+    Reported beside the product's numbers; None where the harness was not built."""
+    import oracle.ref_harness as rh
+    if not rh.available():
+        return None
+    import torch
+    box = np.concatenate([v.min(0), v.max(0)]).astype(np.float32)
+    kw = dict(method=cfg["method"], bits=cfg["bits"])
+    if cfg["method"] == "ploc":
+        kw.update(radius=16, max_radius=256)
+    builds = [rh.build(V, T, box, **kw) for _ in range(reps)]
+    b = builds[-1]
+    nodes = torch.from_numpy(b["nodes"]).cuda()
+    woop = torch.from_numpy(b["woop"]).cuda()
+    tri = torch.from_numpy(b["tri_idx"]).cuda()
+    secs = [rh.trace(nodes, woop, tri, R)[1] for _ in range(reps)]
+    n, nr = T.shape[0], R.shape[0]
+    bs = float(np.median([x["seconds"] for x in builds]))
+    return {"build_ms": 1e3 * bs, "mtris_s": n / bs / 1e6, "trace_mrays_s": nr / float(np.median(secs)) / 1e6,
+            "note": "reference kernels compiled from its sources for sm_100a; CUB radix sort in place of its "
+                    "own sort; times are sums of per-kernel CUDA events as the reference reports them"}
 
 
 def run_reference(args, cfg, rank):
@@ -192,18 +226,13 @@ def run_reference(args, cfg, rank):
     oracle.load()
     steps, warmup = args.steps, args.warmup
     budget = 150.0 / max(1, steps + warmup)
-    n = cfg["n"]
-    m = min(n, 131072)
-    t0 = time.perf_counter()
-    oracle.build_lbvh(v, np.ascontiguousarray(t[:m]), bits=cfg["bits"])
-    dt = time.perf_counter() - t0
-    m = int(min(n, max(m, m * 0.6 * budget / max(dt, 1e-4))))
+    m = cpu_sample(cfg, v, t, 0.6 * budget)
     tm = np.ascontiguousarray(t[:m])
     k = min(rays.shape[0], 1 << 17)
     bt, tt = [], []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
-        r = oracle.build_lbvh(v, tm, bits=cfg["bits"])
+        r = oracle_build(cfg, v, tm)
         t1 = time.perf_counter()
         oracle.trace(r["nodes"], r["woop"], r["tri_idx"], rays[:k])
         t2 = time.perf_counter()
@@ -234,9 +263,16 @@ def main(argv=None):
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--once", action="store_true",
+                    help="one build and one trace, then print the phase times (for profiler runs)")
+    ap.add_argument("--rays", type=int, default=0, help="override the workload's ray count (profiling)")
+    ap.add_argument("--reference-kernels", type=int, default=1,
+                    help="also time the reference's own CUDA kernels where they were built (1 GPU)")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.rays:
+        cfg["rays"] = args.rays
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
@@ -264,6 +300,15 @@ def main(argv=None):
     params = build_params(cfg)
     bvh = ctx.build(V, T, params)
     stream = torch.cuda.current_stream()
+    if args.once:
+        ctx.trace(bvh, R, results=RES)
+        bvh.sync()
+        ctx.check()
+        print(json.dumps({"once": cfg["workload"], "rays": nr, "interior": bvh.c.num_interior,
+                          "leaves": bvh.c.num_leaf}), flush=True)
+        del bvh
+        ctx.close()
+        return 0
 
     def barrier():
         if world > 1:
@@ -378,6 +423,8 @@ def main(argv=None):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, v, t, rays)
+    if rank == 0 and world == 1 and args.reference_kernels:
+        line["reference_kernels_gpu"] = reference_kernels(cfg, V, T, R, v)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del bvh

@@ -54,7 +54,8 @@ class Env:
         check(load().hp_env_create(C.byref(self.h)))
 
     def __del__(self):
-        if getattr(self, "h", None):
+        # At interpreter shutdown module globals may already be gone.
+        if getattr(self, "h", None) and load is not None:
             load().hp_env_destroy(self.h)
             self.h = None
 
@@ -100,7 +101,7 @@ class BVH:
         self.c = hp_bvh()
 
     def __del__(self):
-        if getattr(self, "c", None) is not None and self.c.impl:
+        if getattr(self, "c", None) is not None and self.c.impl and load is not None and C is not None:
             load().hp_bvh_free(self.ctx.h, C.byref(self.c))
 
     def sync(self, stream=None):
@@ -151,7 +152,7 @@ class Context:
         self.device = device
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and load is not None:
             load().hp_ctx_destroy(self.h)
             self.h = None
 
