@@ -273,7 +273,6 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
         return HP_OK;
     }
     hp_mark(ctx, s, "begin");
-    if (p->method == HP_METHOD_ATR) return hp_fail(HP_ERR_UNSUPPORTED, "ATR builder not available in this build");
     return hp_lbvh_build(ctx, m, p, b, taps, s);
 }
 

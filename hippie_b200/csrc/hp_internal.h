@@ -130,6 +130,32 @@ size_t hp_ploc_scratch_bytes(int64_t n);
 hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax,
                         void* scratch, cudaStream_t stream);
+// Depth-first collapse of a binary tree (interior nodes 0..n-2, leaves n-1..2n-2,
+// sorted reference p at leaf n-1+p) into 64-byte nodes, the triangle order and
+// Woop triangles. nbmax.w holds each node's size; counts the surviving interior
+// nodes and collapsed leaves of each subtree. order (2n-1) lists the nodes with
+// every parent before its children; null means parents have lower indices.
+struct hp_topdown_in {
+    int n;
+    const int* left;
+    const int* right;
+    const int* parent;
+    const int2* counts;
+    const uint8_t* state;
+    const float4* nbmin;
+    const float4* nbmax;
+    const int* order;
+    const int32_t* sorted_tri;
+};
+size_t hp_topdown_scratch_bytes(int64_t n);
+hp_status hp_topdown_collapse(hp_ctx* ctx, const hp_mesh* m, const hp_topdown_in& in, hp_bvh_impl* out,
+                              void* scratch, cudaStream_t stream);
+// ATR restructuring of a Karras tree and its collapse (method HP_METHOD_ATR).
+size_t hp_atr_scratch_bytes(int64_t n);
+hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out, int n,
+                       const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
+                       float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
+                       cudaStream_t stream);
 hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
                           cudaStream_t stream);
 

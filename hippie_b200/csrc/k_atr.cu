@@ -1,0 +1,492 @@
+// ATR: agglomerative treelet restructuring of the LBVH, then the collapse of the
+// restructured tree into 64-byte binary nodes.
+//
+// Reference: ATRBuilder::build / optimize (rt/bvh/ATRBuilder.cpp:80-236), kernels
+// optimize / optimizeSmall / computeSurfaceAreas (rt/bvh/ATRBuilderKernels.cu:
+// 12-577) and formTreelet (rt/bvh/TRBuilderUtil.h:141-216).
+//
+// One launch per iteration (gamma = treelet size T, doubled after each one):
+// every thread starts at a leaf and climbs; the second thread to reach a node
+// sets refs = refs(l) + refs(r) and cost = ct*A + cost(l) + cost(r) (a leaf
+// costs ci*A), and a node with refs >= gamma is restructured by its warp right
+// away: the treelet grows from the root's children by expanding the treelet
+// leaf of largest area that is not a BVH leaf until it has T leaves, then the
+// leaves are merged agglomeratively, smallest union area first, and the new
+// topology is written back iff its cost is strictly lower. Every node below a
+// treelet root is final when the root is reached, and treelets restructured at
+// the same time are disjoint, so the result does not depend on scheduling; the
+// two warp searches keep the reference's shuffle-reduction order, which fixes
+// how ties are broken.
+//
+// Differences in form, not in result:
+//   * the first iteration also refits the boxes (the reference runs a refit
+//     and a surface-area kernel before it), and areas are recomputed from the
+//     boxes instead of being stored;
+//   * the distance matrix is always in shared memory (up to T = 32);
+//   * the row/column of a packed triangular index is decoded exactly with
+//     integer arithmetic (the reference uses sqrtf);
+//   * refs of restructured treelet nodes are updated too.
+// Areas use the ATR kernels' formula 2*(x*y + x*z + y*z), which the
+// reference's fast-math build contracts to 2*fma(y, z, fma(x, y, x*z)).
+//
+// Collapse. A final climb evaluates computeNodeStatesAdaptive
+// (BVHCollapserKernels.cu:58-136) on the final topology, the per-subtree counts
+// of surviving interior nodes and collapsed leaves, and for every node the
+// smallest sorted position below it (minpos) and how many nodes below it share
+// that minpos (below). Ordering nodes by (minpos, -size) is a preorder in which
+// each node's child holding the smaller position comes first, so parents
+// precede children; its rank is base[minpos] + chain[minpos] - 1 - below with
+// base the exclusive sum of the chain lengths. The depth-first collapse kernel
+// then walks nodes in that order, which lets every node wait for its parent.
+#include <algorithm>
+#include <cuda_runtime.h>
+#include "hp_device.cuh"
+#include "hp_internal.h"
+
+namespace {
+
+constexpr int AB = 128;  // threads per CTA
+constexpr int AW = AB / 32;
+constexpr int TMAX = 32;
+constexpr int DMAX = TMAX * (TMAX - 1) / 2;
+constexpr float MAXF = 3.402823466e+38f;
+
+__device__ __forceinline__ float atr_area(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
+    const float x = __fsub_rn(mxx, mnx), y = __fsub_rn(mxy, mny), z = __fsub_rn(mxz, mnz);
+    return __fmul_rn(2.0f, __fmaf_rn(y, z, __fmaf_rn(x, y, __fmul_rn(x, z))));
+}
+
+__device__ __forceinline__ int tri_index(int row, int col) { return row * (row - 1) / 2 + col; }
+
+__device__ __forceinline__ void tri_decode(int e, int& row, int& col) {
+    int r = (int)((1.0f + sqrtf((float)(8 * e + 1))) * 0.5f);
+    while (r * (r - 1) / 2 > e) --r;
+    while ((r + 1) * r / 2 <= e) ++r;
+    row = r;
+    col = e - r * (r - 1) / 2;
+}
+
+struct atr_args {
+    int n, T, gamma, init;
+    float ct, ci;
+    int* left;
+    int* right;
+    int* parent;
+    float4* nbmin;  // w: ATR cost
+    float4* nbmax;  // w: reference count (int bits)
+    int* counters;
+    const int32_t* sorted_tri;
+    const float4* tbmin;
+    const float4* tbmax;
+    int* err;
+};
+
+struct box6 {
+    float mn[3], mx[3];
+};
+
+__device__ __forceinline__ box6 shfl_box(const box6& b, int src) {
+    box6 o;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        o.mn[a] = __shfl_sync(HP_FULL_MASK, b.mn[a], src);
+        o.mx[a] = __shfl_sync(HP_FULL_MASK, b.mx[a], src);
+    }
+    return o;
+}
+
+__device__ __forceinline__ box6 join(const box6& a, const box6& b) {
+    box6 o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        o.mn[k] = fminf(a.mn[k], b.mn[k]);
+        o.mx[k] = fmaxf(a.mx[k], b.mx[k]);
+    }
+    return o;
+}
+
+__device__ __forceinline__ float area_of(const box6& b) {
+    return atr_area(b.mn[0], b.mn[1], b.mn[2], b.mx[0], b.mx[1], b.mx[2]);
+}
+
+__device__ __forceinline__ void load_node(const atr_args& A, int v, box6& b, float& cost, int& refs) {
+    const float4 mn = __ldcg(A.nbmin + v), mx = __ldcg(A.nbmax + v);
+    b.mn[0] = mn.x; b.mn[1] = mn.y; b.mn[2] = mn.z;
+    b.mx[0] = mx.x; b.mx[1] = mx.y; b.mx[2] = mx.z;
+    cost = mn.w;
+    refs = __float_as_int(mx.w);
+}
+
+__device__ __forceinline__ bool interior_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(A.n - 1); }
+__device__ __forceinline__ bool node_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(2 * A.n - 1); }
+
+// Restructure the treelet rooted at `root` (whole warp, converged). root_cost
+// is the cost the climb just computed for the root.
+__device__ void atr_treelet(const atr_args& A, int root, float root_cost, float* sd) {
+    const int lane = threadIdx.x & 31;
+    const int T = A.T, n = A.n;
+    // ---- formTreelet: lane k holds treelet leaf k (node, area) and internal node k
+    const int l0 = __ldcg(A.left + root), r0 = __ldcg(A.right + root);
+    int tl = lane == 0 ? l0 : (lane == 1 ? r0 : -1);
+    int ti = lane == 0 ? root : -1;
+    float ta = -MAXF;
+    bool bad = !node_ok(A, l0) || !node_ok(A, r0);
+    if (!bad && lane < 2) {
+        box6 b; float c; int rf;
+        load_node(A, tl, b, c, rf);
+        ta = area_of(b);
+    }
+    for (int it = 0; it < T - 2 && !bad; ++it) {
+        const int m = it + 2;
+        int idx = lane;
+        float a = (lane < m && tl < n - 1) ? ta : -MAXF;
+        // findLeafToExpand: strict '>' keeps the lower lane on ties
+        int cnt = m, sh = cnt / 2;
+        while (cnt > 1) {
+            const int oi = __shfl_down_sync(HP_FULL_MASK, idx, sh);
+            const float oa = __shfl_down_sync(HP_FULL_MASK, a, sh);
+            if (oa > a) { a = oa; idx = oi; }
+            cnt = (cnt + 1) / 2;
+            sh = cnt / 2;
+        }
+        idx = __shfl_sync(HP_FULL_MASK, idx, 0);
+        const int rep = __shfl_sync(HP_FULL_MASK, tl, idx);
+        if (!interior_ok(A, rep)) { bad = true; break; }  // a subtree of >= gamma refs always has one
+        if (lane == it + 1) ti = rep;
+        if (lane == idx || lane == m) {
+            tl = lane == idx ? __ldcg(A.left + rep) : __ldcg(A.right + rep);
+            if (node_ok(A, tl)) {
+                box6 b; float c; int rf;
+                load_node(A, tl, b, c, rf);
+                ta = area_of(b);
+            }
+        }
+        bad = __any_sync(HP_FULL_MASK, (lane == idx || lane == m) && !node_ok(A, tl));
+    }
+    if (bad) {
+        if (lane == 0) hp_report(A.err, HP_DEV_BAD_INDEX, root);
+        return;
+    }
+    // ---- slot state and the distance matrix
+    box6 bx{};
+    float sc = 0.0f;
+    int sr = 0, sn = tl;
+    if (lane < T) load_node(A, tl, bx, sc, sr);
+    const int M = T * (T - 1) / 2;
+    for (int b0 = 0; b0 < M; b0 += 32) {
+        const int e = b0 + lane;
+        int row = 1, col = 0;
+        if (e < M) tri_decode(e, row, col);
+        const box6 br = shfl_box(bx, row), bc = shfl_box(bx, col);
+        if (e < M) sd[e] = area_of(join(br, bc));
+    }
+    __syncwarp();
+    // ---- agglomerative merging; lane k records the internal node made at step k
+    int ol = -1, orr = -1, orf = 0;
+    float oc = 0.0f;
+    box6 ob{};
+    for (int last = T - 1; last >= 1; --last) {
+        const int mm = last * (last + 1) / 2;
+        float best = MAXF;
+        int bi = 0;
+        for (int e = lane; e < mm; e += 32) {
+            const float d = sd[e];
+            if (d < best) { best = d; bi = e; }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float obst = __shfl_down_sync(HP_FULL_MASK, best, off);
+            const int oi = __shfl_down_sync(HP_FULL_MASK, bi, off);
+            if (obst < best) { best = obst; bi = oi; }
+        }
+        bi = __shfl_sync(HP_FULL_MASK, bi, 0);
+        int row, col;
+        tri_decode(bi, row, col);
+        const float c_r = __shfl_sync(HP_FULL_MASK, sc, row), c_c = __shfl_sync(HP_FULL_MASK, sc, col);
+        const int n_r = __shfl_sync(HP_FULL_MASK, sn, row), n_c = __shfl_sync(HP_FULL_MASK, sn, col);
+        const int r_r = __shfl_sync(HP_FULL_MASK, sr, row), r_c = __shfl_sync(HP_FULL_MASK, sr, col);
+        const box6 u = join(shfl_box(bx, row), shfl_box(bx, col));
+        const float uc = __fmaf_rn(A.ct, area_of(u), __fadd_rn(c_r, c_c));
+        const int n_l = __shfl_sync(HP_FULL_MASK, sn, last), r_l = __shfl_sync(HP_FULL_MASK, sr, last);
+        const float c_l = __shfl_sync(HP_FULL_MASK, sc, last);
+        const box6 b_l = shfl_box(bx, last);
+        const int inode = __shfl_sync(HP_FULL_MASK, ti, last - 1);
+        if (lane == last) { ol = n_r; orr = n_c; oc = uc; orf = r_r + r_c; ob = u; }
+        if (lane == col) {
+            sn = inode; sc = uc; sr = r_r + r_c; bx = u;
+        } else if (lane == row) {
+            sn = n_l; sc = c_l; sr = r_l; bx = b_l;
+        }
+        if (last > 1) {
+            float dv = 0.0f;
+            int dst = -1;
+            if (lane < last && lane != row) {
+                dv = sd[tri_index(last, lane)];
+                dst = tri_index(max(row, lane), min(row, lane));
+            }
+            __syncwarp();
+            if (dst >= 0) sd[dst] = dv;
+            __syncwarp();
+            const box6 bc = shfl_box(bx, col);
+            if (lane < last && lane != col) sd[tri_index(max(col, lane), min(col, lane))] = area_of(join(bx, bc));
+            __syncwarp();
+        }
+    }
+    // ---- updateTreelet: keep the new topology iff its cost is strictly lower
+    const float newc = __shfl_sync(HP_FULL_MASK, oc, 1);
+    const int node = __shfl_up_sync(HP_FULL_MASK, ti, 1);
+    if (newc < root_cost && lane >= 1 && lane < T) {
+        __stcg(A.left + node, ol);
+        __stcg(A.right + node, orr);
+        __stcg(A.parent + ol, node);
+        __stcg(A.parent + orr, node);
+        __stcg(A.nbmin + node, make_float4(ob.mn[0], ob.mn[1], ob.mn[2], oc));
+        __stcg(A.nbmax + node, make_float4(ob.mx[0], ob.mx[1], ob.mx[2], __int_as_float(orf)));
+    }
+    __threadfence();
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
+    __shared__ float s_dist[AW][DMAX];
+    const int warp = threadIdx.x >> 5;
+    const int p = blockIdx.x * AB + threadIdx.x;
+    const int n = A.n;
+    int cur = -1;
+    if (p < n) {
+        const int leaf = n - 1 + p;
+        if (A.init) {
+            const int tri = A.sorted_tri[p];
+            if ((unsigned)tri >= (unsigned)n) {
+                hp_report(A.err, HP_DEV_BAD_INDEX, p);
+            } else {
+                const float4 mn = A.tbmin[tri], mx = A.tbmax[tri];
+                const float c = __fmul_rn(A.ci, atr_area(mn.x, mn.y, mn.z, mx.x, mx.y, mx.z));
+                __stcg(A.nbmin + leaf, make_float4(mn.x, mn.y, mn.z, c));
+                __stcg(A.nbmax + leaf, make_float4(mx.x, mx.y, mx.z, __int_as_float(1)));
+            }
+        }
+        cur = __ldcg(A.parent + leaf);
+    }
+    int steps = 0;
+    while (__any_sync(HP_FULL_MASK, cur >= 0)) {
+        if (++steps > n + 1) {  // a valid tree is climbed in at most n - 1 steps
+            if ((threadIdx.x & 31) == 0) hp_report(A.err, HP_DEV_BAD_INDEX, -1);
+            break;
+        }
+        bool arrived = false;
+        int refs = 0;
+        float cost = 0.0f;
+        if (cur >= 0) {
+            if (!interior_ok(A, cur)) {
+                hp_report(A.err, HP_DEV_BAD_INDEX, cur);
+                cur = -1;
+            } else {
+                __threadfence();
+                if (atomicAdd(A.counters + cur, 1) == 0) cur = -1;
+                else arrived = true;
+                __threadfence();
+            }
+        }
+        if (arrived) {
+            const int l = __ldcg(A.left + cur), r = __ldcg(A.right + cur);
+            if (!node_ok(A, l) || !node_ok(A, r)) {
+                hp_report(A.err, HP_DEV_BAD_INDEX, cur);
+                arrived = false;
+                cur = -1;
+            } else {
+                box6 bl, br;
+                float cl, cr;
+                int rl, rr;
+                load_node(A, l, bl, cl, rl);
+                load_node(A, r, br, cr, rr);
+                const box6 u = join(bl, br);
+                refs = rl + rr;
+                cost = __fadd_rn(__fmaf_rn(A.ct, area_of(u), cl), cr);
+                __stcg(A.nbmin + cur, make_float4(u.mn[0], u.mn[1], u.mn[2], cost));
+                __stcg(A.nbmax + cur, make_float4(u.mx[0], u.mx[1], u.mx[2], __int_as_float(refs)));
+            }
+        }
+        unsigned vote = __ballot_sync(HP_FULL_MASK, arrived && refs >= A.gamma);
+        while (vote) {
+            const int src = __ffs(vote) - 1;
+            const int root = __shfl_sync(HP_FULL_MASK, cur, src);
+            const float rc = __shfl_sync(HP_FULL_MASK, cost, src);
+            atr_treelet(A, root, rc, s_dist[warp]);
+            vote &= vote - 1;
+        }
+        if (cur >= 0) cur = __ldcg(A.parent + cur);
+    }
+}
+
+struct fin_args {
+    int n, init, adaptive, max_leaf;
+    float ct, ci;
+    const int* left;
+    const int* right;
+    const int* parent;
+    float4* nbmin;  // w: collapse cost
+    float4* nbmax;  // w: size (int bits)
+    int* counters;
+    uint8_t* state;
+    int2* counts;   // surviving interior nodes, collapsed leaves
+    int2* key;      // minpos, below
+    int* chain;     // [n]: nodes whose minpos is the index
+    const int32_t* sorted_tri;
+    const float4* tbmin;
+    const float4* tbmax;
+    int* err;
+};
+
+// computeSizes + computeNodeStatesAdaptive / computeNodeStates on the final
+// topology, plus the counts and ordering keys of the collapse.
+__global__ void __launch_bounds__(256) k_atr_finish(fin_args F) {
+    const int p = blockIdx.x * 256 + threadIdx.x;
+    const int n = F.n;
+    if (p >= n) return;
+    const int leaf = n - 1 + p;
+    float4 mn, mx;
+    if (F.init) {
+        const int tri = F.sorted_tri[p];
+        if ((unsigned)tri >= (unsigned)n) { hp_report(F.err, HP_DEV_BAD_INDEX, p); return; }
+        mn = F.tbmin[tri];
+        mx = F.tbmax[tri];
+    } else {
+        mn = __ldcg(F.nbmin + leaf);
+        mx = __ldcg(F.nbmax + leaf);
+    }
+    const float lc = F.adaptive ? __fmul_rn(F.ci, hp_area(mn.x, mn.y, mn.z, mx.x, mx.y, mx.z)) : 0.0f;
+    __stcg(F.nbmin + leaf, make_float4(mn.x, mn.y, mn.z, lc));
+    __stcg(F.nbmax + leaf, make_float4(mx.x, mx.y, mx.z, __int_as_float(1)));
+    F.state[leaf] = 0;
+    __stcg(F.counts + leaf, make_int2(0, 1));
+    __stcg(F.key + leaf, make_int2(p, 0));
+    int node = __ldcg(F.parent + leaf);
+    int guard = 0;
+    while (node >= 0) {
+        if (node >= n - 1 || ++guard > n) {
+            hp_report(F.err, HP_DEV_BAD_INDEX, node);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(F.counters + node, 1) == 0) return;
+        __threadfence();
+        const int l = __ldcg(F.left + node), r = __ldcg(F.right + node);
+        if ((unsigned)l >= (unsigned)(2 * n - 1) || (unsigned)r >= (unsigned)(2 * n - 1)) {
+            hp_report(F.err, HP_DEV_BAD_INDEX, node);
+            return;
+        }
+        const float4 lmn = __ldcg(F.nbmin + l), lmx = __ldcg(F.nbmax + l);
+        const float4 rmn = __ldcg(F.nbmin + r), rmx = __ldcg(F.nbmax + r);
+        const float mnx = fminf(lmn.x, rmn.x), mny = fminf(lmn.y, rmn.y), mnz = fminf(lmn.z, rmn.z);
+        const float mxx = fmaxf(lmx.x, rmx.x), mxy = fmaxf(lmx.y, rmx.y), mxz = fmaxf(lmx.z, rmx.z);
+        const int size = __float_as_int(lmx.w) + __float_as_int(rmx.w);
+        int st;
+        float c;
+        if (F.adaptive) {
+            const float area = hp_area(mnx, mny, mnz, mxx, mxy, mxz);
+            const float c_int = __fadd_rn(__fmaf_rn(F.ct, area, lmn.w), rmn.w);
+            const float c_leaf = __fmul_rn(__fmul_rn(F.ci, area), (float)size);
+            st = (c_leaf < c_int) ? 0 : 1;
+            c = st ? c_int : c_leaf;
+        } else {
+            st = (size <= F.max_leaf) ? 0 : 1;
+            c = 0.0f;
+        }
+        const int2 cl = __ldcg(F.counts + l), cr = __ldcg(F.counts + r);
+        const int2 kl = __ldcg(F.key + l), kr = __ldcg(F.key + r);
+        const bool lmin = kl.x < kr.x;
+        const int2 kmin = lmin ? kl : kr, kother = lmin ? kr : kl;
+        F.chain[kother.x] = kother.y + 1;  // the other child ends its chain
+        __stcg(F.nbmin + node, make_float4(mnx, mny, mnz, c));
+        __stcg(F.nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
+        F.state[node] = (uint8_t)st;
+        __stcg(F.counts + node, st ? make_int2(1 + cl.x + cr.x, cl.y + cr.y) : make_int2(0, 1));
+        __stcg(F.key + node, make_int2(kmin.x, kmin.y + 1));
+        if (node == 0) F.chain[kmin.x] = kmin.y + 2;
+        node = __ldcg(F.parent + node);
+    }
+}
+
+// order[rank(v)] = v with rank(v) = base[minpos] + chain[minpos] - 1 - below.
+__global__ void __launch_bounds__(256) k_atr_order(int n, const int2* __restrict__ key,
+                                                   const int* __restrict__ chain, const int* __restrict__ base,
+                                                   int* order, int* err) {
+    const int v = blockIdx.x * 256 + threadIdx.x;
+    if (v >= 2 * n - 1) return;
+    const int2 k = key[v];
+    if ((unsigned)k.x >= (unsigned)n) { hp_report(err, HP_DEV_BAD_INDEX, v); return; }
+    const int r = base[k.x] + chain[k.x] - 1 - k.y;
+    if ((unsigned)r >= (unsigned)(2 * n - 1) || k.y >= chain[k.x]) { hp_report(err, HP_DEV_BAD_INDEX, v); return; }
+    order[r] = v;
+}
+
+}  // namespace
+
+size_t hp_atr_scratch_bytes(int64_t n) {
+    const int64_t nn = 2 * n - 1;
+    size_t b = 0;
+    b += hp_carve::pad(nn);                        // state
+    b += 2 * hp_carve::pad(nn * 8);                // counts, key
+    b += 2 * hp_carve::pad(n * 4);                 // chain, base
+    b += hp_carve::pad(nn * 4);                    // order
+    b += hp_scan2_scratch_bytes(n);
+    b += hp_topdown_scratch_bytes(n);
+    return b;
+}
+
+hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out, int n,
+                       const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
+                       float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
+                       cudaStream_t s) {
+    const int64_t nn = 2 * (int64_t)n - 1;
+    const int T = p->atr_treelet;
+    if (T < 3 || T > TMAX) return hp_fail(HP_ERR_ARG, "ATR treelet size must be in [3, 32]");
+    if (p->atr_iterations < 0) return hp_fail(HP_ERR_ARG, "ATR iterations must be >= 0");
+    hp_carve cv(reinterpret_cast<char*>(scratch));
+    uint8_t* state = cv.take<uint8_t>(nn);
+    int2* counts = cv.take<int2>(nn);
+    int2* key = cv.take<int2>(nn);
+    int* chain = cv.take<int>(n);
+    int* base = cv.take<int>(n);
+    int* order = cv.take<int>(nn);
+    void* scan = cv.take<char>(hp_scan2_scratch_bytes(n));
+    void* td_scratch = cv.take<char>(hp_topdown_scratch_bytes(n));
+    int* err = ctx->d_status;
+
+    atr_args A{};
+    A.n = n; A.T = T; A.ct = p->ct; A.ci = p->ci;
+    A.left = left; A.right = right; A.parent = parent; A.nbmin = nbmin; A.nbmax = nbmax;
+    A.counters = counters; A.sorted_tri = sorted_tri; A.tbmin = tbmin; A.tbmax = tbmax; A.err = err;
+    int gamma = T, runs = 0;
+    for (int i = 0; i < p->atr_iterations; ++i) {
+        A.gamma = gamma;
+        A.init = (i == 0);
+        HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
+        k_atr_iter<<<hp_div_up(n, AB), AB, 0, s>>>(A);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        ++runs;
+        gamma *= 2;
+        if (gamma > n) break;
+    }
+    hp_mark(ctx, s, "atr");
+    fin_args F{};
+    F.n = n; F.init = runs == 0; F.adaptive = p->adaptive_leaf; F.max_leaf = p->max_leaf_size;
+    F.ct = p->ct; F.ci = p->ci; F.left = left; F.right = right; F.parent = parent; F.nbmin = nbmin;
+    F.nbmax = nbmax; F.counters = counters; F.state = state; F.counts = counts; F.key = key; F.chain = chain;
+    F.sorted_tri = sorted_tri; F.tbmin = tbmin; F.tbmax = tbmax; F.err = err;
+    HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
+    k_atr_finish<<<hp_div_up(n, 256), 256, 0, s>>>(F);
+    HP_CUDA(cudaGetLastError());
+    hp_scan2_sum(chain, n, nullptr, 0, base, nullptr, nullptr, scan, err, s);
+    k_atr_order<<<hp_div_up(nn, 256), 256, 0, s>>>(n, key, chain, base, order, err);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch(2);
+    hp_topdown_in in{};
+    in.n = n; in.left = left; in.right = right; in.parent = parent; in.counts = counts; in.state = state;
+    in.nbmin = nbmin; in.nbmax = nbmax; in.order = order; in.sorted_tri = sorted_tri;
+    HP_TRY(hp_topdown_collapse(ctx, m, in, out, td_scratch, s));
+    hp_mark(ctx, s, "collapse");
+    return HP_OK;
+}

@@ -420,6 +420,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits);
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
+    const bool atr = p->method == HP_METHOD_ATR;
     size_t need = 0;
     need += 2 * hp_carve::pad(n * 16);                  // triangle boxes
     need += 2 * hp_carve::pad(n * sizeof(K));           // keys, sorted keys
@@ -427,6 +428,11 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     need += hp_carve::pad(hp_sort_hist_bytes(plan.passes));
     if (ploc) {
         need += hp_carve::pad(n * 4) + hp_ploc_scratch_bytes(n);  // sorted references, clustering
+    } else if (atr) {
+        need += hp_carve::pad(n * 4);                                                     // sorted references
+        need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
+        need += 2 * hp_carve::pad(nn * 16) + hp_carve::pad(n * 4);                        // node boxes, counters
+        need += hp_atr_scratch_bytes(n);
     } else {
         need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
         need += 2 * hp_carve::pad(nn * 16);                   // node boxes
@@ -465,6 +471,49 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
             if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
             if (taps->sorted_refs)
                 HP_CUDA(cudaMemcpyAsync(taps->sorted_refs, sorted_refs, n * 4, cudaMemcpyDeviceToDevice, s));
+            if (taps->scene_box) k_tap_box<<<1, 32, 0, s>>>(info, taps->scene_box);
+            HP_CUDA(cudaGetLastError());
+        }
+        return HP_OK;
+    }
+    if (atr) {
+        int32_t* sorted_refs = cv.take<int32_t>(n);
+        int* parent = cv.take<int>(nn);
+        int* left = cv.take<int>(n);
+        int* right = cv.take<int>(n);
+        int2* range = cv.take<int2>(n);
+        float4* nbmin = cv.take<float4>(nn);
+        float4* nbmax = cv.take<float4>(nn);
+        int* counters = cv.take<int>(n);
+        void* atr_scratch = cv.take<char>(hp_atr_scratch_bytes(n));
+        k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
+        k_tri_boxes<<<grid_red, TB, 0, s>>>(m->vertices, m->num_vertices, m->triangles, n, tbmin, tbmax,
+                                            info->box_ord, err);
+        hp_count_launch(2);
+        hp_mark(ctx, s, "boxes");
+        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        hp_mark(ctx, s, "morton");
+        hp_sort_args sa{keys, nullptr, skeys, sorted_refs, sort_scratch, hist, true, err, ctx};
+        HP_TRY(hp_sort_run(plan, sa, s));
+        k_karras<K><<<grid_n, TB, 0, s>>>(skeys, (int)n, parent, left, right, range);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        hp_mark(ctx, s, "karras");
+        HP_TRY(hp_atr_stage(ctx, m, p, out, (int)n, sorted_refs, parent, left, right, nbmin, nbmax, counters,
+                            tbmin, tbmax, atr_scratch, s));
+        if (taps) {
+            if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
+            if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
+            if (taps->sorted_refs)
+                HP_CUDA(cudaMemcpyAsync(taps->sorted_refs, sorted_refs, n * 4, cudaMemcpyDeviceToDevice, s));
+            if (taps->node_parent || taps->node_left || taps->node_right || taps->node_box_min ||
+                taps->node_box_max)
+                k_tap_tree<<<hp_div_up(nn, TB), TB, 0, s>>>((int)n, parent, left, right, nbmin, nbmax,
+                                                           taps->node_parent, taps->node_left,
+                                                           taps->node_right, (float4*)taps->node_box_min,
+                                                           (float4*)taps->node_box_max);
             if (taps->scene_box) k_tap_box<<<1, 32, 0, s>>>(info, taps->scene_box);
             HP_CUDA(cudaGetLastError());
         }

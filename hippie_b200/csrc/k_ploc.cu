@@ -433,9 +433,12 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
     if (threadIdx.x == 0 && N != 1) hp_report(A.err, HP_DEV_BAD_INDEX, N);
 }
 
-// ---- depth-first collapse of a tree whose parents have lower indices ----------------------
+// ---- depth-first collapse of a tree whose parents come first in processing order ----------
+// Node v is processed at ticket position r with v = order[r] (order null: v = r,
+// which needs parent indices below child indices, as PLOC's are).
 struct td_args {
     int n;
+    const int* order;
     const int* left;
     const int* right;
     const int* parent;
@@ -471,8 +474,13 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
     if (threadIdx.x == 0) s_tile = atomicAdd(T.ticket, 1u);
     __syncthreads();
     const int n = T.n;
-    const int v = (int)s_tile * 256 + threadIdx.x;
-    if (v >= 2 * n - 1) return;
+    const int r = (int)s_tile * 256 + threadIdx.x;
+    if (r >= 2 * n - 1) return;
+    const int v = T.order ? __ldg(T.order + r) : r;
+    if ((unsigned)v >= (unsigned)(2 * n - 1)) {
+        hp_report(T.err, HP_DEV_BAD_INDEX, r);
+        return;
+    }
     const int2 c0 = T.counts[T.left[0]], c1 = T.counts[T.right[0]];
     const int num_int = 1 + c0.x + c1.x;
     int status, iidx = 0, lidx = 0, toff = 0, par = -1;
@@ -482,7 +490,7 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
         T.info->num_leaf = c0.y + c1.y;
     } else {
         const int p = T.parent[v];
-        if (p < 0 || p >= v || p >= n - 1) {
+        if (p < 0 || (!T.order && p >= v) || p >= n - 1) {
             hp_report(T.err, HP_DEV_BAD_INDEX, v);
             return;
         }
@@ -554,6 +562,50 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
 }
 
 }  // namespace
+
+size_t hp_topdown_scratch_bytes(int64_t n) {
+    return hp_carve::pad(n * 16) + hp_carve::pad(n * 4) + hp_carve::pad(64);
+}
+
+hp_status hp_topdown_collapse(hp_ctx* ctx, const hp_mesh* m, const hp_topdown_in& in, hp_bvh_impl* out,
+                              void* scratch, cudaStream_t s) {
+    const int n = in.n;
+    const int64_t nn = 2 * (int64_t)n - 1;
+    hp_carve cv(reinterpret_cast<char*>(scratch));
+    int4* rec = cv.take<int4>(n);
+    int* flag = cv.take<int>(n);
+    unsigned* ticket = cv.take<unsigned>(16);
+    HP_CUDA(cudaMemsetAsync(flag, 0, (size_t)n * 4, s));
+    HP_CUDA(cudaMemsetAsync(ticket, 0, 64, s));
+    td_args T{};
+    T.n = n;
+    T.order = in.order;
+    T.left = in.left;
+    T.right = in.right;
+    T.parent = in.parent;
+    T.counts = in.counts;
+    T.state = in.state;
+    T.nbmin = in.nbmin;
+    T.nbmax = in.nbmax;
+    T.rec = rec;
+    T.flag = flag;
+    T.epoch = 1;
+    T.ticket = ticket;
+    T.sorted_tri = in.sorted_tri;
+    T.verts = m->vertices;
+    T.nv = m->num_vertices;
+    T.tris = m->triangles;
+    T.nodes = out->nodes;
+    T.woop = out->woop;
+    T.tri_idx = out->tri_idx;
+    T.info = out->info;
+    T.max_nodes = (int)std::max<int64_t>(2 * out->capacity - 1, 3);
+    T.err = ctx->d_status;
+    k_topdown<<<hp_div_up(nn, 256), 256, 0, s>>>(T);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    return HP_OK;
+}
 
 size_t hp_ploc_scratch_bytes(int64_t n) {
     const int64_t nn = 2 * n - 1;

@@ -31,6 +31,9 @@ _SIGS = {
     "or_cost": (C.c_double, [_P, C.c_int64, _P, C.c_float, C.c_float]),
     "or_build_ploc": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
                                   C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "or_build_atr": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                 C.c_int, _P, _P, _P, _P, _P, _P, _P]),
+    "or_atr": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
     "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
@@ -142,6 +145,27 @@ def build_ploc(verts, tris, bits=60, radius=16, max_radius=256, adaptive_r=0, ct
                                _p(it))
     return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc,
                 iterations=int(it[0]))
+
+
+def build_atr(verts, tris, bits=60, treelet=9, iterations=2, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+    """LBVH + ATR treelet restructuring + depth-first collapse (ATRBuilder::build)."""
+    n = tris.shape[0]
+    cap = max(2 * n - 1, 3)
+    nodes = np.zeros((cap, 16), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    cnt = load().or_build_atr(_p(verts), _p(tris), n, bits, treelet, iterations, ct, ci, adaptive, max_leaf,
+                              _p(s_in), _p(nodes), _p(woop), _p(tri), _p(counts), _p(box), _p(sc))
+    return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
+
+
+def atr(n, parent, left, right, bmin4, bmax4, treelet=9, iterations=2, ct=3.0, ci=2.0):
+    """ATR iterations in place on a refitted binary tree (arrays over 2n-1 nodes)."""
+    return load().or_atr(n, treelet, iterations, ct, ci, _p(parent), _p(left), _p(right), _p(bmin4), _p(bmax4))
 
 
 def cost(nodes, scene_box, ct=3.0, ci=2.0):

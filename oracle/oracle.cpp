@@ -685,6 +685,280 @@ int64_t or_build_ploc(const float* verts, const int32_t* tris, int64_t n64, int 
                            size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
 }
 
+// ---- A15: ATR, agglomerative treelet restructuring (ATRBuilder::optimize,
+// rt/bvh/ATRBuilder.cpp:80-178; kernels optimize / optimizeSmall,
+// rt/bvh/ATRBuilderKernels.cu:12-554; formTreelet, rt/bvh/TRBuilderUtil.h:141-216).
+//
+// Per iteration (gamma = treelet size, doubled after each one) the reference
+// climbs from the leaves; at every node reached by its second child it sets
+// refs = refs(l) + refs(r), cost = ct*A + cost(l) + cost(r) (leaves: ci*A),
+// and a node with refs >= gamma becomes a treelet root right away. Every node
+// below a treelet root is final when the root is reached and concurrent
+// treelets are disjoint, so a sequential post-order gives the same result.
+// A treelet: starting from the root's two children, the treelet leaf with the
+// largest area that is not a BVH leaf is expanded until there are T leaves
+// (T-1 internal nodes, the root first); the leaves are then merged
+// agglomeratively by the area of the union box, the smallest pair first, the
+// new cluster taking the column slot and the last slot moving into the row
+// slot. The new topology is kept iff its cost is strictly below the old cost.
+// Ties in the two searches are broken by the reference's warp reductions,
+// simulated here lane by lane. Areas use the formula of the ATR kernels,
+// 2*(x*y + x*z + y*z), which the fast-math build contracts to
+// 2*fma(y, z, fma(x, y, x*z)).
+}  // extern "C"
+
+namespace {
+
+inline float atr_area(const float* mn, const float* mx) {
+    const float x = mx[0] - mn[0], y = mx[1] - mn[1], z = mx[2] - mn[2];
+    return 2.0f * std::fmaf(y, z, std::fmaf(x, y, x * z));
+}
+
+inline int tri_index(int row, int col) { return row * (row - 1) / 2 + col; }
+
+inline void tri_decode(int e, int& row, int& col) {
+    int r = (int)((1.0 + std::sqrt(8.0 * e + 1.0)) * 0.5);
+    while (r * (r - 1) / 2 > e) --r;
+    while ((r + 1) * r / 2 <= e) ++r;
+    row = r;
+    col = e - r * (r - 1) / 2;
+}
+
+struct atr_state {
+    int n, T;
+    float ct, ci;
+    int32_t *parent, *left, *right;
+    float *bmin4, *bmax4;
+    std::vector<float> cost;
+    std::vector<int> refs;
+};
+
+// findLeafToExpand (TRBuilderUtil.h:141-153) over `count` lanes: shuffles down
+// by count/2, the lower lane keeping its value unless the other is strictly
+// larger; repeated on ceil(count/2) lanes until one is left. Returns lane 0's index.
+int warp_argmax(const float* a_in, int count) {
+    float a[32];
+    int idx[32];
+    for (int k = 0; k < 32; ++k) { a[k] = k < count ? a_in[k] : -MAXF; idx[k] = k; }
+    int cnt = count, sh = cnt / 2;
+    while (cnt > 1) {
+        float na[32];
+        int ni[32];
+        for (int k = 0; k < 32; ++k) {
+            na[k] = a[k];
+            ni[k] = idx[k];
+            if (k + sh < 32 && a[k + sh] > a[k]) { na[k] = a[k + sh]; ni[k] = idx[k + sh]; }
+        }
+        std::memcpy(a, na, sizeof(a));
+        std::memcpy(idx, ni, sizeof(idx));
+        cnt = (cnt + 1) / 2;
+        sh = cnt / 2;
+    }
+    return idx[0];
+}
+
+// findMinimumDistance (ATRBuilderKernels.cu:68-94): lane l scans entries l,
+// l+32, ... keeping the first strict minimum; then a 32-lane reduction by
+// offsets 16..1 where the lower lane keeps its value unless the other is
+// strictly smaller. Returns the entry lane 0 ends with.
+int warp_argmin(const float* d, int m) {
+    float best[32];
+    int bi[32];
+    for (int l = 0; l < 32; ++l) {
+        best[l] = MAXF;
+        bi[l] = 0;
+        for (int e = l; e < m; e += 32)
+            if (d[e] < best[l]) { best[l] = d[e]; bi[l] = e; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        float nb[32];
+        int ni[32];
+        for (int l = 0; l < 32; ++l) {
+            nb[l] = best[l];
+            ni[l] = bi[l];
+            if (l + off < 32 && best[l + off] < best[l]) { nb[l] = best[l + off]; ni[l] = bi[l + off]; }
+        }
+        std::memcpy(best, nb, sizeof(best));
+        std::memcpy(bi, ni, sizeof(bi));
+    }
+    return bi[0];
+}
+
+void atr_treelet(atr_state& S, int root) {
+    const int T = S.T, n = S.n;
+    auto box = [&](int v, float* mn, float* mx) {
+        for (int a = 0; a < 3; ++a) { mn[a] = S.bmin4[4 * v + a]; mx[a] = S.bmax4[4 * v + a]; }
+    };
+    auto node_area = [&](int v) {
+        float mn[3], mx[3];
+        box(v, mn, mx);
+        return atr_area(mn, mx);
+    };
+    // formTreelet
+    std::vector<int> tl(T), ti(T - 1);
+    std::vector<float> ta(T);
+    tl[0] = S.left[root];
+    tl[1] = S.right[root];
+    ta[0] = node_area(tl[0]);
+    ta[1] = node_area(tl[1]);
+    ti[0] = root;
+    for (int it = 0; it < T - 2; ++it) {
+        const int m = it + 2;
+        float a[32];
+        for (int k = 0; k < m; ++k) a[k] = tl[k] >= n - 1 ? -MAXF : ta[k];
+        const int idx = warp_argmax(a, m);
+        const int rep = tl[idx];
+        ti[it + 1] = rep;
+        tl[idx] = S.left[rep];
+        tl[m] = S.right[rep];
+        ta[idx] = node_area(tl[idx]);
+        ta[m] = node_area(tl[m]);
+    }
+    // slot state and the distance matrix
+    std::vector<int> sn(T), sr(T);
+    std::vector<float> sc(T), smn(3 * T), smx(3 * T);
+    for (int k = 0; k < T; ++k) {
+        sn[k] = tl[k];
+        sc[k] = S.cost[tl[k]];
+        sr[k] = S.refs[tl[k]];
+        box(tl[k], &smn[3 * k], &smx[3 * k]);
+    }
+    auto union_area = [&](int i, int j) {
+        float mn[3], mx[3];
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(smn[3 * i + a], smn[3 * j + a]);
+            mx[a] = std::max(smx[3 * i + a], smx[3 * j + a]);
+        }
+        return atr_area(mn, mx);
+    };
+    std::vector<float> d(T * (T - 1) / 2);
+    for (int i = 1; i < T; ++i)
+        for (int j = 0; j < i; ++j) d[tri_index(i, j)] = union_area(i, j);
+    // outputs: internal node ti[k-1] is created at step k
+    std::vector<int> ol(T), orr(T), orf(T);
+    std::vector<float> oc(T), omn(3 * T), omx(3 * T);
+    for (int last = T - 1; last >= 1; --last) {
+        int row, col;
+        tri_decode(warp_argmin(d.data(), last * (last + 1) / 2), row, col);
+        float umn[3], umx[3];
+        for (int a = 0; a < 3; ++a) {
+            umn[a] = std::min(smn[3 * row + a], smn[3 * col + a]);
+            umx[a] = std::max(smx[3 * row + a], smx[3 * col + a]);
+        }
+        const float uc = std::fmaf(S.ct, atr_area(umn, umx), sc[row] + sc[col]);
+        ol[last] = sn[row];
+        orr[last] = sn[col];
+        oc[last] = uc;
+        orf[last] = sr[row] + sr[col];
+        for (int a = 0; a < 3; ++a) { omn[3 * last + a] = umn[a]; omx[3 * last + a] = umx[a]; }
+        // the last slot moves into the row slot, the new cluster takes the column slot
+        if (row != last) {
+            sn[row] = sn[last];
+            sc[row] = sc[last];
+            sr[row] = sr[last];
+            for (int a = 0; a < 3; ++a) { smn[3 * row + a] = smn[3 * last + a]; smx[3 * row + a] = smx[3 * last + a]; }
+        }
+        sn[col] = ti[last - 1];
+        sc[col] = uc;
+        sr[col] = orf[last];
+        for (int a = 0; a < 3; ++a) { smn[3 * col + a] = umn[a]; smx[3 * col + a] = umx[a]; }
+        if (last > 1) {
+            for (int t = 0; t < last; ++t)
+                if (t != row) d[tri_index(std::max(row, t), std::min(row, t))] = d[tri_index(last, t)];
+            for (int t = 0; t < last; ++t)
+                if (t != col) d[tri_index(std::max(col, t), std::min(col, t))] = union_area(t, col);
+        }
+    }
+    // updateTreelet (ATRBuilderKernels.cu:197-229)
+    if (!(oc[1] < S.cost[root])) return;
+    for (int k = 1; k < T; ++k) {
+        const int v = ti[k - 1];
+        S.left[v] = ol[k];
+        S.right[v] = orr[k];
+        S.parent[ol[k]] = v;
+        S.parent[orr[k]] = v;
+        S.cost[v] = oc[k];
+        S.refs[v] = orf[k];
+        for (int a = 0; a < 3; ++a) { S.bmin4[4 * v + a] = omn[3 * k + a]; S.bmax4[4 * v + a] = omx[3 * k + a]; }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Runs the ATR iterations on a refitted LBVH (parent / left / right / boxes over
+// 2n-1 nodes, leaves n-1..2n-2) in place. Returns the number of iterations run.
+int or_atr(int n, int treelet, int iterations, float ct, float ci, int32_t* parent, int32_t* left,
+           int32_t* right, float* bmin4, float* bmax4) {
+    if (n < 2 || treelet < 3 || treelet > 32) return 0;
+    atr_state S;
+    S.n = n; S.T = treelet; S.ct = ct; S.ci = ci;
+    S.parent = parent; S.left = left; S.right = right; S.bmin4 = bmin4; S.bmax4 = bmax4;
+    S.cost.assign(2 * n - 1, 0.0f);
+    S.refs.assign(2 * n - 1, 0);
+    for (int p = 0; p < n; ++p) {
+        const int j = n - 1 + p;
+        S.cost[j] = ci * atr_area(&bmin4[4 * j], &bmax4[4 * j]);
+        S.refs[j] = 1;
+    }
+    int gamma = treelet, done = 0;
+    for (int i = 0; i < iterations; ++i) {
+        ++done;
+        std::vector<std::pair<int, bool>> st{{0, false}};
+        while (!st.empty()) {
+            auto [v, expanded] = st.back();
+            if (v >= n - 1) { st.pop_back(); continue; }
+            if (!expanded) {
+                st.back().second = true;
+                st.push_back({right[v], false});
+                st.push_back({left[v], false});
+                continue;
+            }
+            st.pop_back();
+            const int l = left[v], r = right[v];
+            for (int a = 0; a < 3; ++a) {
+                bmin4[4 * v + a] = std::min(bmin4[4 * l + a], bmin4[4 * r + a]);
+                bmax4[4 * v + a] = std::max(bmax4[4 * l + a], bmax4[4 * r + a]);
+            }
+            S.refs[v] = S.refs[l] + S.refs[r];
+            S.cost[v] = std::fmaf(ct, atr_area(&bmin4[4 * v], &bmax4[4 * v]), S.cost[l]) + S.cost[r];
+            if (S.refs[v] >= gamma) atr_treelet(S, v);
+        }
+        gamma *= 2;
+        if (gamma > n) break;
+    }
+    return done;
+}
+
+// Whole ATR build (ATRBuilder::build, rt/bvh/ATRBuilder.cpp:180-236): the LBVH
+// stages, the ATR iterations, then the collapse of the restructured tree.
+int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int bits, int treelet, int iterations,
+                     float ct, float ci, int adaptive, int max_leaf, const float* scale_in, void* nodes_out,
+                     float* woop4, int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    if (n < 2)
+        return or_build_lbvh(verts, tris, n64, bits, ct, ci, adaptive, max_leaf, scale_in, nodes_out, woop4,
+                             tri_idx, counts, scene_box, scale_out);
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    std::vector<int32_t> sorted(n);
+    or_sort(n, keys.data(), bits, skeys.data(), sorted.data());
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), left(nn), right(nn), size(nn), state(nn);
+    or_karras(n, skeys.data(), parent.data(), left.data(), right.data());
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn), cost(nn);
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    or_atr(n, treelet, iterations, ct, ci, parent.data(), left.data(), right.data(), nbmin.data(), nbmax.data());
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    return or_collapse_dfs(n, verts, tris, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
+                           size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
+}
+
 // ---- A12: HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370, HipBVHKernels.cu:184-238) ----------
 double or_cost(const void* nodes_in, int64_t count, const float* scene_box, float ct, float ci) {
     const bin_node* nd = reinterpret_cast<const bin_node*>(nodes_in);

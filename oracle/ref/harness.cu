@@ -4,6 +4,8 @@
 // The sequences restate, without Qt or HIP, the reference host code:
 //   LBVHBuilder::build          rt/bvh/LBVHBuilder.cpp:183-241
 //   PLOCBuilder::clustering     rt/bvh/PLOCBuilder.cpp:21-159, build :161-208
+//   ATRBuilder::build / optimize / generateSchedule
+//                               rt/bvh/ATRBuilder.cpp:23-236
 //   BVHCollapser::collapseAdaptive + computeNodeOffsets loop
 //                               rt/bvh/BVHCollapser.cpp:14-306,521-597
 //   HipBVH::woopifyTriangles    rt/bvh/HipBVH.cpp:95-116
@@ -58,8 +60,9 @@ int fail(int code, const char* where) {
 
 // Host check of a binary tree over nodes 0..2n-2 (root 0, leaves n-1..):
 // every interior node's children are in range, name it as parent, and every
-// node but the root is a child exactly once. The collapse kernels climb these
-// links, so they only run on a tree that passes.
+// node but the root is a child exactly once, and a walk from the root reaches
+// all 2n-1 nodes (no detached cycle). Kernels that climb these links only run
+// on a tree that passes.
 bool valid_tree(int n, const int* parent, const int* left, const int* right) {
     const int nn = 2 * n - 1;
     std::vector<int> hp(nn), hl(nn), hr(nn), uses(nn, 0);
@@ -71,7 +74,15 @@ bool valid_tree(int n, const int* parent, const int* left, const int* right) {
     for (int i = 0; i < n - 1; ++i)
         for (int c : {hl[i], hr[i]})
             if (c <= 0 || c >= nn || hp[c] != i || uses[c]++) return false;
-    return true;
+    int seen = 0;
+    std::vector<int> st{0};
+    while (!st.empty()) {
+        const int v = st.back();
+        st.pop_back();
+        if (++seen > nn) return false;
+        if (v < n - 1) { st.push_back(hl[v]); st.push_back(hr[v]); }
+    }
+    return seen == nn;
 }
 
 // BVHCollapser::collapseAdaptive (Bin layout).
@@ -112,13 +123,75 @@ void ref_collapse(timer& T, int n, int* parent, int* left, int* right, float4* n
     cudaFree(node_off); cudaFree(node_idx); cudaFree(ref_off);
 }
 
+// ATRBuilder::generateSchedule (rt/bvh/ATRBuilder.cpp:23-56): the pairs (i, j),
+// j < i < T, packed two per int (a pair per 16 bits), 32 pairs per half-row.
+std::vector<int> atr_schedule(int T) {
+    const int elements = (T - 1) * T / 2;
+    const int iters = (elements + 63) / 64;
+    std::vector<int> s(iters * 32, 0);
+    int count = 0;
+    float mult = 0.0f;
+    for (int i = 0; i < T; ++i) {
+        for (int j = 0; j < i; ++j) {
+            const int idx = count + static_cast<int>(mult) * 32;
+            s[idx] = (s[idx] << 16) | (i << 8) | j;
+            if (++count == 32) {
+                mult += 0.5f;
+                count = 0;
+            }
+        }
+    }
+    if (static_cast<int>(mult + 0.5f) > static_cast<int>(mult))
+        for (int i = count; i < 32; ++i) s[i + static_cast<int>(mult) * 32] <<= 16;
+    return s;
+}
+
+// ATRBuilder::computeSurfaceAreas + optimize on a refitted LBVH.
+int ref_atr(timer& T, int n, int treelet, int iterations, float ct, float ci, int* parent, int* left, int* right,
+            float4* nbmin, float4* nbmax) {
+    const int nn = 2 * n - 1;
+    const std::vector<int> hs = atr_schedule(treelet);
+    int* schedule = dalloc<int>(hs.size());
+    cudaMemcpy(schedule, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice);
+    const int dist_size = (treelet - 1) * treelet / 2;
+    float* areas = dalloc<float>(nn);
+    float* costs = dalloc<float>(nn);
+    int* refs = dalloc<int>(nn);
+    int* counters = dalloc<int>(n);
+    float* dist = treelet > 20 ? dalloc<float>((size_t)dist_size * ((n + 31) / 32)) : nullptr;
+    int smem = ((2 * treelet - 1) * 4 + treelet * 4) * 4;
+    if (treelet <= 20) smem += dist_size * 4 * 4;
+    T.run([&] { hpref_atr_areas(nn, areas, nbmin, nbmax); });
+    int gamma = treelet;
+    for (int i = 0; i < iterations; ++i) {
+        cudaMemset(counters, 0, n * 4);
+        T.run([&] { hpref_atr_optimize(n, treelet, (int)hs.size(), dist_size, gamma, ci, ct, costs, areas, dist,
+                                       left, right, nbmin, nbmax, counters, parent, refs, schedule, smem); });
+        // The next launch climbs parent links with no bound: it only runs on a
+        // tree that is still valid.
+        if (!valid_tree(n, parent, left, right)) {
+            std::fprintf(stderr, "reference ATR produced an invalid tree (iteration %d)\n", i);
+            cudaFree(schedule); cudaFree(areas); cudaFree(costs); cudaFree(refs); cudaFree(counters); cudaFree(dist);
+            return 4;
+        }
+        gamma *= 2;
+        if (gamma > n) break;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(schedule); cudaFree(areas); cudaFree(costs); cudaFree(refs); cudaFree(counters); cudaFree(dist);
+    if (e != cudaSuccess) return fail(9, "after ATR optimize");
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* hpref_last_error(void) { return g_err; }
 
-// Build a BVH with the reference's kernels. method 0 = LBVH, 1 = PLOC.
+// Build a BVH with the reference's kernels. method 0 = LBVH, 1 = PLOC, 2 = ATR
+// (LBVH + treelet restructuring; radius carries the treelet size, max_radius
+// the iteration count).
 // Device inputs: verts, tris. Device outputs: nodes (64 B x (2n-1)), woop
 // (48 B x n), tri_idx (n). Optional device taps (null to skip): morton keys
 // (u64 n) before sorting, sorted keys, sorted reference indices, and the
@@ -198,7 +271,7 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     if (tap_refs) cudaMemcpy(tap_refs, refs0, n * 4, cudaMemcpyDeviceToDevice);
     T.run([&] { hpref_setup_leaves(n, refs0, refs1, tri0, tri1, left, right, nbmin, nbmax, rbmin, rbmax); });
     int iters = 0;
-    if (method == 0) {
+    if (method == 0 || method == 2) {
         T.run([&] { hpref_construct60(n, parent, left, right, keys0); });
         if (!valid_tree(n, parent, left, right)) {
             std::fprintf(stderr, "reference construct60 produced an invalid tree\n");
@@ -208,6 +281,14 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
         cudaMemset(counters, 0, n * 4);
         T.run([&] { hpref_refit(nn, counters, parent, left, right, nbmin, nbmax); });
         cudaFree(counters);
+        if (method == 2) {
+            const int rc = ref_atr(T, n, radius, max_radius, ct, ci, parent, left, right, nbmin, nbmax);
+            if (rc) return rc;
+            if (!valid_tree(n, parent, left, right)) {
+                std::fprintf(stderr, "reference ATR produced an invalid tree\n");
+                return 4;
+            }
+        }
     } else {
         // PLOCBuilder::build: referenceIndices[0] = referenceIndices[1], then clustering
         cudaMemcpy(refs0, refs1, n * 4, cudaMemcpyDeviceToDevice);

@@ -40,6 +40,12 @@ void hpref_collapse_compact(int nodes, int n_int, int* states, int* node_off, in
                             int* sizes, int* ref_off, float4* nbmin, float4* nbmax, void* out_nodes);
 void hpref_collapse_reorder(int n, int* left, int* ref_off, int* tri_in, int* tri_out, int* leaf_idx);
 
+// w_atr.cu
+void hpref_atr_areas(int nodes, float* areas, float4* nbmin, float4* nbmax);
+void hpref_atr_optimize(int n, int treelet, int schedule_size, int dist_size, int gamma, float ci, float ct,
+                        float* costs, float* areas, float* dist_mats, int* left, int* right, float4* nbmin,
+                        float4* nbmax, int* counters, int* parent, int* subtree_refs, int* schedule, int smem);
+
 // w_bvh.cu
 void hpref_woopify(int n, int* tri_idx, const int* tris, const float* verts, float4* woop);
 float hpref_cost(int nodes, float scene_area, float ct, float ci, void* bin_nodes);
