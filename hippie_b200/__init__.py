@@ -13,10 +13,10 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT, HP_TRACE_STATS,
-                   HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, load)
+from ._lib import (HP_BATCH_NO_GRAPH, HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT,
+                   HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, load)
 
-__all__ = ["Context", "BVH", "BuildParams", "Env", "HPError", "gen", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
+__all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
            "HP_METHOD_ATR", "HP_TRACE_ANY_HIT", "HP_TRACE_STATS", "load"]
 
 
@@ -210,6 +210,81 @@ class Context:
         check(load().hp_radix_sort(self.h, _ptr(keys), _ptr(vals), _ptr(ko), _ptr(vo), keys.shape[0], kb, bits,
                                    _stream_ptr(stream)))
         return ko, vo
+
+
+class Batch:
+    """Many meshes built (LBVH) and traced in a fixed number of launches (hp_batch_*).
+
+    meshes: list of (vertices, triangles) CUDA tensors, kept alive by the batch.
+    rays_per_mesh: ray count of every mesh; the rays of mesh m are rows
+    [ray_offset(m), ray_offset(m+1)) of the ray tensor given to trace().
+    With graph=True (default) launches replay a CUDA graph, which needs a
+    non-default stream (torch.cuda.stream(...))."""
+
+    def __init__(self, ctx: Context, meshes, rays_per_mesh, params: BuildParams | None = None):
+        self.ctx = ctx
+        self.meshes = list(meshes)
+        self.h = C.c_void_p()
+        params = params or BuildParams()
+        arr = (hp_mesh * max(len(self.meshes), 1))()
+        for i, (v, t) in enumerate(self.meshes):
+            arr[i] = _mesh(v, t)
+        rc = (C.c_int64 * max(len(self.meshes), 1))(*[int(r) for r in rays_per_mesh])
+        check(load().hp_batch_create(ctx.h, arr, len(self.meshes), rc, C.byref(params.c), C.byref(self.h)))
+        m, n, r = C.c_int32(), C.c_int64(), C.c_int64()
+        check(load().hp_batch_info(self.h, C.byref(m), C.byref(n), C.byref(r)))
+        self.num_meshes, self.num_triangles, self.num_rays = m.value, n.value, r.value
+
+    def close(self):
+        if getattr(self, "h", None) and load is not None:
+            load().hp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def ray_offset(self, m: int) -> int:
+        v = C.c_int64()
+        check(load().hp_batch_ray_offset(self.h, m, C.byref(v)))
+        return v.value
+
+    @staticmethod
+    def _flags(graph, any_hit=False, stats=None):
+        return (0 if graph else HP_BATCH_NO_GRAPH) | (HP_TRACE_ANY_HIT if any_hit else 0) | \
+            (HP_TRACE_STATS if stats is not None else 0)
+
+    @staticmethod
+    def _stream(stream, graph):
+        s = _stream_ptr(stream)
+        if graph and not s.value:
+            raise ValueError("graph launches need a non-default CUDA stream")
+        return s
+
+    def build(self, graph=True, stream=None):
+        check(load().hp_batch_build(self.ctx.h, self.h, self._flags(graph), self._stream(stream, graph)))
+
+    def trace(self, rays, results=None, stats=None, any_hit=False, graph=True, stream=None):
+        import torch
+        if results is None:
+            results = torch.empty((self.num_rays, 4), dtype=torch.int32, device=rays.device)
+        check(load().hp_batch_trace(self.ctx.h, self.h, _ptr(rays), _ptr(results), _ptr(stats),
+                                    self._flags(graph, any_hit, stats), self._stream(stream, graph)))
+        return results
+
+    def build_trace(self, rays, results=None, stats=None, any_hit=False, graph=True, stream=None):
+        import torch
+        if results is None:
+            results = torch.empty((self.num_rays, 4), dtype=torch.int32, device=rays.device)
+        check(load().hp_batch_build_trace(self.ctx.h, self.h, _ptr(rays), _ptr(results), _ptr(stats),
+                                          self._flags(graph, any_hit, stats), self._stream(stream, graph)))
+        return results
+
+    def bvh(self, m: int) -> BVH:
+        """A non-owning BVH view of mesh m (sync / download / cost / validate / Context.trace)."""
+        b = BVH(self.ctx)
+        check(load().hp_batch_bvh(self.h, m, C.byref(b.c)))
+        b.batch = self  # keeps the batch's storage alive
+        return b
 
 
 class gen:

@@ -17,6 +17,7 @@ STATUS_NAMES = {0: "HP_OK", 1: "HP_ERR_CUDA", 2: "HP_ERR_ARG", 3: "HP_ERR_OOM", 
 
 HP_METHOD_LBVH, HP_METHOD_PLOC, HP_METHOD_ATR = 0, 1, 2
 HP_TRACE_ANY_HIT, HP_TRACE_STATS = 1, 2
+HP_BATCH_NO_GRAPH = 0x100
 
 
 class hp_mesh(C.Structure):
@@ -69,6 +70,15 @@ _SIGS = {
     "hp_refit": (C.c_int, [_P, C.POINTER(hp_bvh), C.POINTER(hp_mesh), _P]),
     "hp_trace": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, _P]),
     "hp_trace_adjoint": (C.c_int, [_P, C.POINTER(hp_mesh), _P, _P, _P, C.c_int64, _P, _P]),
+    "hp_batch_create": (C.c_int, [_P, C.POINTER(hp_mesh), C.c_int32, C.POINTER(C.c_int64),
+                                  C.POINTER(hp_build_params), C.POINTER(C.c_void_p)]),
+    "hp_batch_destroy": (C.c_int, [_P]),
+    "hp_batch_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "hp_batch_ray_offset": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int64)]),
+    "hp_batch_build": (C.c_int, [_P, _P, C.c_uint32, _P]),
+    "hp_batch_trace": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
+    "hp_batch_build_trace": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
+    "hp_batch_bvh": (C.c_int, [_P, C.c_int32, C.POINTER(hp_bvh)]),
     "hp_radix_sort": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P]),
     "hp_radix_sort_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "hp_env_create": (C.c_int, [C.POINTER(C.c_void_p)]),

@@ -261,6 +261,8 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
     HP_TRY(check_params(p));
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t n = m->num_triangles;
+    if (out->impl && reinterpret_cast<hp_bvh_impl*>(out->impl)->view)
+        return hp_fail(HP_ERR_ARG, "hp_build: the output is a view into a batch");
     HP_TRY(bvh_alloc(out, n));
     hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
     out->num_refs = n;
@@ -309,6 +311,10 @@ hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh) {
     (void)ctx;
     if (!bvh) return HP_OK;
     hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(bvh->impl);
+    if (b && b->view) {  // a view into a batch: the batch owns the storage
+        std::memset(bvh, 0, sizeof(*bvh));
+        return HP_OK;
+    }
     if (b) {
         cudaFree(b->nodes);
         cudaFree(b->woop);
@@ -464,6 +470,8 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
     if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_refit: null argument");
     HP_TRY(check_mesh(m));
     if (m->num_triangles != bvh->num_refs) return hp_fail(HP_ERR_ARG, "hp_refit: mesh does not match the BVH");
+    if (reinterpret_cast<hp_bvh_impl*>(bvh->impl)->view)
+        return hp_fail(HP_ERR_UNSUPPORTED, "hp_refit: a BVH of a batch is rebuilt with hp_batch_build");
     return hp_refit_launch(ctx, reinterpret_cast<hp_bvh_impl*>(bvh->impl), bvh->num_refs, m,
                            reinterpret_cast<cudaStream_t>(stream));
 }

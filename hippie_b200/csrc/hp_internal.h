@@ -39,6 +39,7 @@ struct hp_bvh_impl {
     int32_t* counters = nullptr;   // refit termination counters [capacity]
     hp_bvh_info* info = nullptr;   // device
     int64_t capacity = 0;          // references
+    bool view = false;             // storage owned by a batch (hp_batch_bvh)
 };
 
 // ---- context: scratch arena, error words, phase events ------------------------
@@ -158,6 +159,33 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
                        cudaStream_t stream);
 hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
                           cudaStream_t stream);
+
+// ---- batches of meshes -------------------------------------------------------------
+// One entry per mesh of a batch (device table). The mesh's sorted positions,
+// woop rows and triangle-index slots start at tri_off, its node slots at
+// node_off (max(2n-1, 3) of them) and its rays at ray_off.
+struct hp_batch_seg {
+    const float* verts;
+    const int32_t* tris;
+    int64_t nv;
+    int32_t n;
+    int32_t tri_off;
+    int64_t node_off;
+    int64_t ray_off;
+};
+struct hp_batch_trace_args {
+    const float* rays;
+    int64_t num_rays;
+    int32_t* results;
+    int32_t* stats;
+    const hp_node_bin* nodes;
+    const float4* woop;
+    const int32_t* tri_idx;
+    const hp_batch_seg* segs;
+    const int64_t* ray_off;   // [num_segs + 1]
+    int num_segs;
+};
+hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint32_t flags, cudaStream_t stream);
 
 // ---- trace / adjoint ---------------------------------------------------------------
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,

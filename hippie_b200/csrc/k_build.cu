@@ -38,31 +38,6 @@ namespace {
 
 constexpr int TB = 256;
 
-__device__ __forceinline__ void load_vertex(const float* __restrict__ v, int64_t nv, int idx,
-                                            float& x, float& y, float& z, int* err) {
-    if (idx < 0 || idx >= nv) {
-        hp_report(err, HP_DEV_BAD_INPUT, idx);
-        idx = 0;
-    }
-    x = __ldg(v + 3 * (int64_t)idx + 0);
-    y = __ldg(v + 3 * (int64_t)idx + 1);
-    z = __ldg(v + 3 * (int64_t)idx + 2);
-}
-
-struct tri_verts {
-    float x0, y0, z0, x1, y1, z1, x2, y2, z2;
-};
-
-__device__ __forceinline__ tri_verts load_tri(const float* __restrict__ v, int64_t nv,
-                                              const int32_t* __restrict__ t, int64_t tri, int* err) {
-    tri_verts r;
-    int a = __ldg(t + 3 * tri + 0), b = __ldg(t + 3 * tri + 1), c = __ldg(t + 3 * tri + 2);
-    load_vertex(v, nv, a, r.x0, r.y0, r.z0, err);
-    load_vertex(v, nv, b, r.x1, r.y1, r.z1, err);
-    load_vertex(v, nv, c, r.x2, r.y2, r.z2, err);
-    return r;
-}
-
 // Per-triangle boxes (setupBoxes) and the scene box as their union
 // (SceneLoader.cpp:144-153 computes it over triangle boxes at load time).
 __global__ void __launch_bounds__(TB) k_tri_boxes(const float* __restrict__ verts, int64_t nv,

@@ -50,12 +50,26 @@ __device__ __forceinline__ float safe_rcp(float d) {
     return __frcp_rn(fabsf(d) > ooeps ? d : copysignf(ooeps, d));
 }
 
-template <bool ANY_HIT, bool STATS>
+// Index of the segment containing element g: the last m with off[m] <= g.
+__device__ __forceinline__ int seg_search(const int64_t* __restrict__ off, int num_segs, int64_t g) {
+    int lo = 0, hi = num_segs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// BATCH: rays of many meshes in one launch; ray g belongs to the segment whose
+// ray range holds it, and the lane traverses that mesh's BVH.
+template <bool ANY_HIT, bool STATS, bool BATCH>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
     const float4* __restrict__ rays, int64_t num_rays, int4* __restrict__ results,
-    int2* __restrict__ stats, const float4* __restrict__ nodes, const float4* __restrict__ woop,
-    const int32_t* __restrict__ tri_idx, int max_nodes, int num_refs,
-    unsigned long long* ray_counter, int* err) {
+    int2* __restrict__ stats, const float4* __restrict__ nodes_all, const float4* __restrict__ woop_all,
+    const int32_t* __restrict__ tri_all, int max_nodes_all, int num_refs_all,
+    unsigned long long* ray_counter, int* err, const hp_batch_seg* __restrict__ segs,
+    const int64_t* __restrict__ ray_off, int num_segs) {
     __shared__ int s_stack[SSTACK * TRACE_BLOCK];
     int* sstack = s_stack + threadIdx.x;
     int lstack[LSTACK];
@@ -69,6 +83,10 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
     int sp = 0;
     int steps = 0;  // node + leaf visits of the current ray (bounded)
     bool exhausted = false;
+    const float4* nodes = nodes_all;
+    const float4* woop = woop_all;
+    const int32_t* tri_idx = tri_all;
+    int max_nodes = max_nodes_all, num_refs = num_refs_all;
 
     while (true) {
         // Refill lanes whose ray is finished (one atomic per warp).
@@ -97,12 +115,28 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
                     steps = 0;
                     leaf = 0;
                     node = 0;
+                    if (BATCH) {
+                        const hp_batch_seg& g = segs[seg_search(ray_off, num_segs, id)];
+                        nodes = nodes_all + 4 * g.node_off;
+                        woop = woop_all + 3 * (int64_t)g.tri_off;
+                        tri_idx = tri_all + g.tri_off;
+                        num_refs = g.n;
+                        max_nodes = max(2 * g.n - 1, 3);
+                        if (g.n == 0) {  // empty mesh: the ray misses
+                            reinterpret_cast<int2*>(results)[2 * id] = make_int2(-1, __float_as_int(d.w));
+                            if (STATS) stats[id] = make_int2(0, 0);
+                            node = SENTINEL;
+                        }
+                    }
                 } else {
                     exhausted = true;
                 }
             }
         }
-        if (__all_sync(HP_FULL_MASK, node == SENTINEL)) break;
+        if (__all_sync(HP_FULL_MASK, node == SENTINEL)) {
+            if (!BATCH || __all_sync(HP_FULL_MASK, exhausted)) break;
+            continue;  // every lane drew a ray of an empty mesh
+        }
 
         // Traverse until fewer than FETCH_THRESHOLD lanes of the warp still hold
         // a ray; the warp reconverges after every round so that the decision
@@ -247,21 +281,47 @@ hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const floa
                    int64_t num_rays, int32_t* results, int32_t* stats, unsigned long long* counter,
                    cudaStream_t s) {
     int per_sm = 0;
-    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S>, TRACE_BLOCK, 0));
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, false>, TRACE_BLOCK, 0));
     int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
     grid = std::min<int64_t>(grid, (num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
     const int max_nodes = (int)std::max<int64_t>(2 * b->capacity - 1, 3);
-    k_trace<A, S><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
+    k_trace<A, S, false><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
         reinterpret_cast<const float4*>(rays), num_rays, reinterpret_cast<int4*>(results),
         reinterpret_cast<int2*>(stats), reinterpret_cast<const float4*>(b->nodes), b->woop, b->tri_idx,
-        max_nodes, (int)n_refs, counter, ctx->d_status);
+        max_nodes, (int)n_refs, counter, ctx->d_status, nullptr, nullptr, 0);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "trace");
     return HP_OK;
 }
 
+template <bool A, bool S>
+hp_status launch_batch_t(hp_ctx* ctx, const hp_batch_trace_args& t, unsigned long long* counter, cudaStream_t s) {
+    int per_sm = 0;
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, true>, TRACE_BLOCK, 0));
+    int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
+    grid = std::min<int64_t>(grid, (t.num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
+    k_trace<A, S, true><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
+        reinterpret_cast<const float4*>(t.rays), t.num_rays, reinterpret_cast<int4*>(t.results),
+        reinterpret_cast<int2*>(t.stats), reinterpret_cast<const float4*>(t.nodes), t.woop, t.tri_idx, 0, 0,
+        counter, ctx->d_status, t.segs, t.ray_off, t.num_segs);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    return HP_OK;
+}
+
 }  // namespace
+
+hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint32_t flags, cudaStream_t s) {
+    if (t.num_rays <= 0) return HP_OK;
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
+    HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+    const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && t.stats;
+    if (any && st) return launch_batch_t<true, true>(ctx, t, counter, s);
+    if (any) return launch_batch_t<true, false>(ctx, t, counter, s);
+    if (st) return launch_batch_t<false, true>(ctx, t, counter, s);
+    return launch_batch_t<false, false>(ctx, t, counter, s);
+}
 
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                           int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,

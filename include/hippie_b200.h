@@ -189,6 +189,34 @@ hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays,
                            const int32_t* results, const float* dl_dtuv, int64_t num_rays,
                            float* dl_dvertices, void* stream);
 
+/* ---- batches of meshes ---------------------------------------------------- */
+/* Many independent meshes of uneven size built (LBVH) and traced in a fixed
+ * number of launches, replayed from a CUDA graph. New entry points with no
+ * counterpart in the reference; each mesh gets exactly the BVH hp_build makes
+ * for it. The meshes' device buffers stay owned by the caller and must live
+ * as long as the batch. Rays of mesh m occupy rays [offset(m), offset(m+1))
+ * of the ray array (hp_batch_ray_offset), in mesh order, 8 floats each;
+ * results and stats follow the same order and layout as hp_trace's, with
+ * mesh-local triangle ids. Morton bits + ceil(log2(num_meshes)) must be <= 64. */
+typedef struct hp_batch hp_batch;
+#define HP_BATCH_NO_GRAPH 0x100u   /* flags: launch directly instead of from a CUDA graph */
+hp_status hp_batch_create(hp_ctx* ctx, const hp_mesh* meshes, int32_t num_meshes,
+                          const int64_t* rays_per_mesh, const hp_build_params* p, hp_batch** out);
+hp_status hp_batch_destroy(hp_batch* b);
+hp_status hp_batch_info(const hp_batch* b, int32_t* num_meshes, int64_t* num_triangles, int64_t* num_rays);
+hp_status hp_batch_ray_offset(const hp_batch* b, int32_t mesh, int64_t* offset);
+/* Build every mesh's BVH, trace every ray against its mesh, or both. A CUDA
+ * graph needs a non-default stream; it is captured on the first call and again
+ * whenever the buffers, flags or the context's scratch arena change. */
+hp_status hp_batch_build(hp_ctx* ctx, hp_batch* b, uint32_t flags, void* stream);
+hp_status hp_batch_trace(hp_ctx* ctx, hp_batch* b, const float* rays, int32_t* results, int32_t* stats,
+                         uint32_t flags, void* stream);
+hp_status hp_batch_build_trace(hp_ctx* ctx, hp_batch* b, const float* rays, int32_t* results,
+                               int32_t* stats, uint32_t flags, void* stream);
+/* A non-owning hp_bvh for mesh m of the batch (for hp_bvh_sync / download /
+ * cost / validate / hp_trace); hp_bvh_free on it releases nothing. */
+hp_status hp_batch_bvh(hp_batch* b, int32_t mesh, hp_bvh* out);
+
 /* ---- primitives ------------------------------------------------------------ */
 /* Stable LSD radix sort of (key, value) pairs by key bits [0, bits). key_bytes
  * is 4 or 8. vals_in may be NULL (values are then 0..n-1). Output in keys_out /

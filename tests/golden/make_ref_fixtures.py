@@ -5,7 +5,7 @@ from the reference sources (oracle/ref/Makefile). For two small synthetic
 meshes it records what the reference's kernels produce: Morton keys, the
 sorted reference order, the pre-collapse LBVH topology and refitted boxes,
 the collapsed binary BVH (nodes, triangle order, Woop triangles), a PLOC BVH,
-and closest hits of the reference tracer. The scene box and the Morton scale
+an ATR BVH (treelet 9, 2 iterations) and closest hits of the reference tracer. The scene box and the Morton scale
 (the approximate reciprocal the reference's fast-math build uses) are stored
 with them, so the CPU oracle can be compared against the reference offline.
 
@@ -41,6 +41,9 @@ def main(out):
         p = R.build(V, T, box, method="ploc", bits=bits, radius=4, max_radius=64)
         for k in ("nodes", "tri_idx", "counts"):
             data[f"{name}_ploc_{k}"] = p[k]
+        a = R.build(V, T, box, method="atr", bits=bits, treelet=9, iterations=2)
+        for k in ("nodes", "tri_idx", "counts"):
+            data[f"{name}_atr_{k}"] = a[k]
         rays = hp.gen.rays_targeted(73, 2000) if name == "uniform" else \
             hp.gen.rays_sphere(74, 2000, np.concatenate([v.min(0), v.max(0)]))
         res, _ = R.trace(torch.from_numpy(ref["nodes"]).cuda(), torch.from_numpy(ref["woop"]).cuda(),

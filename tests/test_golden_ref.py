@@ -73,6 +73,17 @@ def test_oracle_ploc_equals_reference_kernels(fx, name):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_atr_equals_reference_kernels(fx, name):
+    if f"{name}_atr_nodes" not in fx:
+        pytest.skip("fixture predates the ATR vectors")
+    make, bits = CASES[name]
+    v, t = make()
+    r = oracle.build_atr(v, t, bits=bits, treelet=9, iterations=2, scale=fx[f"{name}_scale"])
+    np.testing.assert_array_equal(r["counts"], fx[f"{name}_atr_counts"])
+    assert canonical(r["nodes"], r["tri_idx"]) == canonical(fx[f"{name}_atr_nodes"], fx[f"{name}_atr_tri_idx"])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
 def test_oracle_trace_on_reference_bvh(fx, name):
     """The oracle's traversal of the reference's own BVH finds the reference tracer's hits."""
     v, t = CASES[name][0]()
