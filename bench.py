@@ -217,6 +217,134 @@ def reference_kernels(cfg, V, T, R, v, reps=3):
                     "own sort; times are sums of per-kernel CUDA events as the reference reports them"}
 
 
+def _events(torch, k):
+    return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+
+
+def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2):
+    """Batched build + trace of 2048 meshes (log-uniform 256..262,144 triangles,
+    the uniform generator; 4 rays per triangle, origins uniform in [-0.5,1.5]^3,
+    directions uniform on the sphere) against the same meshes and rays built and
+    traced one mesh at a time through the plain path: as host-loop launches, and
+    with those per-mesh launches captured into one CUDA graph."""
+    import torch
+    import hippie_b200 as hp
+    rng = np.random.default_rng(seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(262144), num_meshes))).astype(np.int64)
+    box = np.array([-0.5, -0.5, -0.5, 1.5, 1.5, 1.5], np.float32)
+    meshes, counts = [], []
+    for m, n in enumerate(sizes):
+        v, t = hp.gen.uniform_mesh(seed + 17 * m, int(n), 0.01)
+        meshes.append((torch.from_numpy(v).cuda(), torch.from_numpy(t).cuda()))
+        counts.append(4 * int(n))
+    R_total = int(sum(counts))
+    R = torch.empty((R_total, 8), dtype=torch.float32, device="cuda")
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for m in range(num_meshes):
+        R[off[m]:off[m + 1]] = torch.from_numpy(hp.gen.rays_sphere(seed + 17 * m + 5, counts[m], box)).cuda()
+    p = hp.BuildParams(method="lbvh", morton_bits=30)
+    res_plain = torch.zeros((R_total, 4), dtype=torch.int32, device="cuda")
+    res_batch = torch.zeros((R_total, 4), dtype=torch.int32, device="cuda")
+    bvhs = [hp.BVH(ctx) for _ in range(num_meshes)]
+    views = [(R[off[m]:off[m + 1]], res_plain[off[m]:off[m + 1]]) for m in range(num_meshes)]
+
+    def plain():
+        for m in range(num_meshes):
+            ctx.build(meshes[m][0], meshes[m][1], p, bvh=bvhs[m])
+            ctx.trace(bvhs[m], views[m][0], results=views[m][1])
+
+    s = torch.cuda.Stream()
+    batch = hp.Batch(ctx, meshes, counts, p)
+    with torch.cuda.stream(s):
+        plain()  # allocates every per-mesh BVH once
+        batch.build_trace(R, results=res_batch)
+        torch.cuda.synchronize()
+        ctx.check()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            plain()
+        ev_loop, ev_graph, ev_batch = _events(torch, steps), _events(torch, steps), _events(torch, steps)
+        for k in range(steps):
+            ev_loop[k][0].record(s)
+            plain()
+            ev_loop[k][1].record(s)
+        for k in range(steps):
+            ev_graph[k][0].record(s)
+            g.replay()
+            ev_graph[k][1].record(s)
+        for k in range(steps):
+            ev_batch[k][0].record(s)
+            batch.build_trace(R, results=res_batch)
+            ev_batch[k][1].record(s)
+        # build and trace separately, for the split
+        batch.build()
+        eb = _events(torch, 2)
+        eb[0][0].record(s)
+        batch.build()
+        eb[0][1].record(s)
+        eb[1][0].record(s)
+        batch.trace(R, results=res_batch)
+        eb[1][1].record(s)
+    torch.cuda.synchronize()
+    ctx.check()
+    same = bool(torch.equal(res_plain, res_batch))
+    t_loop = float(np.median([a.elapsed_time(b) for a, b in ev_loop]))
+    t_graph = float(np.median([a.elapsed_time(b) for a, b in ev_graph]))
+    t_batch = float(np.median([a.elapsed_time(b) for a, b in ev_batch]))
+    out = {"workload": f"{num_meshes} meshes, {int(sizes.sum())} triangles (log-uniform 256..262144), "
+                       f"{R_total} sphere rays", "triangles": int(sizes.sum()), "rays": R_total,
+           "plain_host_loop_ms": t_loop, "plain_graph_ms": t_graph, "batched_ms": t_batch,
+           "speedup_vs_plain_host_loop": t_loop / t_batch, "speedup_vs_plain_graph": t_graph / t_batch,
+           "batched_build_ms": eb[0][0].elapsed_time(eb[0][1]), "batched_trace_ms": eb[1][0].elapsed_time(eb[1][1]),
+           "results_identical": same}
+    del g
+    batch.close()
+    return out
+
+
+def extra_differentiable(ctx, steps=10, seed=SEED + 3):
+    """Heightfield of 512 x 1024 vertices (1,045,506 triangles, 16 sinusoids),
+    4,194,304 downward rays on a jittered 2048 x 2048 grid, loss weights
+    w ~ N(0,1): forward trace, adjoint into vertex gradients, refit after a
+    vertex step. Ratio (forward + adjoint) / forward on CUDA events."""
+    import torch
+    import hippie_b200 as hp
+    v, t = hp.gen.heightfield(seed, 512, 1024, 1.0, 2.0, 16)
+    rays = hp.gen.rays_grid_down(seed + 1, 2048, 2048, 1.0, 2.0, 1.0)
+    w = np.random.default_rng(seed + 2).standard_normal((rays.shape[0], 3)).astype(np.float32)
+    V, T, R, W = (torch.from_numpy(x).cuda() for x in (v, t, rays, w))
+    p = hp.BuildParams(method="lbvh", morton_bits=60)
+    bvh = ctx.build(V, T, p)
+    res = torch.zeros((R.shape[0], 4), dtype=torch.int32, device="cuda")
+    grad = torch.zeros_like(V)
+    s = torch.cuda.current_stream()
+    for _ in range(3):
+        ctx.trace(bvh, R, results=res)
+        grad.zero_()
+        ctx.adjoint(V, T, R, res, W, dl_dverts=grad)
+        ctx.refit(bvh, V, T)
+    torch.cuda.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(steps)]
+    for k in range(steps):
+        ev[k][0].record(s)
+        ctx.trace(bvh, R, results=res)
+        ev[k][1].record(s)
+        grad.zero_()
+        ev[k][2].record(s)
+        ctx.adjoint(V, T, R, res, W, dl_dverts=grad)
+        ev[k][3].record(s)
+        ctx.refit(bvh, V, T)
+        ev[k][4].record(s)
+    torch.cuda.synchronize()
+    ctx.check()
+    fwd = float(np.median([e[0].elapsed_time(e[1]) for e in ev]))
+    adj = float(np.median([e[2].elapsed_time(e[3]) for e in ev]))
+    ref = float(np.median([e[3].elapsed_time(e[4]) for e in ev]))
+    return {"workload": "heightfield 512x1024 (1,045,506 triangles), 4,194,304 downward rays",
+            "forward_ms": fwd, "adjoint_ms": adj, "refit_ms": ref, "fwd_plus_adjoint_over_fwd": (fwd + adj) / fwd,
+            "hits": int((res[:, 0] >= 0).sum())}
+
+
 def run_reference(args, cfg, rank):
     """CPU restatement of the path, timed on the host cores (rank 0 only)."""
     if rank != 0:
@@ -265,6 +393,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one build and one trace, then print the phase times (for profiler runs)")
+    ap.add_argument("--extras", type=int, default=1,
+                    help="also measure the batched (2048 meshes) and differentiable (heightfield) workloads")
     ap.add_argument("--rays", type=int, default=0, help="override the workload's ray count (profiling)")
     ap.add_argument("--reference-kernels", type=int, default=1,
                     help="also time the reference's own CUDA kernels where they were built (1 GPU)")
@@ -425,6 +555,12 @@ def main(argv=None):
         line["cpu_baseline"] = cpu_baseline(cfg, v, t, rays)
     if rank == 0 and world == 1 and args.reference_kernels:
         line["reference_kernels_gpu"] = reference_kernels(cfg, V, T, R, v)
+    if world == 1 and args.extras:
+        del V, T, R, RES
+        torch.cuda.empty_cache()
+        line["batched"] = extra_batched(ctx)
+        torch.cuda.empty_cache()
+        line["differentiable"] = extra_differentiable(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del bvh
