@@ -221,27 +221,33 @@ def _events(torch, k):
     return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
 
 
-def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2):
+def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2, rank=0, world=1):
     """Batched build + trace of 2048 meshes (log-uniform 256..262,144 triangles,
     the uniform generator; 4 rays per triangle, origins uniform in [-0.5,1.5]^3,
     directions uniform on the sphere) against the same meshes and rays built and
     traced one mesh at a time through the plain path: as host-loop launches, and
-    with those per-mesh launches captured into one CUDA graph."""
+    with those per-mesh launches captured into one CUDA graph. Under torchrun
+    the meshes are split across ranks by LPT (no data-path collective) and the
+    times are the max over ranks."""
     import torch
     import hippie_b200 as hp
+    from hippie_b200.shard import lpt_partition, mesh_work
     rng = np.random.default_rng(seed)
-    sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(262144), num_meshes))).astype(np.int64)
+    all_sizes = np.round(np.exp(rng.uniform(np.log(256), np.log(262144), num_meshes))).astype(np.int64)
+    mine = lpt_partition(mesh_work(all_sizes, 4 * all_sizes), world)[rank]
+    sizes = all_sizes[mine]
+    num_meshes = len(mine)
     box = np.array([-0.5, -0.5, -0.5, 1.5, 1.5, 1.5], np.float32)
     meshes, counts = [], []
-    for m, n in enumerate(sizes):
-        v, t = hp.gen.uniform_mesh(seed + 17 * m, int(n), 0.01)
+    for j, m in enumerate(mine):
+        v, t = hp.gen.uniform_mesh(seed + 17 * int(m), int(sizes[j]), 0.01)
         meshes.append((torch.from_numpy(v).cuda(), torch.from_numpy(t).cuda()))
-        counts.append(4 * int(n))
+        counts.append(4 * int(sizes[j]))
     R_total = int(sum(counts))
-    R = torch.empty((R_total, 8), dtype=torch.float32, device="cuda")
-    off = np.concatenate([[0], np.cumsum(counts)])
-    for m in range(num_meshes):
-        R[off[m]:off[m + 1]] = torch.from_numpy(hp.gen.rays_sphere(seed + 17 * m + 5, counts[m], box)).cuda()
+    R = torch.empty((max(R_total, 1), 8), dtype=torch.float32, device="cuda")
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    for j, m in enumerate(mine):
+        R[off[j]:off[j + 1]] = torch.from_numpy(hp.gen.rays_sphere(seed + 17 * int(m) + 5, counts[j], box)).cuda()
     p = hp.BuildParams(method="lbvh", morton_bits=30)
     res_plain = torch.zeros((R_total, 4), dtype=torch.int32, device="cuda")
     res_batch = torch.zeros((R_total, 4), dtype=torch.int32, device="cuda")
@@ -288,15 +294,23 @@ def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2):
     torch.cuda.synchronize()
     ctx.check()
     same = bool(torch.equal(res_plain, res_batch))
-    t_loop = float(np.median([a.elapsed_time(b) for a, b in ev_loop]))
-    t_graph = float(np.median([a.elapsed_time(b) for a, b in ev_graph]))
-    t_batch = float(np.median([a.elapsed_time(b) for a, b in ev_batch]))
-    out = {"workload": f"{num_meshes} meshes, {int(sizes.sum())} triangles (log-uniform 256..262144), "
-                       f"{R_total} sphere rays", "triangles": int(sizes.sum()), "rays": R_total,
+    t = torch.tensor([float(np.median([a.elapsed_time(b) for a, b in ev_loop])),
+                      float(np.median([a.elapsed_time(b) for a, b in ev_graph])),
+                      float(np.median([a.elapsed_time(b) for a, b in ev_batch])),
+                      eb[0][0].elapsed_time(eb[0][1]), eb[1][0].elapsed_time(eb[1][1]),
+                      0.0 if same else 1.0], device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_loop, t_graph, t_batch, t_build, t_trace, bad = t.tolist()
+    tris, rays = int(all_sizes.sum()), int(4 * all_sizes.sum())
+    out = {"workload": f"{len(all_sizes)} meshes, {tris} triangles (log-uniform 256..262144), "
+                       f"{rays} sphere rays", "triangles": tris, "rays": rays,
            "plain_host_loop_ms": t_loop, "plain_graph_ms": t_graph, "batched_ms": t_batch,
            "speedup_vs_plain_host_loop": t_loop / t_batch, "speedup_vs_plain_graph": t_graph / t_batch,
-           "batched_build_ms": eb[0][0].elapsed_time(eb[0][1]), "batched_trace_ms": eb[1][0].elapsed_time(eb[1][1]),
-           "results_identical": same}
+           "batched_build_ms": t_build, "batched_trace_ms": t_trace,
+           "batched_mtris_s": tris / t_batch / 1e3, "batched_mrays_s": rays / t_batch / 1e3,
+           "results_identical": bad == 0.0, "sharding": f"LPT over {world} rank(s), max over ranks"}
     del g
     batch.close()
     return out
@@ -555,12 +569,13 @@ def main(argv=None):
         line["cpu_baseline"] = cpu_baseline(cfg, v, t, rays)
     if rank == 0 and world == 1 and args.reference_kernels:
         line["reference_kernels_gpu"] = reference_kernels(cfg, V, T, R, v)
-    if world == 1 and args.extras:
+    if args.extras:
         del V, T, R, RES
         torch.cuda.empty_cache()
-        line["batched"] = extra_batched(ctx)
-        torch.cuda.empty_cache()
-        line["differentiable"] = extra_differentiable(ctx)
+        line["batched"] = extra_batched(ctx, rank=rank, world=world)
+        if world == 1:
+            torch.cuda.empty_cache()
+            line["differentiable"] = extra_differentiable(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del bvh
