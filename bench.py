@@ -359,6 +359,77 @@ def extra_differentiable(ctx, steps=10, seed=SEED + 3):
             "hits": int((res[:, 0] >= 0).sum())}
 
 
+def extra_large(ctx, steps=3, seed=SEED + 4):
+    """33,554,432 triangles (16,777,216 from the uniform generator interleaved with
+    16,777,216 from the clustered one), LBVH 60-bit then ATR (treelet 9, 2
+    iterations); 64 Mi rays: 32 Mi pinhole primaries on an 8192 x 4096 grid
+    (camera at (0.5, 0.5, -1.5) looking at the unit box, 45 degree field of view,
+    pixel-table order) and 32 Mi rays from origins uniform in the scene box with
+    directions uniform on the sphere, traced plain and in ray Morton order."""
+    import torch
+    import hippie_b200 as hp
+    half = 1 << 24
+    v1, t1 = hp.gen.uniform_mesh(seed, half, 0.01)
+    v2, t2 = hp.gen.clustered_mesh(seed + 1, half, 1024, 0.02, 0.005)
+    tris = np.empty((2 * half, 3), np.int32)
+    tris[0::2] = t1
+    tris[1::2] = t2 + v1.shape[0]
+    verts = np.concatenate([v1, v2])
+    del v1, v2, t1, t2
+    V, T = torch.from_numpy(verts).cuda(), torch.from_numpy(tris).cuda()
+    box = np.concatenate([verts.min(0), verts.max(0)]).astype(np.float32)
+    del verts, tris
+    n = 2 * half
+    w, h = 8192, 4096
+    pos = np.array([0.5, 0.5, -1.5], np.float32)
+    m = hp.camera_screen_to_world(pos, [0.0, 0.0, 1.0], 45.0, w, h, 0.01, 100.0)
+    table = torch.from_numpy(hp.pixel_table(w, h)).cuda()
+    prim = ctx.primary_rays(pos, m, w, h, index_to_pixel=table)
+    sec = torch.from_numpy(hp.gen.rays_sphere(seed + 2, w * h, box)).cuda()
+    res = torch.zeros((w * h, 4), dtype=torch.int32, device="cuda")
+    p_atr = hp.BuildParams(method="atr", morton_bits=60, atr_treelet=9, atr_iterations=2)
+    p_lbvh = hp.BuildParams(method="lbvh", morton_bits=60)
+    lb = ctx.build(V, T, p_lbvh)
+    at = ctx.build(V, T, p_atr)
+    s = torch.cuda.current_stream()
+    ctx.trace(at, prim, results=res)
+    ctx.trace_sorted(at, sec, results=res)
+    torch.cuda.synchronize()
+    ctx.check()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(7)] for _ in range(steps)]
+    for k in range(steps):
+        e = ev[k]
+        e[0].record(s)
+        ctx.build(V, T, p_lbvh, bvh=lb)
+        e[1].record(s)
+        ctx.build(V, T, p_atr, bvh=at)
+        e[2].record(s)
+        ctx.primary_rays(pos, m, w, h, index_to_pixel=table, out=prim)
+        e[3].record(s)
+        ctx.trace(at, prim, results=res)
+        e[4].record(s)
+        ctx.trace(at, sec, results=res)
+        e[5].record(s)
+        ctx.trace_sorted(at, sec, results=res)
+        e[6].record(s)
+    torch.cuda.synchronize()
+    ctx.check()
+
+    def med(a, b):
+        return float(np.median([e[a].elapsed_time(e[b]) for e in ev]))
+
+    t_lbvh, t_atr, t_gen, t_prim, t_sec, t_sort = (med(0, 1), med(1, 2), med(2, 3), med(3, 4), med(4, 5),
+                                                   med(5, 6))
+    return {"workload": "33,554,432 tris (uniform + clustered, interleaved), LBVH 60-bit + ATR treelet 9 x 2; "
+                        "32Mi pinhole primaries (8192x4096) + 32Mi sphere rays",
+            "lbvh_build_ms": t_lbvh, "atr_build_ms": t_atr, "atr_mtris_s": n / t_atr / 1e3,
+            "lbvh_mtris_s": n / t_lbvh / 1e3, "sah_cost_lbvh": lb.cost(), "sah_cost_atr": at.cost(),
+            "primary_gen_ms": t_gen, "primary_trace_mrays_s": w * h / t_prim / 1e3,
+            "secondary_trace_mrays_s": w * h / t_sec / 1e3,
+            "secondary_sorted_trace_mrays_s": w * h / t_sort / 1e3,
+            "rays_total": 2 * w * h}
+
+
 def run_reference(args, cfg, rank):
     """CPU restatement of the path, timed on the host cores (rank 0 only)."""
     if rank != 0:
@@ -576,6 +647,8 @@ def main(argv=None):
         if world == 1:
             torch.cuda.empty_cache()
             line["differentiable"] = extra_differentiable(ctx)
+            torch.cuda.empty_cache()
+            line["large"] = extra_large(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     del bvh

@@ -16,7 +16,8 @@ import numpy as np
 from ._lib import (HP_BATCH_NO_GRAPH, HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT,
                    HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, load)
 
-__all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
+__all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "pixel_table",
+           "camera_screen_to_world", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
            "HP_METHOD_ATR", "HP_TRACE_ANY_HIT", "HP_TRACE_STATS", "load"]
 
 
@@ -192,6 +193,38 @@ class Context:
                               _stream_ptr(stream)))
         return results
 
+    def trace_sorted(self, bvh: BVH, rays, results=None, stats=None, any_hit=False, bits=30, order=None,
+                     stream=None):
+        """HipTracer::traceSort: trace in ray Morton order; results at each ray's own index."""
+        import torch
+        n = rays.shape[0]
+        if results is None:
+            results = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+        flags = (HP_TRACE_ANY_HIT if any_hit else 0) | (HP_TRACE_STATS if stats is not None else 0)
+        check(load().hp_trace_sorted(self.h, C.byref(bvh.c), _ptr(rays), n, _ptr(results), _ptr(stats), flags,
+                                     bits, _ptr(order), _stream_ptr(stream)))
+        return results
+
+    def ray_keys(self, rays, bits=30, box=None, stream=None):
+        import torch
+        keys = torch.empty(rays.shape[0], dtype=torch.int64, device=rays.device)
+        b = None if box is None else np.ascontiguousarray(box, np.float32)
+        check(load().hp_ray_keys(self.h, _ptr(rays), rays.shape[0], None if b is None else b.ctypes.data, bits,
+                                 _ptr(keys), _stream_ptr(stream)))
+        return keys
+
+    def primary_rays(self, position, screen_to_world, width, height, max_dist=float("inf"), sample_index=0,
+                     index_to_pixel=None, out=None, stream=None):
+        """RayGen::primary: width*height pinhole rays (8 floats each) in pixel-table order."""
+        import torch
+        rays = out if out is not None else torch.empty((width * height, 8), dtype=torch.float32,
+                                                       device=f"cuda:{self.device}")
+        pos = np.ascontiguousarray(position, np.float32)
+        m = np.ascontiguousarray(screen_to_world, np.float32).reshape(16)
+        check(load().hp_gen_primary_rays(self.h, pos.ctypes.data, m.ctypes.data, width, height, max_dist,
+                                         sample_index, _ptr(index_to_pixel), _ptr(rays), _stream_ptr(stream)))
+        return rays
+
     def adjoint(self, verts, tris, rays, results, dl_dtuv, dl_dverts=None, stream=None):
         import torch
         if dl_dverts is None:
@@ -285,6 +318,23 @@ class Batch:
         check(load().hp_batch_bvh(self.h, m, C.byref(b.c)))
         b.batch = self  # keeps the batch's storage alive
         return b
+
+
+def pixel_table(width: int, height: int):
+    """PixelTable::recalculate: pixel index of every ray slot (host int32 array)."""
+    t = np.empty(width * height, np.int32)
+    check(load().hp_pixel_table(width, height, t.ctypes.data))
+    return t
+
+
+def camera_screen_to_world(position, direction, fov_deg, width, height, near=0.01, far=100.0):
+    """inverse(projection * view) of the reference's Camera, row-major 4x4 (float32)."""
+    out = np.empty(16, np.float32)
+    p = np.ascontiguousarray(position, np.float32)
+    d = np.ascontiguousarray(direction, np.float32)
+    check(load().hp_camera_screen_to_world(p.ctypes.data, d.ctypes.data, fov_deg, width, height, near, far,
+                                           out.ctypes.data))
+    return out.reshape(4, 4)
 
 
 class gen:

@@ -79,6 +79,11 @@ _SIGS = {
     "hp_batch_trace": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "hp_batch_build_trace": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "hp_batch_bvh": (C.c_int, [_P, C.c_int32, C.POINTER(hp_bvh)]),
+    "hp_trace_sorted": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, C.c_int32, _P, _P]),
+    "hp_pixel_table": (C.c_int, [C.c_int32, C.c_int32, _P]),
+    "hp_camera_screen_to_world": (C.c_int, [_P, _P, C.c_float, C.c_int32, C.c_int32, C.c_float, C.c_float, _P]),
+    "hp_gen_primary_rays": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_int32, _P, _P, _P]),
+    "hp_ray_keys": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int32, _P, _P]),
     "hp_radix_sort": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P]),
     "hp_radix_sort_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "hp_env_create": (C.c_int, [C.POINTER(C.c_void_p)]),

@@ -188,9 +188,10 @@ struct hp_batch_trace_args {
 hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint32_t flags, cudaStream_t stream);
 
 // ---- trace / adjoint ---------------------------------------------------------------
+// order (or null): slot k of the launch traces ray order[k].
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                           int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const int32_t* order = nullptr);
 hp_status hp_adjoint_launch(hp_ctx* ctx, const hp_mesh* m, const float* rays,
                             const int32_t* results, const float* dl_dtuv, int64_t num_rays,
                             float* dl_dvertices, cudaStream_t stream);

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
     int2* __restrict__ stats, const float4* __restrict__ nodes_all, const float4* __restrict__ woop_all,
     const int32_t* __restrict__ tri_all, int max_nodes_all, int num_refs_all,
     unsigned long long* ray_counter, int* err, const hp_batch_seg* __restrict__ segs,
-    const int64_t* __restrict__ ray_off, int num_segs) {
+    const int64_t* __restrict__ ray_off, int num_segs, const int32_t* __restrict__ order) {
     __shared__ int s_stack[SSTACK * TRACE_BLOCK];
     int* sstack = s_stack + threadIdx.x;
     int lstack[LSTACK];
@@ -98,8 +98,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
             if (lane == leader) base = atomicAdd(ray_counter, (unsigned long long)__popc(need_mask));
             base = __shfl_sync(HP_FULL_MASK, base, leader);
             if (need) {
-                const int64_t id = (int64_t)base + __popc(need_mask & lt_mask);
-                if (id < num_rays) {
+                const int64_t slot = (int64_t)base + __popc(need_mask & lt_mask);
+                // traceSort: slot k traces ray order[k] (rays in Morton order)
+                const int64_t id = (order && slot < num_rays) ? (int64_t)__ldg(order + slot) : slot;
+                if (slot < num_rays && (uint64_t)id >= (uint64_t)num_rays) {
+                    hp_report(err, HP_DEV_BAD_INDEX, (int)slot);
+                    exhausted = true;
+                } else if (id < num_rays) {
                     ray = id;
                     const float4 o = __ldg(rays + 2 * id), d = __ldg(rays + 2 * id + 1);
                     r.ox = o.x; r.oy = o.y; r.oz = o.z; r.tmin = o.w;
@@ -279,7 +284,7 @@ __global__ void k_trace_empty(const float4* rays, int64_t num_rays, int4* result
 template <bool A, bool S>
 hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                    int64_t num_rays, int32_t* results, int32_t* stats, unsigned long long* counter,
-                   cudaStream_t s) {
+                   const int32_t* order, cudaStream_t s) {
     int per_sm = 0;
     HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, false>, TRACE_BLOCK, 0));
     int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
@@ -288,7 +293,7 @@ hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const floa
     k_trace<A, S, false><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
         reinterpret_cast<const float4*>(rays), num_rays, reinterpret_cast<int4*>(results),
         reinterpret_cast<int2*>(stats), reinterpret_cast<const float4*>(b->nodes), b->woop, b->tri_idx,
-        max_nodes, (int)n_refs, counter, ctx->d_status, nullptr, nullptr, 0);
+        max_nodes, (int)n_refs, counter, ctx->d_status, nullptr, nullptr, 0, order);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "trace");
@@ -304,7 +309,7 @@ hp_status launch_batch_t(hp_ctx* ctx, const hp_batch_trace_args& t, unsigned lon
     k_trace<A, S, true><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
         reinterpret_cast<const float4*>(t.rays), t.num_rays, reinterpret_cast<int4*>(t.results),
         reinterpret_cast<int2*>(t.stats), reinterpret_cast<const float4*>(t.nodes), t.woop, t.tri_idx, 0, 0,
-        counter, ctx->d_status, t.segs, t.ray_off, t.num_segs);
+        counter, ctx->d_status, t.segs, t.ray_off, t.num_segs, nullptr);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     return HP_OK;
@@ -325,7 +330,7 @@ hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint3
 
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                           int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
-                          cudaStream_t s) {
+                          cudaStream_t s, const int32_t* order) {
     if (num_rays <= 0) return HP_OK;
     if (n_refs <= 0) {
         k_trace_empty<<<hp_div_up(num_rays, 256), 256, 0, s>>>(
@@ -339,8 +344,8 @@ hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, con
     HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     hp_mark(ctx, s, "trace_begin");
     const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && stats;
-    if (any && st) return launch_t<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
-    if (any) return launch_t<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
-    if (st) return launch_t<false, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
-    return launch_t<false, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, s);
+    if (any && st) return launch_t<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    if (any) return launch_t<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    if (st) return launch_t<false, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    return launch_t<false, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
 }

@@ -9,12 +9,17 @@
  * paths relative to src/hippie/):
  *   hp_build            BVHBuilder::build / rebuild           rt/bvh/BVHBuilder.h:16-68,
  *                       LBVHBuilder::build                    rt/bvh/LBVHBuilder.cpp:183-241,
- *                       PLOCBuilder::build                    rt/bvh/PLOCBuilder.cpp:161-208
+ *                       PLOCBuilder::build                    rt/bvh/PLOCBuilder.cpp:161-208,
+ *                       ATRBuilder::build                     rt/bvh/ATRBuilder.cpp:180-236
  *   hp_bvh_*            HipBVH (nodes, woop, triangle idx)    rt/bvh/HipBVH.h:19-106
  *   hp_bvh_cost         HipBVH::getCost                       rt/bvh/HipBVH.cpp:346-370
  *   hp_bvh_validate     HipBVH::validate                      rt/bvh/HipBVH.cpp:157-307
  *   hp_refit            HipBVH::update (woopify + refit)      rt/bvh/HipBVH.cpp:472-477
  *   hp_trace            HipTracer::trace / traceStats         rt/tracer/HipTracer.cpp:13-52
+ *   hp_trace_sorted     HipTracer::traceSort                  rt/tracer/HipTracer.cpp:109-125
+ *   hp_gen_primary_rays RayGen::primary                       rt/ray/RayGen.cpp:35-62
+ *   hp_pixel_table      PixelTable::recalculate               rt/ray/PixelTable.cpp:10-80
+ *   hp_ray_keys         RayBuffer::computeMortonCodes         rt/ray/RayBuffer.cpp:31-80
  *   hp_radix_sort       RadixSort::sort                       radix_sort/RadixSort.cpp:181-238
  *   hp_env_*            Environment / AppEnvironment          environment/Environment.cpp:290-466,
  *                                                             environment/AppEnvironment.cpp:10-91
@@ -180,6 +185,42 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream);
  * lower triangle id. */
 hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays,
                    int32_t* results, int32_t* stats, uint32_t flags, void* stream);
+
+/* Trace in ray Morton order (HipTracer::traceSort, rt/tracer/HipTracer.cpp:109-125;
+ * RayBuffer::mortonSort, rt/ray/RayBuffer.cpp:112-131): keys as hp_ray_keys
+ * with the reference's [0,1]^3 ray box and `bits` key bits (the reference's
+ * default is 30), a stable radix sort, then a traversal whose slot k takes
+ * ray order[k]. Results land at each ray's own index, as with hp_trace.
+ * order_out (device, num_rays int32, or NULL) receives the ray order. */
+hp_status hp_trace_sorted(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays,
+                          int32_t* results, int32_t* stats, uint32_t flags, int32_t bits,
+                          int32_t* order_out, void* stream);
+
+/* ---- ray generation (RayGen, PixelTable) ---------------------------------- */
+/* Pixel order of PixelTable::recalculate (rt/ray/PixelTable.cpp:10-80): 8x8
+ * blocks in Morton order, pixels swizzled within a block, then the stripes
+ * below and to the right. Host memory, width*height entries. */
+hp_status hp_pixel_table(int32_t width, int32_t height, int32_t* index_to_pixel);
+/* inverse(projection * view) of the reference's Camera (rt/scene/Camera.cpp:95-109)
+ * for a camera at `position` looking along `direction` (no roll), vertical
+ * field of view fov_deg, aspect width/height; row-major 4x4 into out16. */
+hp_status hp_camera_screen_to_world(const float* position, const float* direction, float fov_deg,
+                                    int32_t width, int32_t height, float near_plane, float far_plane,
+                                    float* out16);
+/* Primary rays (RayGen::primary, rt/ray/RayGen.cpp:35-62; generatePrimaryRays,
+ * rt/ray/RayGenKernels.cu:106-153): ray k goes through pixel index_to_pixel[k]
+ * (device array, or NULL for row-major order) jittered by the Halton point of
+ * sample_index, from `position` (host, 3 floats), tmin 0, tmax max_dist.
+ * rays: device, width*height rays of 8 floats. */
+hp_status hp_gen_primary_rays(hp_ctx* ctx, const float* position, const float* screen_to_world16,
+                              int32_t width, int32_t height, float max_dist, int32_t sample_index,
+                              const int32_t* index_to_pixel, float* rays, void* stream);
+/* Ray Morton keys (computeMortonCodesAila64, rt/ray/RayBufferKernels.cu:556-615):
+ * origin normalised to ray_box6 (host {min xyz, max xyz}; NULL = [0,1]^3 as
+ * the reference), direction mapped to [0,1]^3, 13 bits per axis, interleaved;
+ * the top `bits` of the 64-bit code. keys: device, num_rays uint64. */
+hp_status hp_ray_keys(hp_ctx* ctx, const float* rays, int64_t num_rays, const float* ray_box6,
+                      int32_t bits, uint64_t* keys, void* stream);
 
 /* ---- adjoint ------------------------------------------------------------ */
 /* Scatter dL/d(t,u,v) (3 floats per ray) of closest hits into dL/dvertices

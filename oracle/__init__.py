@@ -34,6 +34,9 @@ _SIGS = {
     "or_build_atr": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
                                  C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "or_atr": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
+    "or_pixel_table": (C.c_int32, [C.c_int32, C.c_int32, _P]),
+    "or_primary_rays": (None, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P, _P]),
+    "or_ray_keys": (None, [_P, C.c_int64, _P, C.c_int32, _P]),
     "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
@@ -166,6 +169,40 @@ def build_atr(verts, tris, bits=60, treelet=9, iterations=2, ct=3.0, ci=2.0, ada
 def atr(n, parent, left, right, bmin4, bmax4, treelet=9, iterations=2, ct=3.0, ci=2.0):
     """ATR iterations in place on a refitted binary tree (arrays over 2n-1 nodes)."""
     return load().or_atr(n, treelet, iterations, ct, ci, _p(parent), _p(left), _p(right), _p(bmin4), _p(bmax4))
+
+
+def pixel_table(width, height):
+    t = np.empty(width * height, np.int32)
+    k = load().or_pixel_table(width, height, _p(t))
+    assert k == width * height
+    return t
+
+
+def halton(i, base):
+    """Radical inverse as the library computes it (double, then rounded to float)."""
+    r, f = 0.0, 1.0 / base
+    while i > 0:
+        r += f * (i % base)
+        i //= base
+        f /= base
+    return np.float32(r)
+
+
+def primary_rays(origin, m, width, height, sample_index=0, max_dist=np.inf, index_to_pixel=None):
+    rays = np.empty((width * height, 8), np.float32)
+    o = np.ascontiguousarray(origin, np.float32)
+    mm = np.ascontiguousarray(m, np.float32).reshape(16)
+    tbl = None if index_to_pixel is None else np.ascontiguousarray(index_to_pixel, np.int32)
+    load().or_primary_rays(_p(o), _p(mm), width, height, float(halton(sample_index, 2)),
+                           float(halton(sample_index, 3)), max_dist, _p(tbl), _p(rays))
+    return rays
+
+
+def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1)):
+    keys = np.empty(rays.shape[0], np.uint64)
+    b = np.ascontiguousarray(box, np.float32)
+    load().or_ray_keys(_p(np.ascontiguousarray(rays)), rays.shape[0], _p(b), bits, _p(keys))
+    return keys
 
 
 def cost(nodes, scene_box, ct=3.0, ci=2.0):

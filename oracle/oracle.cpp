@@ -959,6 +959,108 @@ int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int b
                            size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
 }
 
+// ---- ray generation and ray keys ---------------------------------------------------
+// PixelTable::recalculate (rt/ray/PixelTable.cpp:10-80), walked as the reference
+// does: Morton indices over a square of block coordinates whose side is the
+// power of two the reference's bit-smearing gives, keeping blocks inside the
+// image, then the bottom stripe column by column and the right stripe row by row.
+int32_t or_pixel_table(int32_t width, int32_t height, int32_t* idxtopos) {
+    int idx = 0;
+    const int bheight = height & ~7, bwidth = width & ~7;
+    int maxdim = bwidth > bheight ? bwidth : bheight;
+    maxdim |= maxdim >> 1;
+    maxdim |= maxdim >> 2;
+    maxdim |= maxdim >> 4;
+    maxdim |= maxdim >> 8;
+    maxdim |= maxdim >> 16;
+    maxdim = (maxdim + 1) >> 1;
+    const int width8 = bwidth >> 3, height8 = bheight >> 3;
+    for (int64_t i = 0; i < (int64_t)maxdim * maxdim; ++i) {
+        int tx = 0, ty = 0, bit = 1;
+        int64_t val = i;
+        while (val) {
+            if (val & 1) tx |= bit;
+            if (val & 2) ty |= bit;
+            bit += bit;
+            val >>= 2;
+        }
+        if (tx < width8 && ty < height8) {
+            for (int inner = 0; inner < 64; inner++) {
+                const int ix = ((inner & 1) >> 0) | ((inner & 4) >> 1) | ((inner & 16) >> 2);
+                const int iy = ((inner & 2) >> 1) | ((inner & 8) >> 2) | ((inner & 32) >> 3);
+                idxtopos[idx++] = (ty * 8 + iy) * width + (tx * 8 + ix);
+            }
+        }
+    }
+    for (int px = 0; px < bwidth; px++)
+        for (int py = bheight; py < height; py++) idxtopos[idx++] = px + py * width;
+    for (int py = 0; py < height; py++)
+        for (int px = bwidth; px < width; px++) idxtopos[idx++] = px + py * width;
+    return idx;
+}
+
+// generatePrimaryRays (rt/ray/RayGenKernels.cu:106-153) with IEEE rounding and
+// the fma order of the CUDA kernel; hx, hy: the sample's Halton point.
+void or_primary_rays(const float* origin, const float* m, int32_t width, int32_t height, float hx, float hy,
+                     float max_dist, const int32_t* index_to_pixel, float* rays) {
+    const int64_t n = (int64_t)width * height;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t pixel = index_to_pixel ? index_to_pixel[i] : i;
+        const float x = (float)(pixel % width) + hx, y = (float)(pixel / width) + hy;
+        const float nx = (2.0f * x) / (float)width - 1.0f, ny = (2.0f * y) / (float)height - 1.0f;
+        float w[4];
+        for (int r = 0; r < 4; ++r) w[r] = std::fmaf(m[4 * r], nx, std::fmaf(m[4 * r + 1], ny, m[4 * r + 3]));
+        const float dx = w[0] / w[3] - origin[0], dy = w[1] / w[3] - origin[1], dz = w[2] / w[3] - origin[2];
+        const float len = std::sqrt(std::fmaf(dz, dz, std::fmaf(dy, dy, dx * dx)));
+        float* r = rays + 8 * i;
+        r[0] = origin[0]; r[1] = origin[1]; r[2] = origin[2]; r[3] = 0.0f;
+        r[4] = dx / len; r[5] = dy / len; r[6] = dz / len; r[7] = max_dist;
+    }
+}
+
+// computeMortonCodesAila64 (rt/ray/RayBufferKernels.cu:556-615), IEEE-rounded.
+void or_ray_keys(const float* rays, int64_t n, const float* box6, int32_t bits, uint64_t* keys) {
+    float mn[3], inv[3];
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = box6[a];
+        const float ext = box6[3 + a] - box6[a];
+        inv[a] = ext > 0.0f ? 1.0f / ext : 0.0f;
+    }
+    auto q = [](float a) { return (int)std::trunc(a * 8191.0f); };
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        int ia[3], ib[3];
+        const float len = std::sqrt(std::fmaf(r[6], r[6], std::fmaf(r[5], r[5], r[4] * r[4])));
+        for (int a = 0; a < 3; ++a) {
+            ia[a] = q((r[a] - mn[a]) * inv[a]);
+            ib[a] = q((r[4 + a] / len + 1.0f) * 0.5f);
+        }
+        uint64_t c = 0;
+        c |= (uint64_t)((ia[0] >> 12) & 1) << 63;
+        c |= (uint64_t)((ia[1] >> 12) & 1) << 62;
+        c |= (uint64_t)((ia[2] >> 12) & 1) << 61;
+        c |= (uint64_t)((ia[0] >> 11) & 1) << 60;
+        c |= (uint64_t)((ia[1] >> 11) & 1) << 59;
+        c |= (uint64_t)((ia[2] >> 11) & 1) << 58;
+        c |= (uint64_t)((ia[0] >> 10) & 1) << 57;
+        c |= (uint64_t)((ia[1] >> 10) & 1) << 56;
+        c |= (uint64_t)((ia[2] >> 10) & 1) << 55;
+        for (int b = 9; b >= 1; --b) {
+            c |= (uint64_t)((ia[0] >> b) & 1) << (6 * b + 0);
+            c |= (uint64_t)((ia[1] >> b) & 1) << (6 * b - 1);
+            c |= (uint64_t)((ia[2] >> b) & 1) << (6 * b - 2);
+        }
+        for (int b = 12; b >= 4; --b) {
+            c |= (uint64_t)((ib[0] >> b) & 1) << (6 * b - 21);
+            c |= (uint64_t)((ib[1] >> b) & 1) << (6 * b - 22);
+            c |= (uint64_t)((ib[2] >> b) & 1) << (6 * b - 23);
+        }
+        keys[i] = c >> (64 - bits);
+    }
+}
+
 // ---- A12: HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370, HipBVHKernels.cu:184-238) ----------
 double or_cost(const void* nodes_in, int64_t count, const float* scene_box, float ct, float ci) {
     const bin_node* nd = reinterpret_cast<const bin_node*>(nodes_in);
