@@ -62,4 +62,5 @@ def test_primary_rays_trace(ctx):
     res = ctx.trace(bvh, R, results=torch.zeros((w * h, 4), dtype=torch.int32, device="cuda")).cpu().numpy()
     nodes, woop, tri = bvh.download()
     np.testing.assert_array_equal(res, oracle.trace(nodes, woop, tri, R.cpu().numpy()))
-    assert (res[:, 0] >= 0).mean() > 0.5
+    # the unit box covers about 40 % of this 2:1 image
+    assert 0.1 < (res[:, 0] >= 0).mean() < 0.6
