@@ -566,6 +566,22 @@ def main(argv=None):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         build_ms, trace_ms, step_ms = tt.tolist()
 
+    # ---- the same rays traced in ray Morton order (keys + sort + trace, HipTracer::traceSort) ----
+    for _ in range(2):
+        ctx.trace_sorted(bvh, R, results=RES)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    for k in range(args.steps):
+        evs[k][0].record(stream)
+        ctx.trace_sorted(bvh, R, results=RES)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    ctx.check()
+    sorted_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    if world > 1:
+        tt = torch.tensor([sorted_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        sorted_ms = tt.item()
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e_b, e2e_t = [], []
     for k in range(max(3, args.steps // 2)):
@@ -623,6 +639,7 @@ def main(argv=None):
                    "morton_bits": cfg["bits"], "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (mesh 200 MB, rays 512 MB)"},
         "trace_mrays_s": world * nr / (trace_ms * 1e-3) / 1e6,
+        "trace_sorted_mrays_s": world * nr / (sorted_ms * 1e-3) / 1e6,
         "build_ms": build_ms, "trace_ms": trace_ms,
         "phases_ms": {k: round(x, 4) for k, x in phases.items()},
         "e2e": {"value": world * n / e2e_b_s / 1e6, "unit": "Mtris/s",

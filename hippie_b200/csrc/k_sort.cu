@@ -6,12 +6,13 @@
 // after each launch. Here every 8-bit digit is one kernel:
 //   * all digit histograms are counted in one read of the keys up front
 //     (or by the kernel that produced the keys);
-//   * each pass ranks a tile of keys with warp-level match/popc, finds the
-//     tile's global digit offsets by decoupled look-back over earlier tiles
+//   * each pass counts a tile's digits and publishes the counts first, finds
+//     the tile's global digit offsets by decoupled look-back over earlier tiles
 //     (tiles are taken in launch order from an atomic ticket, so a tile only
-//     waits on tiles that are already running; every wait is bounded), and
-//     writes keys and values out of a shared-memory staging buffer so that
-//     runs of equal digits leave as contiguous stores.
+//     waits on tiles that are already running; every wait is bounded), ranks
+//     keys within each warp with ballots, and writes keys and values out of a
+//     shared-memory staging buffer so that runs of equal digits leave as
+//     contiguous stores.
 // The result equals a stable sort by key: ties keep their input order, so
 // with values 0..n-1 ties are ordered by original index, as in the reference.
 #include <algorithm>
@@ -95,6 +96,51 @@ __device__ __forceinline__ void scan256x2(uint32_t a, uint32_t b, uint32_t& ea, 
     }
 }
 
+// Digit-offset look-back for digit `tid` of this tile: the sum of the digit's
+// counts over all earlier tiles, walking back over LB status words per round
+// until a tile whose inclusive prefix is published. Every wait is bounded.
+__device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t tile, int tid, int* err) {
+    constexpr int LB = 4;
+    uint32_t prefix = 0, spins = 0;
+    int64_t t = (int64_t)tile - 1;
+    bool done = tile == 0;
+    while (!done) {
+        uint32_t sw[LB];
+#pragma unroll
+        for (int k = 0; k < LB; ++k)
+            sw[k] = (t - k >= 0) ? ld_relaxed_u32(&status[(size_t)(t - k) * 256 + tid]) : 0u;
+#pragma unroll
+        for (int k = 0; k < LB; ++k) {
+            if (done) break;
+            if (t - k < 0) { done = true; break; }
+            uint32_t s = sw[k];
+            while ((s & ~ST_MASK) == 0u) {
+                if (++spins > LOOKBACK_SPIN_LIMIT) {
+                    hp_report(err, HP_DEV_SPIN_LIMIT, (int)tile);
+                    s = ST_FLAG_P;
+                    break;
+                }
+                s = ld_relaxed_u32(&status[(size_t)(t - k) * 256 + tid]);
+            }
+            prefix += s & ST_MASK;
+            if ((s & ~ST_MASK) == ST_FLAG_P || t - k == 0) done = true;
+        }
+        t -= LB;
+    }
+    return prefix;
+}
+
+// One LSD pass over a tile of TILE keys:
+//   1. load the keys (and values) of the tile;
+//   2. count the tile's digits with shared-memory atomics and publish the
+//      counts at once, so that later tiles' look-backs see them early;
+//   3. look back for the digit offsets of all earlier tiles (256 threads, one
+//      per digit) while the other warps go on to rank;
+//   4. rank within each warp in index order (round i, then lane): the lanes
+//      of equal digit are found with 8 ballots, and per-warp counters carry
+//      the counts from round to round;
+//   5. stage the keys in shared memory in digit order and write them out, so
+//      that runs of equal digits leave as contiguous stores.
 template <typename K, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK) k_onesweep(
     const K* __restrict__ keys_in, const int32_t* __restrict__ vals_in,
@@ -108,6 +154,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     uint32_t* cnt = reinterpret_cast<uint32_t*>(smem);          // [NW][256] while ranking
     K* skeys = reinterpret_cast<K*>(smem);                        // [TILE] while scattering
     int32_t* svals = reinterpret_cast<int32_t*>(smem + (size_t)TILE * sizeof(K));
+    __shared__ uint32_t s_count[256];
     __shared__ uint32_t s_block_start[256];
     __shared__ uint32_t s_global[256];
     __shared__ uint32_t s_w[2][8];
@@ -116,6 +163,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int i = tid; i < NW * 256; i += BLOCK) cnt[i] = 0;
+    if (tid < 256) s_count[tid] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const int64_t base = (int64_t)tile * TILE;
@@ -132,32 +180,14 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
         key[i] = valid ? keys_in[idx] : K(0);
         val[i] = valid ? (vals_in ? vals_in[idx] : (int32_t)idx) : 0;
     }
-    // Rank within the warp: items are visited in index order (round i, then lane).
-    uint32_t* wcnt = cnt + warp * 256;
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        int64_t idx = wbase + i * 32 + lane;
-        bool valid = idx < n;
-        uint32_t d = valid ? digit_of(key[i], shift, dmask) : 256u + lane;
-        uint32_t peers = __match_any_sync(HP_FULL_MASK, d);
-        uint32_t below = __popc(peers & lt_mask);
-        uint32_t c = valid ? wcnt[d] : 0u;
-        __syncwarp();
-        if (valid && below == 0) wcnt[d] = c + __popc(peers);
-        __syncwarp();
-        rnk[i] = c + below;
-    }
+    for (int i = 0; i < ITEMS; ++i)
+        if (wbase + i * 32 + lane < n) atomicAdd(&s_count[digit_of(key[i], shift, dmask)], 1u);
     __syncthreads();
 
-    // Per digit: offsets of each warp, tile total, and tile-level publication.
     uint32_t total = 0, hval = 0;
     if (tid < 256) {
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            uint32_t c = cnt[w * 256 + tid];
-            cnt[w * 256 + tid] = total;
-            total += c;
-        }
+        total = s_count[tid];
         st_relaxed_u32(&status[(size_t)tile * 256 + tid], (tile == 0 ? ST_FLAG_P : ST_FLAG_A) | total);
         hval = hist[tid];
     }
@@ -165,33 +195,47 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     scan256x2(total, hval, block_start, hist_excl, s_w);
     if (tid < 256) {
         s_block_start[tid] = block_start;
-        uint32_t prefix = 0;
-        if (tile > 0) {
-            int64_t t = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (true) {
-                uint32_t s = ld_relaxed_u32(&status[(size_t)t * 256 + tid]);
-                uint32_t f = s & ~ST_MASK;
-                if (f == 0u) {
-                    if (++spins > LOOKBACK_SPIN_LIMIT) {
-                        hp_report(err, HP_DEV_SPIN_LIMIT, (int)tile);
-                        break;
-                    }
-                    continue;
-                }
-                prefix += s & ST_MASK;
-                if (f == ST_FLAG_P || t == 0) break;
-                --t;
-            }
-            st_relaxed_u32(&status[(size_t)tile * 256 + tid], ST_FLAG_P | (prefix + total));
-        }
+        const uint32_t prefix = lookback(status, tile, tid, err);
+        if (tile > 0) st_relaxed_u32(&status[(size_t)tile * 256 + tid], ST_FLAG_P | (prefix + total));
         s_global[tid] = hist_excl + prefix - block_start;
+    }
+
+    // Rank within the warp: items are visited in index order (round i, then lane).
+    uint32_t* wcnt = cnt + warp * 256;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        const int64_t idx = wbase + i * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? digit_of(key[i], shift, dmask) : 0u;
+        uint32_t peers = __ballot_sync(HP_FULL_MASK, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t bal = __ballot_sync(HP_FULL_MASK, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
+        const uint32_t below = __popc(peers & lt_mask);
+        const uint32_t c = valid ? wcnt[d] : 0u;
+        __syncwarp();
+        if (valid && below == 0) wcnt[d] = c + __popc(peers);
+        __syncwarp();
+        rnk[i] = c + below;
+    }
+    __syncthreads();
+    // Per digit: exclusive offsets of the warps within the tile.
+    if (tid < 256) {
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const uint32_t c = cnt[w * 256 + tid];
+            cnt[w * 256 + tid] = run;
+            run += c;
+        }
     }
     __syncthreads();
     uint32_t pos[ITEMS];
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
-        uint32_t d = digit_of(key[i], shift, dmask);
+        const uint32_t d = digit_of(key[i], shift, dmask);
         pos[i] = s_block_start[d] + cnt[warp * 256 + d] + rnk[i];
     }
     __syncthreads();
@@ -471,8 +515,10 @@ constexpr size_t noalloc_sort_scratch(int64_t n, size_t key_bytes, int tile, int
 constexpr size_t noalloc_max(size_t a, size_t b) { return a > b ? a : b; }
 // Largest sort scratch over both key widths, plus the digit histograms and an error word.
 constexpr size_t NOALLOC_BYTES =
-    noalloc_max(noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 8, 512 * 8, 8),
-                noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 4, 512 * 12, 4)) +
+    noalloc_max(noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 8,
+                                     sort_cfg<uint64_t>::BLOCK * sort_cfg<uint64_t>::ITEMS, 8),
+                noalloc_sort_scratch(HP_NOALLOC_SORT_MAX_KEYS, 4,
+                                     sort_cfg<uint32_t>::BLOCK * sort_cfg<uint32_t>::ITEMS, 4)) +
     noalloc_pad(8 * 256 * 4) + 256;
 
 __device__ __align__(256) unsigned char g_noalloc_sort_scratch[NOALLOC_BYTES];
