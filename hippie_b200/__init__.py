@@ -14,7 +14,8 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (HP_BATCH_NO_GRAPH, HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT,
-                   HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, load)
+                   HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, hp_tune,
+                   load)
 
 __all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "pixel_table",
            "camera_screen_to_world", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
@@ -224,6 +225,36 @@ class Context:
         check(load().hp_gen_primary_rays(self.h, pos.ctypes.data, m.ctypes.data, width, height, max_dist,
                                          sample_index, _ptr(index_to_pixel), _ptr(rays), _stream_ptr(stream)))
         return rays
+
+    _TUNE_FIELDS = ("sort_block", "trace_ctas_per_sm", "trace_stack", "trace_sorted", "ploc_radius",
+                    "ploc_adaptive", "ploc_max_radius", "build_ms", "trace_ms")
+
+    def get_tune(self) -> dict:
+        t = hp_tune()
+        check(load().hp_ctx_get_tune(self.h, C.byref(t)))
+        return {k: getattr(t, k) for k in self._TUNE_FIELDS}
+
+    def set_tune(self, **kw):
+        """Set launch choices (sort_block, trace_ctas_per_sm, trace_stack, trace_sorted); others keep theirs."""
+        t = hp_tune()
+        check(load().hp_ctx_get_tune(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, v)
+        check(load().hp_ctx_set_tune(self.h, C.byref(t)))
+
+    def reset_tune(self):
+        t = hp_tune()
+        load().hp_tune_default(C.byref(t))
+        check(load().hp_ctx_set_tune(self.h, C.byref(t)))
+
+    def autotune(self, verts, tris, rays, params: BuildParams | None = None, ploc_radius=False, stream=None) -> dict:
+        """hp_autotune on this mesh and rays; applies the result-neutral choices, returns all of them."""
+        params = params or BuildParams()
+        m = _mesh(verts, tris)
+        t = hp_tune()
+        check(load().hp_autotune(self.h, C.byref(m), C.byref(params.c), _ptr(rays), rays.shape[0],
+                                 1 if ploc_radius else 0, C.byref(t), _stream_ptr(stream)))
+        return {k: getattr(t, k) for k in self._TUNE_FIELDS}
 
     def adjoint(self, verts, tris, rays, results, dl_dtuv, dl_dverts=None, stream=None):
         import torch

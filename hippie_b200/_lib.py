@@ -40,6 +40,13 @@ class hp_bvh(C.Structure):
                 ("method", C.c_int32), ("ct", C.c_float), ("ci", C.c_float), ("impl", C.c_void_p)]
 
 
+class hp_tune(C.Structure):
+    _fields_ = [("sort_block", C.c_int32), ("trace_ctas_per_sm", C.c_int32), ("trace_stack", C.c_int32),
+                ("trace_sorted", C.c_int32), ("ploc_radius", C.c_int32), ("ploc_adaptive", C.c_int32),
+                ("ploc_max_radius", C.c_int32), ("build_ms", C.c_float), ("trace_ms", C.c_float),
+                ("reserved", C.c_int32 * 7)]
+
+
 class hp_build_taps(C.Structure):
     _fields_ = [("morton_keys", C.c_void_p), ("sorted_keys", C.c_void_p), ("sorted_refs", C.c_void_p),
                 ("node_parent", C.c_void_p), ("node_left", C.c_void_p), ("node_right", C.c_void_p),
@@ -84,6 +91,11 @@ _SIGS = {
     "hp_camera_screen_to_world": (C.c_int, [_P, _P, C.c_float, C.c_int32, C.c_int32, C.c_float, C.c_float, _P]),
     "hp_gen_primary_rays": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_int32, _P, _P, _P]),
     "hp_ray_keys": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int32, _P, _P]),
+    "hp_tune_default": (None, [C.POINTER(hp_tune)]),
+    "hp_ctx_set_tune": (C.c_int, [_P, C.POINTER(hp_tune)]),
+    "hp_ctx_get_tune": (C.c_int, [_P, C.POINTER(hp_tune)]),
+    "hp_autotune": (C.c_int, [_P, C.POINTER(hp_mesh), C.POINTER(hp_build_params), _P, C.c_int64, C.c_uint32,
+                              C.POINTER(hp_tune), _P]),
     "hp_radix_sort": (C.c_int, [_P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P]),
     "hp_radix_sort_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "hp_env_create": (C.c_int, [C.POINTER(C.c_void_p)]),

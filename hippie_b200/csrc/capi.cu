@@ -481,6 +481,9 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
     if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_trace: null argument");
     if (num_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace: negative ray count");
     if (num_rays > 0 && (!rays || !results)) return hp_fail(HP_ERR_ARG, "hp_trace: null ray or result buffer");
+    // A context tuned for it traces large batches in ray Morton order (same results).
+    if (ctx->tune.trace_sorted && num_rays >= 65536 && num_rays < (int64_t(1) << 30))
+        return hp_trace_sorted(ctx, bvh, rays, num_rays, results, stats, flags, 30, nullptr, stream);
     return hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays,
                            num_rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -505,7 +508,7 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
     if (n == 0) return HP_OK;
     if (!keys_in || !keys_out || !vals_out) return hp_fail(HP_ERR_ARG, "hp_radix_sort: null buffer");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    hp_sort_plan plan = hp_sort_make_plan(n, key_bytes, bits);
+    hp_sort_plan plan = hp_sort_make_plan(n, key_bytes, bits, ctx->tune.sort_block);
     const size_t hist_bytes = hp_carve::pad(hp_sort_hist_bytes(plan.passes));
     HP_TRY(hp_ctx_reserve(ctx, hp_carve::pad(plan.scratch_bytes) + hist_bytes, s));
     hp_carve cv(ctx->arena);

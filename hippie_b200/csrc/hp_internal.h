@@ -60,6 +60,7 @@ struct hp_ctx {
     hp_prof_mark* marks = nullptr; // event pool
     int num_marks = 0;
     int cap_marks = 0;
+    hp_tune tune{512, 0, 16, 0, 0, 0, 0, 0.0f, 0.0f, {0}};  // launch choices (hp_ctx_set_tune)
 };
 
 // Record a phase boundary on the stream when profiling is enabled.
@@ -92,8 +93,9 @@ struct hp_sort_plan {
     int tile = 0;
     int64_t tiles = 0;
     size_t scratch_bytes = 0;      // keys/vals ping-pong + histograms + status
+    int block = 512;               // threads per pass CTA: 512 or 256
 };
-hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits);
+hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block = 512);
 // Histograms [passes][256] (uint32) must be zero before the first key is
 // counted; hp_sort_run zeroes them itself unless hist_ready is set, in which
 // case the caller has already filled them (the Morton kernel does).

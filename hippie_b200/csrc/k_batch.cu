@@ -453,16 +453,17 @@ struct hp_batch {
     int32_t* g_stats = nullptr;
     uint32_t g_flags = 0;
     int g_mode = -1;                     // 0 build, 1 trace, 2 both
-    const hp_ctx* g_ctx = nullptr;       // context and scratch arena the graph was captured with
+    const hp_ctx* g_ctx = nullptr;       // context, scratch arena and launch choices of the capture
     const char* g_arena = nullptr;
+    int g_tune[4] = {0, 0, 0, 0};
     int64_t graph_launches = 0;
 };
 
 namespace {
 
-size_t batch_scratch(const hp_batch& b, hp_sort_plan& plan) {
+size_t batch_scratch(const hp_batch& b, hp_sort_plan& plan, int sort_block) {
     const int64_t N = std::max<int64_t>(b.N, 1), NN = std::max<int64_t>(b.NN, 1);
-    plan = hp_sort_make_plan(N, 8, b.key_bits);
+    plan = hp_sort_make_plan(N, 8, b.key_bits, sort_block);
     size_t need = 0;
     need += 2 * hp_carve::pad(N * 16);                 // triangle boxes
     need += 2 * hp_carve::pad(N * 8);                  // keys, sorted keys
@@ -482,7 +483,7 @@ hp_status batch_build_seq(hp_ctx* ctx, hp_batch* b, cudaStream_t s) {
         return HP_OK;
     }
     hp_sort_plan plan;
-    batch_scratch(*b, plan);
+    batch_scratch(*b, plan, ctx->tune.sort_block);
     hp_carve cv(ctx->arena);
     const int64_t N = b->N, NN = b->NN;
     bargs B{};
@@ -597,7 +598,9 @@ hp_status batch_run(hp_ctx* ctx, hp_batch* b, int mode, const float* rays, int32
     if (s == nullptr) return hp_fail(HP_ERR_ARG, "batched launches from a CUDA graph need a non-default stream");
     const uint32_t gflags = flags & (HP_TRACE_ANY_HIT | HP_TRACE_STATS);
     if (!b->exec || b->g_mode != mode || b->g_rays != rays || b->g_results != results || b->g_stats != stats ||
-        b->g_flags != gflags || b->g_ctx != ctx || b->g_arena != ctx->arena) {
+        b->g_flags != gflags || b->g_ctx != ctx || b->g_arena != ctx->arena ||
+        b->g_tune[0] != ctx->tune.sort_block || b->g_tune[1] != ctx->tune.trace_ctas_per_sm ||
+        b->g_tune[2] != ctx->tune.trace_stack) {
         drop_graph(b);
         cudaGraph_t graph = nullptr;
         HP_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -623,6 +626,9 @@ hp_status batch_run(hp_ctx* ctx, hp_batch* b, int mode, const float* rays, int32
         b->g_flags = gflags;
         b->g_ctx = ctx;
         b->g_arena = ctx->arena;
+        b->g_tune[0] = ctx->tune.sort_block;
+        b->g_tune[1] = ctx->tune.trace_ctas_per_sm;
+        b->g_tune[2] = ctx->tune.trace_stack;
         hp_count_launch(-(int)b->graph_launches);  // counted when the graph runs
     }
     HP_CUDA(cudaGraphLaunch(b->exec, s));
@@ -718,9 +724,10 @@ hp_status hp_batch_create(hp_ctx* ctx, const hp_mesh* meshes, int32_t num_meshes
         v.capacity = b->segs[m].n;
         v.view = true;
     }
-    // reserve the scratch now: nothing may allocate inside a graph capture
+    // reserve the scratch now (for either sort CTA size): nothing may allocate
+    // inside a graph capture
     hp_sort_plan plan;
-    b->scratch = batch_scratch(*b, plan);
+    b->scratch = std::max(batch_scratch(*b, plan, 512), batch_scratch(*b, plan, 256));
     const hp_status st = hp_ctx_reserve(ctx, b->scratch, nullptr);
     if (st != HP_OK) {
         hp_batch_destroy(b);

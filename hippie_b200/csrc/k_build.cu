@@ -392,7 +392,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                  const hp_build_taps* taps, cudaStream_t s) {
     const int64_t n = m->num_triangles;
     const int bits = p->morton_bits;
-    const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits);
+    const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits, ctx->tune.sort_block);
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
     const bool atr = p->method == HP_METHOD_ATR;

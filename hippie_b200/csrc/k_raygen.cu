@@ -283,7 +283,7 @@ extern "C" hp_status hp_trace_sorted(hp_ctx* ctx, const hp_bvh* bvh, const float
     if (num_rays >= (int64_t(1) << 30)) return hp_fail(HP_ERR_ARG, "hp_trace_sorted: too many rays");
     if (num_rays == 0) return HP_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const hp_sort_plan plan = hp_sort_make_plan(num_rays, 8, bits);
+    const hp_sort_plan plan = hp_sort_make_plan(num_rays, 8, bits, ctx->tune.sort_block);
     size_t need = 2 * hp_carve::pad(num_rays * 8) + hp_carve::pad(num_rays * 4) + hp_carve::pad(plan.scratch_bytes) +
                   hp_carve::pad(hp_sort_hist_bytes(plan.passes));
     HP_TRY(hp_ctx_reserve(ctx, need, s));

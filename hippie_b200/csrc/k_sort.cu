@@ -257,21 +257,23 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     }
 }
 
+// Keys per thread of a pass; the CTA size (512 by default, 256 as a tuning
+// choice) is chosen at run time.
 template <typename K> struct sort_cfg;
 template <> struct sort_cfg<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 12; };
 template <> struct sort_cfg<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
 
-template <typename K>
+template <typename K, int BLOCK>
 constexpr size_t onesweep_smem() {
-    constexpr int TILE = sort_cfg<K>::BLOCK * sort_cfg<K>::ITEMS;
-    constexpr size_t a = (size_t)(sort_cfg<K>::BLOCK / 32) * 256 * 4;
+    constexpr int TILE = BLOCK * sort_cfg<K>::ITEMS;
+    constexpr size_t a = (size_t)(BLOCK / 32) * 256 * 4;
     constexpr size_t b = (size_t)TILE * (sizeof(K) + 4);
     return a > b ? a : b;
 }
 
-template <typename K>
+template <typename K, int BLOCK>
 hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream_t stream) {
-    constexpr int BLOCK = sort_cfg<K>::BLOCK, ITEMS = sort_cfg<K>::ITEMS;
+    constexpr int ITEMS = sort_cfg<K>::ITEMS;
     const int64_t n = plan.n;
     hp_carve cv(reinterpret_cast<char*>(a.scratch));
     K* kA = cv.take<K>(n);
@@ -290,7 +292,7 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
         hp_count_launch();
         hp_mark(a.ctx, stream, "sort_hist");
     }
-    constexpr size_t smem = onesweep_smem<K>();
+    constexpr size_t smem = onesweep_smem<K, BLOCK>();
     HP_CUDA(cudaFuncSetAttribute(k_onesweep<K, BLOCK, ITEMS>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const K* kin = reinterpret_cast<const K*>(a.keys_in);
@@ -446,14 +448,14 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_lb(
 
 }  // namespace
 
-hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits) {
+hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block) {
     hp_sort_plan p;
     p.n = n;
     p.key_bytes = key_bytes;
     p.bits = bits;
     p.passes = (bits + 7) / 8;
-    p.tile = key_bytes == 4 ? sort_cfg<uint32_t>::BLOCK * sort_cfg<uint32_t>::ITEMS
-                            : sort_cfg<uint64_t>::BLOCK * sort_cfg<uint64_t>::ITEMS;
+    p.block = block == 256 ? 256 : 512;
+    p.tile = p.block * (key_bytes == 4 ? sort_cfg<uint32_t>::ITEMS : sort_cfg<uint64_t>::ITEMS);
     p.tiles = std::max<int64_t>(1, (n + p.tile - 1) / p.tile);
     size_t kv = hp_carve::pad((size_t)n * key_bytes) + hp_carve::pad((size_t)n * 4);
     p.scratch_bytes = 2 * kv + hp_carve::pad(((size_t)p.passes * p.tiles * 256 + 64) * 4);
@@ -466,8 +468,12 @@ hp_status hp_sort_run(const hp_sort_plan& plan, const hp_sort_args& a, cudaStrea
     if (plan.n <= 0) return HP_OK;
     if (plan.n >= (int64_t(1) << 30))
         return hp_fail(HP_ERR_ARG, "radix sort: n must be below 2^30");
-    if (plan.key_bytes == 4) return sort_run_t<uint32_t>(plan, a, stream);
-    return sort_run_t<uint64_t>(plan, a, stream);
+    if (plan.block == 256) {
+        if (plan.key_bytes == 4) return sort_run_t<uint32_t, 256>(plan, a, stream);
+        return sort_run_t<uint64_t, 256>(plan, a, stream);
+    }
+    if (plan.key_bytes == 4) return sort_run_t<uint32_t, 512>(plan, a, stream);
+    return sort_run_t<uint64_t, 512>(plan, a, stream);
 }
 
 size_t hp_scan2_scratch_bytes(int64_t n) {

@@ -8,7 +8,8 @@
 // fewer than 20 lanes of a warp still traverse.
 //
 // Differences by design:
-//   * the traversal stack is split: its first 16 entries live in shared memory
+//   * the traversal stack (64 entries) is split: its first SST entries (16 by
+//     default; 8 or 32 as a tuning choice) live in shared memory
 //     (bank-conflict-free, one column per thread), deeper entries in local memory;
 //   * every floating-point step is written out (fma, IEEE reciprocal), so a CPU
 //     restatement of the per-ray algorithm reproduces the results bit for bit;
@@ -23,8 +24,7 @@
 namespace {
 
 constexpr int TRACE_BLOCK = 128;
-constexpr int SSTACK = 16;        // shared-memory stack entries per thread
-constexpr int LSTACK = 48;        // local-memory overflow entries per thread
+constexpr int STACK = 64;         // traversal stack entries per ray: SST in shared memory, the rest local
 constexpr int SENTINEL = 0x76543210;
 constexpr int FETCH_THRESHOLD = 20;
 constexpr int TRAVERSAL_LIMIT = 1 << 22;  // visits per ray before the ray is abandoned with an error
@@ -63,13 +63,14 @@ __device__ __forceinline__ int seg_search(const int64_t* __restrict__ off, int n
 
 // BATCH: rays of many meshes in one launch; ray g belongs to the segment whose
 // ray range holds it, and the lane traverses that mesh's BVH.
-template <bool ANY_HIT, bool STATS, bool BATCH>
+template <bool ANY_HIT, bool STATS, bool BATCH, int SST>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace(
     const float4* __restrict__ rays, int64_t num_rays, int4* __restrict__ results,
     int2* __restrict__ stats, const float4* __restrict__ nodes_all, const float4* __restrict__ woop_all,
     const int32_t* __restrict__ tri_all, int max_nodes_all, int num_refs_all,
     unsigned long long* ray_counter, int* err, const hp_batch_seg* __restrict__ segs,
     const int64_t* __restrict__ ray_off, int num_segs, const int32_t* __restrict__ order) {
+    constexpr int SSTACK = SST, LSTACK = STACK - SST;
     __shared__ int s_stack[SSTACK * TRACE_BLOCK];
     int* sstack = s_stack + threadIdx.x;
     int lstack[LSTACK];
@@ -281,16 +282,22 @@ __global__ void k_trace_empty(const float4* rays, int64_t num_rays, int4* result
     if (stats) stats[i] = make_int2(0, 0);
 }
 
-template <bool A, bool S>
+// Persistent grid: the tuned CTAs per SM, or as many as fit.
+int trace_grid(const hp_ctx* ctx, int per_sm, int64_t num_rays) {
+    int k = std::max(per_sm, 1);
+    if (ctx->tune.trace_ctas_per_sm > 0) k = std::min(k, (int)ctx->tune.trace_ctas_per_sm);
+    const int64_t grid = std::min<int64_t>((int64_t)ctx->sm_count * k, (num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
+    return (int)std::max<int64_t>(grid, 1);
+}
+
+template <bool A, bool S, int SST>
 hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                    int64_t num_rays, int32_t* results, int32_t* stats, unsigned long long* counter,
                    const int32_t* order, cudaStream_t s) {
     int per_sm = 0;
-    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, false>, TRACE_BLOCK, 0));
-    int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
-    grid = std::min<int64_t>(grid, (num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, false, SST>, TRACE_BLOCK, 0));
     const int max_nodes = (int)std::max<int64_t>(2 * b->capacity - 1, 3);
-    k_trace<A, S, false><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
+    k_trace<A, S, false, SST><<<trace_grid(ctx, per_sm, num_rays), TRACE_BLOCK, 0, s>>>(
         reinterpret_cast<const float4*>(rays), num_rays, reinterpret_cast<int4*>(results),
         reinterpret_cast<int2*>(stats), reinterpret_cast<const float4*>(b->nodes), b->woop, b->tri_idx,
         max_nodes, (int)n_refs, counter, ctx->d_status, nullptr, nullptr, 0, order);
@@ -301,18 +308,36 @@ hp_status launch_t(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const floa
 }
 
 template <bool A, bool S>
+hp_status launch_st(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                    int64_t num_rays, int32_t* results, int32_t* stats, unsigned long long* counter,
+                    const int32_t* order, cudaStream_t s) {
+    switch (ctx->tune.trace_stack) {
+        case 8: return launch_t<A, S, 8>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+        case 32: return launch_t<A, S, 32>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+        default: return launch_t<A, S, 16>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    }
+}
+
+template <bool A, bool S, int SST>
 hp_status launch_batch_t(hp_ctx* ctx, const hp_batch_trace_args& t, unsigned long long* counter, cudaStream_t s) {
     int per_sm = 0;
-    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, true>, TRACE_BLOCK, 0));
-    int64_t grid = (int64_t)ctx->sm_count * std::max(per_sm, 1);
-    grid = std::min<int64_t>(grid, (t.num_rays + TRACE_BLOCK - 1) / TRACE_BLOCK);
-    k_trace<A, S, true><<<(unsigned)std::max<int64_t>(grid, 1), TRACE_BLOCK, 0, s>>>(
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<A, S, true, SST>, TRACE_BLOCK, 0));
+    k_trace<A, S, true, SST><<<trace_grid(ctx, per_sm, t.num_rays), TRACE_BLOCK, 0, s>>>(
         reinterpret_cast<const float4*>(t.rays), t.num_rays, reinterpret_cast<int4*>(t.results),
         reinterpret_cast<int2*>(t.stats), reinterpret_cast<const float4*>(t.nodes), t.woop, t.tri_idx, 0, 0,
         counter, ctx->d_status, t.segs, t.ray_off, t.num_segs, nullptr);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     return HP_OK;
+}
+
+template <bool A, bool S>
+hp_status launch_batch_st(hp_ctx* ctx, const hp_batch_trace_args& t, unsigned long long* counter, cudaStream_t s) {
+    switch (ctx->tune.trace_stack) {
+        case 8: return launch_batch_t<A, S, 8>(ctx, t, counter, s);
+        case 32: return launch_batch_t<A, S, 32>(ctx, t, counter, s);
+        default: return launch_batch_t<A, S, 16>(ctx, t, counter, s);
+    }
 }
 
 }  // namespace
@@ -322,10 +347,10 @@ hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint3
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
     HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && t.stats;
-    if (any && st) return launch_batch_t<true, true>(ctx, t, counter, s);
-    if (any) return launch_batch_t<true, false>(ctx, t, counter, s);
-    if (st) return launch_batch_t<false, true>(ctx, t, counter, s);
-    return launch_batch_t<false, false>(ctx, t, counter, s);
+    if (any && st) return launch_batch_st<true, true>(ctx, t, counter, s);
+    if (any) return launch_batch_st<true, false>(ctx, t, counter, s);
+    if (st) return launch_batch_st<false, true>(ctx, t, counter, s);
+    return launch_batch_st<false, false>(ctx, t, counter, s);
 }
 
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
@@ -344,8 +369,8 @@ hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, con
     HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     hp_mark(ctx, s, "trace_begin");
     const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && stats;
-    if (any && st) return launch_t<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
-    if (any) return launch_t<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
-    if (st) return launch_t<false, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
-    return launch_t<false, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    if (any && st) return launch_st<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    if (any) return launch_st<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    if (st) return launch_st<false, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
+    return launch_st<false, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
 }

@@ -230,6 +230,41 @@ hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays,
                            const int32_t* results, const float* dl_dtuv, int64_t num_rays,
                            float* dl_dvertices, void* stream);
 
+/* ---- tuning ---------------------------------------------------------------- */
+/* Launch choices of a context. The first four never change a result: they are
+ * the sort's CTA size (its tile), the tracer's persistent CTAs per SM (warps
+ * per SM = 4 x that) and shared-memory stack depth, and tracing in ray Morton
+ * order. The PLOC radius fields report the schedule hp_autotune measured best;
+ * it changes the tree, so it is applied only by the caller (hp_build_params).
+ * New: the reference has no tuner. */
+typedef struct hp_tune {
+    int32_t sort_block;        /* threads per radix-sort CTA: 512 (default) or 256 */
+    int32_t trace_ctas_per_sm; /* persistent tracer CTAs of 128 threads per SM; 0 = as many as fit */
+    int32_t trace_stack;       /* traversal stack entries per ray kept in shared memory: 8, 16 (default), 32 */
+    int32_t trace_sorted;      /* 1: hp_trace traces in ray Morton order (30-bit keys, as hp_trace_sorted) */
+    int32_t ploc_radius;       /* hp_autotune: best PLOC radius found (0 = not tuned) */
+    int32_t ploc_adaptive;     /* hp_autotune: 1 if the adaptive schedule was best */
+    int32_t ploc_max_radius;   /* hp_autotune: the schedule's maximum radius */
+    float build_ms;            /* hp_autotune: build time with the chosen settings */
+    float trace_ms;            /* hp_autotune: trace time of the ray sample with the chosen settings */
+    int32_t reserved[7];
+} hp_tune;
+#define HP_TUNE_PLOC_RADIUS 1u     /* hp_autotune flag: also compare PLOC radius schedules */
+void hp_tune_default(hp_tune* t);
+/* Set / read the context's launch choices (validated; HP_ERR_ARG if out of range). */
+hp_status hp_ctx_set_tune(hp_ctx* ctx, const hp_tune* t);
+hp_status hp_ctx_get_tune(hp_ctx* ctx, hp_tune* t);
+/* Time the launch choices on the caller's mesh and rays (a sample of at most
+ * 2^21 rays): sort CTA size on the build, then stack depth x CTAs per SM x
+ * Morton order on the trace, each by CUDA events (median of three runs). The
+ * fastest result-neutral choices are applied to the context and written to
+ * *out; with HP_TUNE_PLOC_RADIUS and a PLOC method, the radius schedules
+ * {8, 16, 32 fixed; adaptive from 4 up to 64} are also compared by build time
+ * plus the sample's trace time scaled to num_rays, and the best is reported
+ * in *out (not applied). Synchronous; allocates a temporary BVH and buffers. */
+hp_status hp_autotune(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, const float* rays,
+                      int64_t num_rays, uint32_t flags, hp_tune* out, void* stream);
+
 /* ---- batches of meshes ---------------------------------------------------- */
 /* Many independent meshes of uneven size built (LBVH) and traced in a fixed
  * number of launches, replayed from a CUDA graph. New entry points with no

@@ -66,3 +66,13 @@ def test_generators_deterministic():
     assert np.abs(vh[:, 2]).max() <= 16 * 0.05
     rg = hp.gen.rays_grid_down(1, 8, 8)
     assert np.all(rg[:, 6] == -1) and np.all(rg[:, 2] == 1)
+
+
+def test_tune_defaults():
+    """hp_tune_default: the launch choices every context starts from (host only)."""
+    import ctypes as C
+    t = _lib.hp_tune()
+    _lib.load().hp_tune_default(C.byref(t))
+    assert (t.sort_block, t.trace_ctas_per_sm, t.trace_stack, t.trace_sorted) == (512, 0, 16, 0)
+    assert (t.ploc_radius, t.ploc_adaptive, t.ploc_max_radius) == (0, 0, 0)
+    assert C.sizeof(t) == 64
