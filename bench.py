@@ -478,6 +478,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one build and one trace, then print the phase times (for profiler runs)")
+    ap.add_argument("--tune", type=int, default=1, help="run the autotuner and report its trace rate")
     ap.add_argument("--extras", type=int, default=1,
                     help="also measure the batched (2048 meshes) and differentiable (heightfield) workloads")
     ap.add_argument("--rays", type=int, default=0, help="override the workload's ray count (profiling)")
@@ -582,6 +583,29 @@ def main(argv=None):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         sorted_ms = tt.item()
 
+    # ---- the autotuner on this workload: its choices and the trace rate they give ----
+    tuned = None
+    if args.tune:
+        t0 = time.perf_counter()
+        choice = ctx.autotune(V, T, R, params, ploc_radius=True)
+        tune_s = time.perf_counter() - t0
+        ctx.trace(bvh, R, results=RES)
+        evt = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+        for k in range(args.steps):
+            evt[k][0].record(stream)
+            ctx.trace(bvh, R, results=RES)
+            evt[k][1].record(stream)
+        torch.cuda.synchronize()
+        ctx.check()
+        tuned_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evt]))
+        if world > 1:
+            tt = torch.tensor([tuned_ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tuned_ms = tt.item()
+        ctx.reset_tune()
+        tuned = {"choice": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in choice.items()},
+                 "trace_mrays_s": world * nr / (tuned_ms * 1e-3) / 1e6, "tuning_s": tune_s}
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e_b, e2e_t = [], []
     for k in range(max(3, args.steps // 2)):
@@ -640,6 +664,7 @@ def main(argv=None):
                    "l2": "inputs larger than L2 (mesh 200 MB, rays 512 MB)"},
         "trace_mrays_s": world * nr / (trace_ms * 1e-3) / 1e6,
         "trace_sorted_mrays_s": world * nr / (sorted_ms * 1e-3) / 1e6,
+        "autotuned": tuned,
         "build_ms": build_ms, "trace_ms": trace_ms,
         "phases_ms": {k: round(x, 4) for k, x in phases.items()},
         "e2e": {"value": world * n / e2e_b_s / 1e6, "unit": "Mtris/s",
