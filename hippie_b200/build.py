@@ -25,6 +25,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libhippie_b200.so"
+CLI_SRC = PKG / "cli" / "bench_main.cpp"
+CLI = PKG / "hippie_b200_bench"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -87,7 +89,24 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         os.replace(tmp, LIB)
         if verbose:
             print(f"built {LIB}")
+    _build_cli(force, verbose)
     return LIB
+
+
+def _build_cli(force: bool, verbose: bool) -> None:
+    """The C++ bench CLI (hippie_b200_bench) over the C++ facade of the C ABI."""
+    deps = [CLI_SRC, LIB, INCLUDE / "hippie_b200.hpp", INCLUDE / "hippie_b200.h"]
+    if not force and CLI.exists() and CLI.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return
+    cuda = Path(_cuda_include()).parent
+    cmd = ["g++", "-std=c++17", "-O2", "-I", str(INCLUDE), "-I", _cuda_include(), str(CLI_SRC), "-o", str(CLI),
+           "-L", str(PKG), "-lhippie_b200", "-L", str(cuda / "lib64"), "-lcudart_static", "-ldl", "-lrt",
+           "-lpthread", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"CLI build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if verbose:
+        print(f"built {CLI}")
 
 
 def main(argv=None) -> int:
