@@ -30,14 +30,13 @@
 // reference's fast-math build contracts to 2*fma(y, z, fma(x, y, x*z)).
 //
 // Collapse. A final climb evaluates computeNodeStatesAdaptive
-// (BVHCollapserKernels.cu:58-136) on the final topology, the per-subtree counts
-// of surviving interior nodes and collapsed leaves, and for every node the
-// smallest sorted position below it (minpos) and how many nodes below it share
-// that minpos (below). Ordering nodes by (minpos, -size) is a preorder in which
-// each node's child holding the smaller position comes first, so parents
-// precede children; its rank is base[minpos] + chain[minpos] - 1 - below with
-// base the exclusive sum of the chain lengths. The depth-first collapse kernel
-// then walks nodes in that order, which lets every node wait for its parent.
+// (BVHCollapserKernels.cu:58-136) on the final topology and the per-subtree
+// counts of surviving interior nodes and collapsed leaves. The depth-first
+// collapse kernel then processes the nodes in an order where every parent
+// comes first, so that each node can wait for its parent's record: interior
+// nodes by decreasing subtree size (a radix sort of n - size), then the leaves.
+// A parent is larger than its children and usually far larger, so the waits
+// rarely chain. The output is numbered in left-first preorder.
 #include <algorithm>
 #include <cuda_runtime.h>
 #include "hp_device.cuh"
@@ -330,8 +329,6 @@ struct fin_args {
     int* counters;
     uint8_t* state;
     int2* counts;   // surviving interior nodes, collapsed leaves
-    int2* key;      // minpos, below
-    int* chain;     // [n]: nodes whose minpos is the index
     const int32_t* sorted_tri;
     const float4* tbmin;
     const float4* tbmax;
@@ -339,7 +336,7 @@ struct fin_args {
 };
 
 // computeSizes + computeNodeStatesAdaptive / computeNodeStates on the final
-// topology, plus the counts and ordering keys of the collapse.
+// topology, plus the per-subtree counts of the collapse.
 __global__ void __launch_bounds__(256) k_atr_finish(fin_args F) {
     const int p = blockIdx.x * 256 + threadIdx.x;
     const int n = F.n;
@@ -360,7 +357,6 @@ __global__ void __launch_bounds__(256) k_atr_finish(fin_args F) {
     __stcg(F.nbmax + leaf, make_float4(mx.x, mx.y, mx.z, __int_as_float(1)));
     F.state[leaf] = 0;
     __stcg(F.counts + leaf, make_int2(0, 1));
-    __stcg(F.key + leaf, make_int2(p, 0));
     int node = __ldcg(F.parent + leaf);
     int guard = 0;
     while (node >= 0) {
@@ -394,31 +390,25 @@ __global__ void __launch_bounds__(256) k_atr_finish(fin_args F) {
             c = 0.0f;
         }
         const int2 cl = __ldcg(F.counts + l), cr = __ldcg(F.counts + r);
-        const int2 kl = __ldcg(F.key + l), kr = __ldcg(F.key + r);
-        const bool lmin = kl.x < kr.x;
-        const int2 kmin = lmin ? kl : kr, kother = lmin ? kr : kl;
-        F.chain[kother.x] = kother.y + 1;  // the other child ends its chain
         __stcg(F.nbmin + node, make_float4(mnx, mny, mnz, c));
         __stcg(F.nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
         F.state[node] = (uint8_t)st;
         __stcg(F.counts + node, st ? make_int2(1 + cl.x + cr.x, cl.y + cr.y) : make_int2(0, 1));
-        __stcg(F.key + node, make_int2(kmin.x, kmin.y + 1));
-        if (node == 0) F.chain[kmin.x] = kmin.y + 2;
         node = __ldcg(F.parent + node);
     }
 }
 
-// order[rank(v)] = v with rank(v) = base[minpos] + chain[minpos] - 1 - below.
-__global__ void __launch_bounds__(256) k_atr_order(int n, const int2* __restrict__ key,
-                                                   const int* __restrict__ chain, const int* __restrict__ base,
-                                                   int* order, int* err) {
+// Sort keys of the interior nodes: n - size, so that a stable ascending sort
+// lists larger subtrees first.
+__global__ void __launch_bounds__(256) k_size_keys(int n, const float4* __restrict__ nbmax, uint32_t* keys) {
     const int v = blockIdx.x * 256 + threadIdx.x;
-    if (v >= 2 * n - 1) return;
-    const int2 k = key[v];
-    if ((unsigned)k.x >= (unsigned)n) { hp_report(err, HP_DEV_BAD_INDEX, v); return; }
-    const int r = base[k.x] + chain[k.x] - 1 - k.y;
-    if ((unsigned)r >= (unsigned)(2 * n - 1) || k.y >= chain[k.x]) { hp_report(err, HP_DEV_BAD_INDEX, v); return; }
-    order[r] = v;
+    if (v >= n - 1) return;
+    keys[v] = (uint32_t)(n - __float_as_int(__ldg(&nbmax[v].w)));
+}
+
+__global__ void __launch_bounds__(256) k_leaf_order(int n, int* order) {
+    const int p = blockIdx.x * 256 + threadIdx.x;
+    if (p < n) order[n - 1 + p] = n - 1 + p;
 }
 
 }  // namespace
@@ -427,10 +417,11 @@ size_t hp_atr_scratch_bytes(int64_t n) {
     const int64_t nn = 2 * n - 1;
     size_t b = 0;
     b += hp_carve::pad(nn);                        // state
-    b += 2 * hp_carve::pad(nn * 8);                // counts, key
-    b += 2 * hp_carve::pad(n * 4);                 // chain, base
+    b += hp_carve::pad(nn * 8);                    // counts
+    b += 2 * hp_carve::pad(n * 4);                 // size keys, sorted keys
     b += hp_carve::pad(nn * 4);                    // order
-    b += hp_scan2_scratch_bytes(n);
+    const hp_sort_plan plan = hp_sort_make_plan(n, 4, 32);
+    b += hp_carve::pad(plan.scratch_bytes) + hp_carve::pad(hp_sort_hist_bytes(plan.passes));
     b += hp_topdown_scratch_bytes(n);
     return b;
 }
@@ -446,11 +437,15 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
     hp_carve cv(reinterpret_cast<char*>(scratch));
     uint8_t* state = cv.take<uint8_t>(nn);
     int2* counts = cv.take<int2>(nn);
-    int2* key = cv.take<int2>(nn);
-    int* chain = cv.take<int>(n);
-    int* base = cv.take<int>(n);
+    uint32_t* keys = cv.take<uint32_t>(n);
+    uint32_t* skeys = cv.take<uint32_t>(n);
     int* order = cv.take<int>(nn);
-    void* scan = cv.take<char>(hp_scan2_scratch_bytes(n));
+    int bits = 1;
+    while ((int64_t(1) << bits) <= n) ++bits;
+    const hp_sort_plan plan = hp_sort_make_plan(n - 1, 4, bits, 512);
+    const hp_sort_plan pmax = hp_sort_make_plan(n, 4, 32);
+    void* sort_scratch = cv.take<char>(pmax.scratch_bytes);
+    uint32_t* hist = cv.take<uint32_t>(pmax.passes * 256);
     void* td_scratch = cv.take<char>(hp_topdown_scratch_bytes(n));
     int* err = ctx->d_status;
 
@@ -466,23 +461,26 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
         k_atr_iter<<<hp_div_up(n, AB), AB, 0, s>>>(A);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
+        hp_mark(ctx, s, "atr_iteration");
         ++runs;
         gamma *= 2;
         if (gamma > n) break;
     }
-    hp_mark(ctx, s, "atr");
     fin_args F{};
     F.n = n; F.init = runs == 0; F.adaptive = p->adaptive_leaf; F.max_leaf = p->max_leaf_size;
     F.ct = p->ct; F.ci = p->ci; F.left = left; F.right = right; F.parent = parent; F.nbmin = nbmin;
-    F.nbmax = nbmax; F.counters = counters; F.state = state; F.counts = counts; F.key = key; F.chain = chain;
+    F.nbmax = nbmax; F.counters = counters; F.state = state; F.counts = counts;
     F.sorted_tri = sorted_tri; F.tbmin = tbmin; F.tbmax = tbmax; F.err = err;
     HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
     k_atr_finish<<<hp_div_up(n, 256), 256, 0, s>>>(F);
     HP_CUDA(cudaGetLastError());
-    hp_scan2_sum(chain, n, nullptr, 0, base, nullptr, nullptr, scan, err, s);
-    k_atr_order<<<hp_div_up(nn, 256), 256, 0, s>>>(n, key, chain, base, order, err);
+    hp_mark(ctx, s, "atr_finish");
+    k_size_keys<<<hp_div_up(n, 256), 256, 0, s>>>(n, nbmax, keys);
+    k_leaf_order<<<hp_div_up(n, 256), 256, 0, s>>>(n, order);
     HP_CUDA(cudaGetLastError());
     hp_count_launch(2);
+    hp_sort_args sa{keys, nullptr, skeys, order, sort_scratch, hist, false, err, nullptr};
+    HP_TRY(hp_sort_run(plan, sa, s));
     hp_topdown_in in{};
     in.n = n; in.left = left; in.right = right; in.parent = parent; in.counts = counts; in.state = state;
     in.nbmin = nbmin; in.nbmax = nbmax; in.order = order; in.sorted_tri = sorted_tri;
