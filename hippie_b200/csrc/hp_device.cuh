@@ -32,6 +32,15 @@ __device__ __forceinline__ void hp_report(int* status, int code, int info) {
     }
 }
 
+// Arrival at a node in a bottom-up climb: returns the count before this
+// arrival. The add is acq_rel at GPU scope, so the second thread to arrive sees
+// every write the first one made before its arrival.
+__device__ __forceinline__ int hp_arrive(int* counter) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
+}
+
 // ---- float <-> order-preserving uint (for atomicMin/atomicMax on floats) ----
 __device__ __forceinline__ uint32_t hp_f2ord(float f) {
     uint32_t u = __float_as_uint(f);

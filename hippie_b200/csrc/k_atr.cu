@@ -108,6 +108,26 @@ __device__ __forceinline__ float area_of(const box6& b) {
     return atr_area(b.mn[0], b.mn[1], b.mn[2], b.mx[0], b.mx[1], b.mx[2]);
 }
 
+// Per-warp treelet state in shared memory: the slots being merged (box, cost,
+// refs, node), the record of the internal node made at each merge step, and the
+// packed lower triangle of pairwise union areas.
+struct atr_smem {
+    float4 lo[TMAX];   // slot: min corner, cost
+    float4 hi[TMAX];   // slot: max corner, refs (int bits)
+    int node[TMAX];
+    float4 olo[TMAX];  // record of merge step k: min corner, cost
+    float4 ohi[TMAX];  // max corner, refs (int bits)
+    int2 okids[TMAX];  // children
+    float d[DMAX];
+};
+
+__device__ __forceinline__ box6 box_of(const float4& lo, const float4& hi) {
+    box6 b;
+    b.mn[0] = lo.x; b.mn[1] = lo.y; b.mn[2] = lo.z;
+    b.mx[0] = hi.x; b.mx[1] = hi.y; b.mx[2] = hi.z;
+    return b;
+}
+
 __device__ __forceinline__ void load_node(const atr_args& A, int v, box6& b, float& cost, int& refs) {
     const float4 mn = __ldcg(A.nbmin + v), mx = __ldcg(A.nbmax + v);
     b.mn[0] = mn.x; b.mn[1] = mn.y; b.mn[2] = mn.z;
@@ -119,26 +139,35 @@ __device__ __forceinline__ void load_node(const atr_args& A, int v, box6& b, flo
 __device__ __forceinline__ bool interior_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(A.n - 1); }
 __device__ __forceinline__ bool node_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(2 * A.n - 1); }
 
-// Restructure the treelet rooted at `root` (whole warp, converged). root_cost
-// is the cost the climb just computed for the root.
-__device__ void atr_treelet(const atr_args& A, int root, float root_cost, float* sd) {
+// Restructure the treelet rooted at `root` with children l0, r0 (whole warp,
+// converged). root_cost is the cost the climb just computed for the root.
+// Lane k holds treelet leaf k: its node, box, cost, refs and, for an interior
+// node, its two children, fetched together so that each expansion costs one
+// dependent round trip to memory.
+__device__ void atr_treelet(const atr_args& A, int root, float root_cost, int l0, int r0, atr_smem& W,
+                            const uint16_t* rc_of) {
     const int lane = threadIdx.x & 31;
     const int T = A.T, n = A.n;
-    // ---- formTreelet: lane k holds treelet leaf k (node, area) and internal node k
-    const int l0 = __ldcg(A.left + root), r0 = __ldcg(A.right + root);
+    // ---- formTreelet: lane k holds treelet leaf k and internal node k
     int tl = lane == 0 ? l0 : (lane == 1 ? r0 : -1);
     int ti = lane == 0 ? root : -1;
-    float ta = -MAXF;
+    int kl = -1, kr = -1;
+    float4 lo = make_float4(0.0f, 0.0f, 0.0f, 0.0f), hi = lo;
+    float ta = -MAXF;  // area of an interior treelet leaf
     bool bad = !node_ok(A, l0) || !node_ok(A, r0);
     if (!bad && lane < 2) {
-        box6 b; float c; int rf;
-        load_node(A, tl, b, c, rf);
-        ta = area_of(b);
+        lo = __ldcg(A.nbmin + tl);
+        hi = __ldcg(A.nbmax + tl);
+        if (interior_ok(A, tl)) {
+            kl = __ldcg(A.left + tl);
+            kr = __ldcg(A.right + tl);
+            ta = area_of(box_of(lo, hi));
+        }
     }
     for (int it = 0; it < T - 2 && !bad; ++it) {
         const int m = it + 2;
         int idx = lane;
-        float a = (lane < m && tl < n - 1) ? ta : -MAXF;
+        float a = lane < m ? ta : -MAXF;
         // findLeafToExpand: strict '>' keeps the lower lane on ties
         int cnt = m, sh = cnt / 2;
         while (cnt > 1) {
@@ -150,46 +179,47 @@ __device__ void atr_treelet(const atr_args& A, int root, float root_cost, float*
         }
         idx = __shfl_sync(HP_FULL_MASK, idx, 0);
         const int rep = __shfl_sync(HP_FULL_MASK, tl, idx);
-        if (!interior_ok(A, rep)) { bad = true; break; }  // a subtree of >= gamma refs always has one
+        const int rl = __shfl_sync(HP_FULL_MASK, kl, idx), rr = __shfl_sync(HP_FULL_MASK, kr, idx);
+        // a subtree of >= gamma refs always has an interior leaf to expand
+        if (!interior_ok(A, rep) || !node_ok(A, rl) || !node_ok(A, rr)) { bad = true; break; }
         if (lane == it + 1) ti = rep;
         if (lane == idx || lane == m) {
-            tl = lane == idx ? __ldcg(A.left + rep) : __ldcg(A.right + rep);
-            if (node_ok(A, tl)) {
-                box6 b; float c; int rf;
-                load_node(A, tl, b, c, rf);
-                ta = area_of(b);
+            tl = lane == idx ? rl : rr;
+            lo = __ldcg(A.nbmin + tl);
+            hi = __ldcg(A.nbmax + tl);
+            kl = kr = -1;
+            ta = -MAXF;
+            if (interior_ok(A, tl)) {
+                kl = __ldcg(A.left + tl);
+                kr = __ldcg(A.right + tl);
+                ta = area_of(box_of(lo, hi));
             }
         }
-        bad = __any_sync(HP_FULL_MASK, (lane == idx || lane == m) && !node_ok(A, tl));
     }
     if (bad) {
         if (lane == 0) hp_report(A.err, HP_DEV_BAD_INDEX, root);
         return;
     }
-    // ---- slot state and the distance matrix
-    box6 bx{};
-    float sc = 0.0f;
-    int sr = 0, sn = tl;
-    if (lane < T) load_node(A, tl, bx, sc, sr);
-    const int M = T * (T - 1) / 2;
-    for (int b0 = 0; b0 < M; b0 += 32) {
-        const int e = b0 + lane;
-        int row = 1, col = 0;
-        if (e < M) tri_decode(e, row, col);
-        const box6 br = shfl_box(bx, row), bc = shfl_box(bx, col);
-        if (e < M) sd[e] = area_of(join(br, bc));
+    // ---- slots and the distance matrix
+    if (lane < T) {
+        W.lo[lane] = lo;
+        W.hi[lane] = hi;
+        W.node[lane] = tl;
     }
     __syncwarp();
-    // ---- agglomerative merging; lane k records the internal node made at step k
-    int ol = -1, orr = -1, orf = 0;
-    float oc = 0.0f;
-    box6 ob{};
+    const int M = T * (T - 1) / 2;
+    for (int e = lane; e < M; e += 32) {
+        const int rc = rc_of[e], row = rc >> 8, col = rc & 255;
+        W.d[e] = area_of(join(box_of(W.lo[row], W.hi[row]), box_of(W.lo[col], W.hi[col])));
+    }
+    __syncwarp();
+    // ---- agglomerative merging; step `last` makes internal node ti[last - 1]
     for (int last = T - 1; last >= 1; --last) {
         const int mm = last * (last + 1) / 2;
         float best = MAXF;
         int bi = 0;
         for (int e = lane; e < mm; e += 32) {
-            const float d = sd[e];
+            const float d = W.d[e];
             if (d < best) { best = d; bi = e; }
         }
 #pragma unroll
@@ -199,55 +229,67 @@ __device__ void atr_treelet(const atr_args& A, int root, float root_cost, float*
             if (obst < best) { best = obst; bi = oi; }
         }
         bi = __shfl_sync(HP_FULL_MASK, bi, 0);
-        int row, col;
-        tri_decode(bi, row, col);
-        const float c_r = __shfl_sync(HP_FULL_MASK, sc, row), c_c = __shfl_sync(HP_FULL_MASK, sc, col);
-        const int n_r = __shfl_sync(HP_FULL_MASK, sn, row), n_c = __shfl_sync(HP_FULL_MASK, sn, col);
-        const int r_r = __shfl_sync(HP_FULL_MASK, sr, row), r_c = __shfl_sync(HP_FULL_MASK, sr, col);
-        const box6 u = join(shfl_box(bx, row), shfl_box(bx, col));
-        const float uc = __fmaf_rn(A.ct, area_of(u), __fadd_rn(c_r, c_c));
-        const int n_l = __shfl_sync(HP_FULL_MASK, sn, last), r_l = __shfl_sync(HP_FULL_MASK, sr, last);
-        const float c_l = __shfl_sync(HP_FULL_MASK, sc, last);
-        const box6 b_l = shfl_box(bx, last);
+        const int rc = rc_of[bi], row = rc >> 8, col = rc & 255;
+        const float4 rlo = W.lo[row], rhi = W.hi[row], clo = W.lo[col], chi = W.hi[col];
+        const box6 u = join(box_of(rlo, rhi), box_of(clo, chi));
+        const float uc = __fmaf_rn(A.ct, area_of(u), __fadd_rn(rlo.w, clo.w));
+        const float4 ulo = make_float4(u.mn[0], u.mn[1], u.mn[2], uc);
+        const float4 uhi = make_float4(u.mx[0], u.mx[1], u.mx[2],
+                                       __int_as_float(__float_as_int(rhi.w) + __float_as_int(chi.w)));
+        const int n_r = W.node[row], n_c = W.node[col];
+        const float4 llo = W.lo[last], lhi = W.hi[last];
+        const int n_l = W.node[last];
         const int inode = __shfl_sync(HP_FULL_MASK, ti, last - 1);
-        if (lane == last) { ol = n_r; orr = n_c; oc = uc; orf = r_r + r_c; ob = u; }
-        if (lane == col) {
-            sn = inode; sc = uc; sr = r_r + r_c; bx = u;
-        } else if (lane == row) {
-            sn = n_l; sc = c_l; sr = r_l; bx = b_l;
+        float dv = 0.0f;
+        int dst = -1;
+        if (last > 1 && lane < last && lane != row) {
+            dv = W.d[tri_index(last, lane)];
+            dst = tri_index(max(row, lane), min(row, lane));
         }
-        if (last > 1) {
-            float dv = 0.0f;
-            int dst = -1;
-            if (lane < last && lane != row) {
-                dv = sd[tri_index(last, lane)];
-                dst = tri_index(max(row, lane), min(row, lane));
-            }
-            __syncwarp();
-            if (dst >= 0) sd[dst] = dv;
-            __syncwarp();
-            const box6 bc = shfl_box(bx, col);
-            if (lane < last && lane != col) sd[tri_index(max(col, lane), min(col, lane))] = area_of(join(bx, bc));
-            __syncwarp();
+        __syncwarp();
+        if (lane == 0) {
+            W.olo[last] = ulo;
+            W.ohi[last] = uhi;
+            W.okids[last] = make_int2(n_r, n_c);
+            W.lo[col] = ulo;
+            W.hi[col] = uhi;
+            W.node[col] = inode;
+            W.lo[row] = llo;
+            W.hi[row] = lhi;
+            W.node[row] = n_l;
         }
+        if (dst >= 0) W.d[dst] = dv;
+        __syncwarp();
+        if (last > 1 && lane < last && lane != col)
+            W.d[tri_index(max(col, lane), min(col, lane))] = area_of(join(box_of(W.lo[lane], W.hi[lane]), u));
+        __syncwarp();
     }
     // ---- updateTreelet: keep the new topology iff its cost is strictly lower
-    const float newc = __shfl_sync(HP_FULL_MASK, oc, 1);
+    const float newc = W.olo[1].w;
     const int node = __shfl_up_sync(HP_FULL_MASK, ti, 1);
     if (newc < root_cost && lane >= 1 && lane < T) {
-        __stcg(A.left + node, ol);
-        __stcg(A.right + node, orr);
-        __stcg(A.parent + ol, node);
-        __stcg(A.parent + orr, node);
-        __stcg(A.nbmin + node, make_float4(ob.mn[0], ob.mn[1], ob.mn[2], oc));
-        __stcg(A.nbmax + node, make_float4(ob.mx[0], ob.mx[1], ob.mx[2], __int_as_float(orf)));
+        const float4 olo = W.olo[lane], ohi = W.ohi[lane];
+        const int2 k = W.okids[lane];
+        __stcg(A.left + node, k.x);
+        __stcg(A.right + node, k.y);
+        __stcg(A.parent + k.x, node);
+        __stcg(A.parent + k.y, node);
+        __stcg(A.nbmin + node, olo);
+        __stcg(A.nbmax + node, ohi);
     }
     __threadfence();
     __syncwarp();
 }
 
 __global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
-    __shared__ float s_dist[AW][DMAX];
+    __shared__ atr_smem s_w[AW];
+    __shared__ uint16_t s_rc[DMAX];  // packed triangle index -> (row << 8) | col
+    for (int e = threadIdx.x; e < DMAX; e += AB) {
+        int row, col;
+        tri_decode(e, row, col);
+        s_rc[e] = (uint16_t)((row << 8) | col);
+    }
+    __syncthreads();
     const int warp = threadIdx.x >> 5;
     const int p = blockIdx.x * AB + threadIdx.x;
     const int n = A.n;
@@ -274,21 +316,22 @@ __global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
             break;
         }
         bool arrived = false;
-        int refs = 0;
+        int refs = 0, l = -1, r = -1;
         float cost = 0.0f;
         if (cur >= 0) {
             if (!interior_ok(A, cur)) {
                 hp_report(A.err, HP_DEV_BAD_INDEX, cur);
                 cur = -1;
             } else {
-                __threadfence();
-                if (atomicAdd(A.counters + cur, 1) == 0) cur = -1;
+                if (hp_arrive(A.counters + cur) == 0) cur = -1;
                 else arrived = true;
-                __threadfence();
             }
         }
+        int up = -1;
         if (arrived) {
-            const int l = __ldcg(A.left + cur), r = __ldcg(A.right + cur);
+            l = __ldcg(A.left + cur);
+            r = __ldcg(A.right + cur);
+            up = __ldcg(A.parent + cur);  // a treelet rooted at cur keeps cur's parent
             if (!node_ok(A, l) || !node_ok(A, r)) {
                 hp_report(A.err, HP_DEV_BAD_INDEX, cur);
                 arrived = false;
@@ -311,10 +354,11 @@ __global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
             const int src = __ffs(vote) - 1;
             const int root = __shfl_sync(HP_FULL_MASK, cur, src);
             const float rc = __shfl_sync(HP_FULL_MASK, cost, src);
-            atr_treelet(A, root, rc, s_dist[warp]);
+            const int l0 = __shfl_sync(HP_FULL_MASK, l, src), r0 = __shfl_sync(HP_FULL_MASK, r, src);
+            atr_treelet(A, root, rc, l0, r0, s_w[warp], s_rc);
             vote &= vote - 1;
         }
-        if (cur >= 0) cur = __ldcg(A.parent + cur);
+        cur = arrived ? up : -1;
     }
 }
 
