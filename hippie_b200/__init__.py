@@ -14,10 +14,11 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (HP_BATCH_NO_GRAPH, HP_METHOD_ATR, HP_METHOD_LBVH, HP_METHOD_PLOC, HP_TRACE_ANY_HIT,
-                   HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_mesh, hp_tune,
-                   load)
+                   HP_TRACE_STATS, HPError, check, hp_build_params, hp_build_taps, hp_bvh, hp_bvh_stats, hp_host_scene,
+                   hp_mesh, hp_tune, load)
 
-__all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "pixel_table",
+__all__ = ["Context", "BVH", "Batch", "BuildParams", "Env", "HPError", "gen", "pixel_table", "Scene",
+           "load_scene", "read_scene_bin", "read_scene_obj",
            "camera_screen_to_world", "HP_METHOD_LBVH", "HP_METHOD_PLOC",
            "HP_METHOD_ATR", "HP_TRACE_ANY_HIT", "HP_TRACE_STATS", "load"]
 
@@ -118,6 +119,14 @@ class BVH:
         v = C.c_double()
         check(load().hp_bvh_cost(self.ctx.h, C.byref(self.c), C.byref(v), _stream_ptr(stream)))
         return v.value
+
+    def stats(self, stream=None) -> dict:
+        """HipBVH::getCost / getAvgLeafSize / getLeafSizeHistogram in one device pass."""
+        st = hp_bvh_stats()
+        check(load().hp_bvh_stats_get(self.ctx.h, C.byref(self.c), C.byref(st), _stream_ptr(stream)))
+        return {"sah_cost": st.sah_cost, "avg_leaf_size": st.avg_leaf_size,
+                "sum_of_leaf_sizes": st.sum_of_leaf_sizes, "num_interior": st.num_interior,
+                "num_leaf": st.num_leaf, "leaf_size_histogram": list(st.leaf_size_histogram)}
 
     def validate(self, verts, tris, stream=None) -> bool:
         m = _mesh(verts, tris)
@@ -349,6 +358,73 @@ class Batch:
         check(load().hp_batch_bvh(self.h, m, C.byref(b.c)))
         b.batch = self  # keeps the batch's storage alive
         return b
+
+
+class Scene:
+    """A host triangle mesh: vertices (V x 3 float32), triangles (T x 3 int32) and
+    the box stored with it (min xyz, max xyz, before any normalisation)."""
+
+    def __init__(self, vertices, triangles, box=None):
+        self.vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        self.triangles = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+        if box is None:
+            box = np.concatenate([self.vertices.min(0), self.vertices.max(0)]) if len(self.vertices) else \
+                np.zeros(6, np.float32)
+        self.box = np.asarray(box, np.float32).copy()
+
+    def _c(self) -> hp_host_scene:
+        c = hp_host_scene()
+        c.vertices = self.vertices.ctypes.data_as(C.POINTER(C.c_float))
+        c.triangles = self.triangles.ctypes.data_as(C.POINTER(C.c_int32))
+        c.num_vertices = len(self.vertices)
+        c.num_triangles = len(self.triangles)
+        c.box[:] = self.box.tolist()
+        return c
+
+    @staticmethod
+    def _take(c: hp_host_scene) -> "Scene":
+        try:
+            v = np.ctypeslib.as_array(c.vertices, (c.num_vertices * 3,)).copy() if c.num_vertices else \
+                np.zeros(0, np.float32)
+            t = np.ctypeslib.as_array(c.triangles, (c.num_triangles * 3,)).copy() if c.num_triangles else \
+                np.zeros(0, np.int32)
+            return Scene(v, t, np.array(c.box[:], np.float32))
+        finally:
+            load().hp_scene_free(C.byref(c))
+
+    def write_bin(self, path) -> None:
+        """BinExporter::exportScene (zero normals, texture coordinates, material indices)."""
+        c = self._c()
+        check(load().hp_scene_write_bin(str(path).encode(), C.byref(c)))
+
+    def normalized(self) -> "Scene":
+        """SceneLoader::loadStaticScene's normalisation, done by the library."""
+        out = Scene(self.vertices.copy(), self.triangles, self.box)
+        c = out._c()
+        check(load().hp_scene_normalize(C.byref(c)))
+        return out
+
+
+def read_scene_bin(path) -> Scene:
+    """BinImporter::importScene: geometry of a scene in the binary cache format."""
+    c = hp_host_scene()
+    check(load().hp_scene_read_bin(str(path).encode(), C.byref(c)))
+    return Scene._take(c)
+
+
+def read_scene_obj(path) -> Scene:
+    """Geometry of a Wavefront OBJ file (polygon fans, degenerate triangles dropped)."""
+    c = hp_host_scene()
+    check(load().hp_scene_read_obj(str(path).encode(), C.byref(c)))
+    return Scene._take(c)
+
+
+def load_scene(path, write_cache: bool = True) -> Scene:
+    """SceneLoader::loadStaticScene: path + ".bin" if present, else the OBJ file
+    (cached to path + ".bin" when write_cache), normalised to the unit box."""
+    c = hp_host_scene()
+    check(load().hp_scene_load(str(path).encode(), 1 if write_cache else 0, C.byref(c)))
+    return Scene._take(c)
 
 
 def pixel_table(width: int, height: int):

@@ -40,6 +40,17 @@ class hp_bvh(C.Structure):
                 ("method", C.c_int32), ("ct", C.c_float), ("ci", C.c_float), ("impl", C.c_void_p)]
 
 
+class hp_bvh_stats(C.Structure):
+    _fields_ = [("sah_cost", C.c_double), ("avg_leaf_size", C.c_double), ("sum_of_leaf_sizes", C.c_int64),
+                ("num_interior", C.c_int32), ("num_leaf", C.c_int32),
+                ("leaf_size_histogram", C.c_float * 33), ("pad", C.c_int32)]
+
+
+class hp_host_scene(C.Structure):
+    _fields_ = [("vertices", C.POINTER(C.c_float)), ("triangles", C.POINTER(C.c_int32)),
+                ("num_vertices", C.c_int64), ("num_triangles", C.c_int64), ("box", C.c_float * 6)]
+
+
 class hp_tune(C.Structure):
     _fields_ = [("sort_block", C.c_int32), ("trace_ctas_per_sm", C.c_int32), ("trace_stack", C.c_int32),
                 ("trace_sorted", C.c_int32), ("ploc_radius", C.c_int32), ("ploc_adaptive", C.c_int32),
@@ -74,6 +85,7 @@ _SIGS = {
     "hp_bvh_download": (C.c_int, [_P, C.POINTER(hp_bvh), _P, _P, _P, _P]),
     "hp_bvh_cost": (C.c_int, [_P, C.POINTER(hp_bvh), C.POINTER(C.c_double), _P]),
     "hp_bvh_validate": (C.c_int, [_P, C.POINTER(hp_bvh), C.POINTER(hp_mesh), C.POINTER(C.c_int32), _P]),
+    "hp_bvh_stats_get": (C.c_int, [_P, C.POINTER(hp_bvh), C.POINTER(hp_bvh_stats), _P]),
     "hp_refit": (C.c_int, [_P, C.POINTER(hp_bvh), C.POINTER(hp_mesh), _P]),
     "hp_trace": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, _P]),
     "hp_trace_adjoint": (C.c_int, [_P, C.POINTER(hp_mesh), _P, _P, _P, C.c_int64, _P, _P]),
@@ -88,6 +100,12 @@ _SIGS = {
     "hp_batch_bvh": (C.c_int, [_P, C.c_int32, C.POINTER(hp_bvh)]),
     "hp_trace_sorted": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, C.c_int32, _P, _P]),
     "hp_pixel_table": (C.c_int, [C.c_int32, C.c_int32, _P]),
+    "hp_scene_read_bin": (C.c_int, [C.c_char_p, C.POINTER(hp_host_scene)]),
+    "hp_scene_write_bin": (C.c_int, [C.c_char_p, C.POINTER(hp_host_scene)]),
+    "hp_scene_read_obj": (C.c_int, [C.c_char_p, C.POINTER(hp_host_scene)]),
+    "hp_scene_normalize": (C.c_int, [C.POINTER(hp_host_scene)]),
+    "hp_scene_load": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(hp_host_scene)]),
+    "hp_scene_free": (None, [C.POINTER(hp_host_scene)]),
     "hp_camera_screen_to_world": (C.c_int, [_P, _P, C.c_float, C.c_int32, C.c_int32, C.c_float, C.c_float, _P]),
     "hp_gen_primary_rays": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_int32, _P, _P, _P]),
     "hp_ray_keys": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int32, _P, _P]),

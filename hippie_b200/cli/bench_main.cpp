@@ -8,9 +8,15 @@
 // Halton-jittered sample per Renderer.numberOfPrimarySamples, in pixel-table
 // order, and traces them (closest hit). It prints one JSON line.
 //
-// Scene.filename: a Wavefront OBJ file (vertices and faces, polygons fanned into
-// triangles), or a synthetic scene: "synthetic:uniform:<n>",
+// Scene.filename: a scene file loaded as SceneLoader::loadStaticScene does
+// (the binary cache "<file>.bin" if present, else a Wavefront OBJ file whose
+// geometry is then cached; vertices normalised to the unit box), or a
+// synthetic scene, used as generated: "synthetic:uniform:<n>",
 // "synthetic:clustered:<n>" or "synthetic:heightfield:<nx>x<ny>".
+//
+// Besides build and trace rates, the line carries the BVH statistics that
+// Benchmark::testStatic prints (Benchmark.cpp:80-90): SAH cost, average leaf
+// size and the leaf-size histogram.
 //
 // Usage: hippie_b200_bench <file.env> [--steps K] [--dry-run]
 //   --dry-run  parse the env file, load the scene and print the resolved
@@ -38,34 +44,15 @@ struct HostMesh {
     std::vector<int32_t> t;  // three vertex indices per triangle
 };
 
-// OBJ: "v x y z" and "f a b c ..." (1-based or negative indices, "a/b/c" forms).
-HostMesh load_obj(const std::string& path) {
-    std::ifstream in(path);
-    if (!in) throw Error(HP_ERR_ARG, "cannot open scene file " + path);
+// A scene file as SceneLoader::loadStaticScene reads it: the binary cache
+// beside it (name + ".bin") or the OBJ file itself (then cached), normalised.
+HostMesh load_file(const std::string& path) {
+    hp_host_scene sc;
+    check(hp_scene_load(path.c_str(), 1, &sc), "hp_scene_load");
     HostMesh m;
-    std::string line;
-    while (std::getline(in, line)) {
-        std::istringstream is(line);
-        std::string tag;
-        if (!(is >> tag)) continue;
-        if (tag == "v") {
-            float x, y, z;
-            if (!(is >> x >> y >> z)) throw Error(HP_ERR_PARSE, "bad vertex line: " + line);
-            m.v.insert(m.v.end(), {x, y, z});
-        } else if (tag == "f") {
-            std::vector<int32_t> idx;
-            std::string tok;
-            const long nv = (long)(m.v.size() / 3);
-            while (is >> tok) {
-                const long k = std::strtol(tok.c_str(), nullptr, 10);
-                const long i = k > 0 ? k - 1 : nv + k;
-                if (k == 0 || i < 0 || i >= nv) throw Error(HP_ERR_PARSE, "bad face index in: " + line);
-                idx.push_back((int32_t)i);
-            }
-            for (size_t j = 1; j + 1 < idx.size(); ++j) m.t.insert(m.t.end(), {idx[0], idx[j], idx[j + 1]});
-        }
-    }
-    if (m.t.empty()) throw Error(HP_ERR_PARSE, "no triangles in " + path);
+    m.v.assign(sc.vertices, sc.vertices + 3 * sc.num_vertices);
+    m.t.assign(sc.triangles, sc.triangles + 3 * sc.num_triangles);
+    hp_scene_free(&sc);
     return m;
 }
 
@@ -73,7 +60,7 @@ HostMesh make_scene(const std::string& name) {
     HostMesh m;
     auto num = [&](const std::string& s) { return std::strtoll(s.c_str(), nullptr, 10); };
     const std::string pre = "synthetic:";
-    if (name.compare(0, pre.size(), pre) != 0) return load_obj(name);
+    if (name.compare(0, pre.size(), pre) != 0) return load_file(name);
     const std::string rest = name.substr(pre.size());
     const size_t colon = rest.find(':');
     const std::string kind = rest.substr(0, colon), arg = colon == std::string::npos ? "" : rest.substr(colon + 1);
@@ -157,8 +144,15 @@ int run(int argc, char** argv) {
     for (int k = 0; k < steps; ++k) build_s += builder.rebuild(bvh, mesh);
     build_s /= steps;
     const int nodes = bvh.getNumberOfNodes();
-    const double cost = bvh.getCost();
+    const hp_bvh_stats st = bvh.stats();
+    const double cost = st.sah_cost;
     const bool valid = bvh.validate(mesh);
+    std::string hist;
+    for (int k = 0; k <= HP_MAX_LEAF_SIZE_HIST; ++k) {
+        char buf[32];
+        std::snprintf(buf, sizeof(buf), "%s%.9g", k ? ", " : "", st.leaf_size_histogram[k]);
+        hist += buf;
+    }
 
     std::vector<int32_t> table((size_t)w * h);
     check(hp_pixel_table(w, h, table.data()), "hp_pixel_table");
@@ -186,11 +180,12 @@ int run(int argc, char** argv) {
     const int64_t tris = mesh.num_triangles;
     std::printf("{\"scene\": \"%s\", \"triangles\": %lld, \"method\": \"%s\", \"nodes\": %d, \"valid\": %s, "
                 "\"sah_cost\": %.17g, \"build_ms\": %.4f, \"build_mtris_s\": %.2f, \"rays\": %lld, "
-                "\"trace_ms\": %.4f, \"trace_mrays_s\": %.2f, \"hits\": %lld, \"hit_fraction\": %.17g}\n",
+                "\"trace_ms\": %.4f, \"trace_mrays_s\": %.2f, \"hits\": %lld, \"hit_fraction\": %.17g, "
+                "\"avg_leaf_size\": %.17g, \"leaf_size_histogram\": [%s]}\n",
                 scene.c_str(), (long long)tris, method_name(p.method), nodes, valid ? "true" : "false", cost,
                 build_s * 1e3, tris / build_s / 1e6, (long long)(nrays * samples), trace_s * 1e3,
                 nrays * samples / trace_s / 1e6, (long long)hits,
-                samples ? (double)hits / (double)(nrays * samples) : 0.0);
+                samples ? (double)hits / (double)(nrays * samples) : 0.0, st.avg_leaf_size, hist.c_str());
     cudaFree(dv);
     cudaFree(dt);
     cudaFree(dtable);

@@ -327,143 +327,34 @@ hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh) {
     return HP_OK;
 }
 
-namespace {
-struct host_node {
-    float f[12];
-    int32_t c0, c1, size, parent;
-};
-static_assert(sizeof(host_node) == 64, "host node");
-
-float area_of(float mnx, float mny, float mnz, float mxx, float mxy, float mxz) {
-    if (!(mnx <= mxx && mny <= mxy && mnz <= mxz)) return 0.0f;
-    float dx = mxx - mnx, dy = mxy - mny, dz = mxz - mnz;
-    return 2.0f * std::fmaf(dz, dx, std::fmaf(dx, dy, dy * dz));
-}
-
-// Union of the two child boxes stored in a node (HipBVHNodeN<2>::getBoundingBox).
-void node_box(const host_node& n, float* mn, float* mx) {
-    mn[0] = std::min(n.f[0], n.f[4]); mx[0] = std::max(n.f[1], n.f[5]);
-    mn[1] = std::min(n.f[2], n.f[6]); mx[1] = std::max(n.f[3], n.f[7]);
-    mn[2] = std::min(n.f[8], n.f[10]); mx[2] = std::max(n.f[9], n.f[11]);
-}
-
-hp_status fetch_nodes(hp_ctx* ctx, hp_bvh* bvh, std::vector<host_node>& nodes, void* stream) {
-    HP_TRY(hp_bvh_sync(ctx, bvh, stream));
-    const int64_t count = (int64_t)bvh->num_interior + bvh->num_leaf;
-    nodes.resize(count);
-    if (count)
-        HP_CUDA(cudaMemcpy(nodes.data(), bvh->nodes, count * sizeof(host_node), cudaMemcpyDeviceToHost));
-    return HP_OK;
-}
-}  // namespace
-
-hp_status hp_bvh_cost(hp_ctx* ctx, const hp_bvh* bvh_in, double* cost, void* stream) {
-    if (!ctx || !bvh_in || !cost || !bvh_in->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_cost: null argument");
-    hp_bvh bvh = *bvh_in;
-    std::vector<host_node> nodes;
-    HP_TRY(fetch_nodes(ctx, &bvh, nodes, stream));
-    const float* sb = bvh.scene_box;
-    const double scene_area = area_of(sb[0], sb[1], sb[2], sb[3], sb[4], sb[5]);
-    double c = 0.0;
-    for (const host_node& n : nodes) {
-        float mn[3], mx[3];
-        node_box(n, mn, mx);
-        double a = area_of(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) / scene_area;
-        if (n.size < 0) c += (double)bvh.ci * a * (double)(~n.size);
-        else c += (double)bvh.ct * a;
-    }
-    *cost = c;
+// HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370) on the device (k_stats.cu).
+hp_status hp_bvh_cost(hp_ctx* ctx, const hp_bvh* bvh, double* cost, void* stream) {
+    if (!ctx || !bvh || !cost || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_cost: null argument");
+    hp_bvh_stats st;
+    HP_TRY(hp_bvh_stats_run(ctx, bvh, &st, reinterpret_cast<cudaStream_t>(stream)));
+    *cost = st.sah_cost;
     return HP_OK;
 }
 
-// HipBVH::validate (rt/bvh/HipBVH.cpp:157-307): every triangle referenced once,
-// parent links, node sizes, non-empty leaves whose box overlaps their
-// triangles, every node reachable exactly once. Also checks that child boxes
-// contain the triangles below them.
-hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh_in, const hp_mesh* m, int32_t* valid,
-                          void* stream) {
-    if (!ctx || !bvh_in || !valid || !bvh_in->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: null argument");
+// getCost, getAvgLeafSize and getLeafSizeHistogram (rt/bvh/HipBVH.cpp:346-442).
+hp_status hp_bvh_stats_get(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, void* stream) {
+    if (!ctx || !bvh || !out || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_stats_get: null argument");
+    return hp_bvh_stats_run(ctx, bvh, out, reinterpret_cast<cudaStream_t>(stream));
+}
+
+// HipBVH::validate (rt/bvh/HipBVH.cpp:157-307) on the device (k_stats.cu).
+hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, int32_t* valid, void* stream) {
+    if (!ctx || !bvh || !valid || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: null argument");
     HP_TRY(check_mesh(m));
     *valid = 0;
-    hp_bvh bvh = *bvh_in;
-    std::vector<host_node> nodes;
-    HP_TRY(fetch_nodes(ctx, &bvh, nodes, stream));
-    const int64_t n = bvh.num_refs;
-    if (n != m->num_triangles) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: mesh does not match the BVH");
-    if (n == 0) { *valid = nodes.empty(); return HP_OK; }
-    std::vector<int32_t> tri(n), tris(3 * m->num_triangles);
-    std::vector<float> verts(3 * m->num_vertices);
-    HP_CUDA(cudaMemcpy(tri.data(), bvh.tri_indices, n * 4, cudaMemcpyDeviceToHost));
-    HP_CUDA(cudaMemcpy(tris.data(), m->triangles, tris.size() * 4, cudaMemcpyDeviceToHost));
-    HP_CUDA(cudaMemcpy(verts.data(), m->vertices, verts.size() * 4, cudaMemcpyDeviceToHost));
-    bool ok = true;
-    std::string why;
-    auto bad = [&](const std::string& w) { if (ok) why = w; ok = false; };
-    const int64_t count = (int64_t)nodes.size();
-    std::vector<int> seen(count, 0), tri_seen(n, 0);
-    for (int64_t i = 0; i < n; ++i) {
-        if (tri[i] < 0 || tri[i] >= n) { bad("invalid triangle index"); break; }
-        tri_seen[tri[i]]++;
+    if (bvh->num_refs != m->num_triangles) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: mesh does not match the BVH");
+    if (bvh->num_refs == 0) {
+        hp_bvh tmp = *bvh;
+        HP_TRY(hp_bvh_sync(ctx, &tmp, stream));
+        *valid = (tmp.num_interior + tmp.num_leaf) == 0;
+        return HP_OK;
     }
-    for (int64_t i = 0; i < n && ok; ++i)
-        if (tri_seen[i] != 1) bad("triangle not referenced exactly once");
-    std::vector<int64_t> stack{0};
-    if (count == 0) bad("no nodes");
-    else seen[0] = 1;
-    if (ok && nodes[0].parent != -1) bad("root parent is not -1");
-    while (ok && !stack.empty()) {
-        int64_t ni = stack.back();
-        stack.pop_back();
-        const host_node& nd = nodes[ni];
-        if (nd.size >= 0) {
-            if (ni >= bvh.num_interior) { bad("interior node in the leaf range"); break; }
-            int64_t size = 0;
-            for (int c = 0; c < 2; ++c) {
-                int32_t raw = c == 0 ? nd.c0 : nd.c1;
-                int64_t ci = raw < 0 ? ~raw : raw;
-                if (ci <= 0 || ci >= count) { bad("child index out of range"); break; }
-                const host_node& ch = nodes[ci];
-                if ((raw < 0) != (ch.size < 0)) { bad("child leaf flag mismatch"); break; }
-                if (ch.parent != ni) { bad("invalid parent index"); break; }
-                size += ch.size < 0 ? ~ch.size : ch.size;
-                seen[ci]++;
-                stack.push_back(ci);
-                // the child box stored here must contain the child's own box
-                float cmn[3], cmx[3];
-                node_box(ch, cmn, cmx);
-                const float* f = nd.f;
-                float bmn[3] = {f[4 * c + 0], f[4 * c + 2], f[8 + 2 * c]};
-                float bmx[3] = {f[4 * c + 1], f[4 * c + 3], f[9 + 2 * c]};
-                bool empty_child = (ch.size < 0) && (ch.c0 == ch.c1);
-                for (int a = 0; a < 3 && !empty_child; ++a)
-                    if (cmn[a] < bmn[a] || cmx[a] > bmx[a]) { bad("child box not enclosed"); break; }
-            }
-            if (ok && size != nd.size) bad("invalid node size");
-        } else {
-            if (ni < bvh.num_interior) { bad("leaf node in the interior range"); break; }
-            int32_t b0 = nd.c0, e0 = nd.c1;
-            if (b0 > e0 || b0 < 0 || e0 > n || (b0 == e0 && n != 1)) { bad("invalid leaf bounds"); break; }
-            if (e0 - b0 != ~nd.size) { bad("leaf size does not match its range"); break; }
-            float mn[3], mx[3];
-            node_box(nd, mn, mx);
-            for (int32_t r = b0; r < e0 && ok; ++r) {
-                const int32_t t = tri[r];
-                for (int k = 0; k < 3; ++k) {
-                    int32_t vi = tris[3 * (int64_t)t + k];
-                    if (vi < 0 || vi >= m->num_vertices) { bad("vertex index out of range"); break; }
-                    for (int a = 0; a < 3; ++a) {
-                        float x = verts[3 * (int64_t)vi + a];
-                        if (x < mn[a] || x > mx[a]) { bad("triangle is not in its leaf box"); break; }
-                    }
-                }
-            }
-        }
-    }
-    for (int64_t i = 0; i < count && ok; ++i)
-        if (seen[i] != 1) bad("node not referenced exactly once");
-    if (!ok) hp_set_error("validate: " + why);
-    *valid = ok ? 1 : 0;
-    return HP_OK;
+    return hp_bvh_validate_run(ctx, bvh, m, valid, reinterpret_cast<cudaStream_t>(stream));
 }
 
 hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {

@@ -84,6 +84,10 @@ struct hp_carve {
     static size_t pad(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 };
 
+// ---- BVH statistics and validation (k_stats.cu) ------------------------------
+hp_status hp_bvh_stats_run(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, cudaStream_t s);
+hp_status hp_bvh_validate_run(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, int32_t* valid, cudaStream_t s);
+
 // ---- radix sort ------------------------------------------------------------
 struct hp_sort_plan {
     int64_t n = 0;

@@ -14,6 +14,8 @@
  *   hp_bvh_*            HipBVH (nodes, woop, triangle idx)    rt/bvh/HipBVH.h:19-106
  *   hp_bvh_cost         HipBVH::getCost                       rt/bvh/HipBVH.cpp:346-370
  *   hp_bvh_validate     HipBVH::validate                      rt/bvh/HipBVH.cpp:157-307
+ *   hp_bvh_stats_get    HipBVH::getAvgLeafSize, getLeafSizeHistogram
+ *                                                             rt/bvh/HipBVH.cpp:372-442
  *   hp_refit            HipBVH::update (woopify + refit)      rt/bvh/HipBVH.cpp:472-477
  *   hp_trace            HipTracer::trace / traceStats         rt/tracer/HipTracer.cpp:13-52
  *   hp_trace_sorted     HipTracer::traceSort                  rt/tracer/HipTracer.cpp:109-125
@@ -150,6 +152,36 @@ hp_status hp_profile_get(hp_ctx* ctx, int32_t i, char* name, int64_t name_size, 
 /* Number of kernels this library has launched from the calling thread. */
 int64_t hp_launch_count(void);
 
+/* ---- scene files (host) ------------------------------------------------------
+ * A triangle mesh in host memory, allocated by the library (hp_scene_free).
+ *   hp_scene_read_bin   BinImporter::importScene   util/BinImporter.cpp:16-84
+ *   hp_scene_write_bin  BinExporter::exportScene   util/BinExporter.cpp:14-70
+ *                       (zero normals, texture coordinates and material
+ *                       indices; no materials or textures)
+ *   hp_scene_read_obj   the geometry AssimpImporter::importScene returns for
+ *                       an OBJ file (util/AssimpImporter.cpp:20-200): polygons
+ *                       as triangle fans, triangles whose box has zero area
+ *                       dropped, box = bound of all vertices
+ *   hp_scene_normalize  SceneLoader::loadStaticScene (rt/scene/SceneLoader.cpp:
+ *                       125-134): v = (v - box.min) * (1 / longest box side)
+ *   hp_scene_load       SceneLoader::loadScene + loadStaticScene: path + ".bin"
+ *                       if it exists (or path itself if it ends in ".bin"),
+ *                       else the OBJ file, whose geometry is then written to
+ *                       path + ".bin" when write_cache is set; then normalised. */
+typedef struct hp_host_scene {
+    float* vertices;          /* [num_vertices][3] */
+    int32_t* triangles;       /* [num_triangles][3] */
+    int64_t num_vertices;
+    int64_t num_triangles;
+    float box[6];             /* as stored / computed, before normalisation */
+} hp_host_scene;
+hp_status hp_scene_read_bin(const char* path, hp_host_scene* out);
+hp_status hp_scene_write_bin(const char* path, const hp_host_scene* scene);
+hp_status hp_scene_read_obj(const char* path, hp_host_scene* out);
+hp_status hp_scene_normalize(hp_host_scene* scene);
+hp_status hp_scene_load(const char* path, int32_t write_cache, hp_host_scene* out);
+void hp_scene_free(hp_host_scene* scene);
+
 /* ---- build (BVHBuilder) --------------------------------------------------- */
 void hp_build_params_default(hp_build_params* p);
 /* Build a BVH over mesh m into *out (allocates on first use; reuses the
@@ -167,10 +199,33 @@ hp_status hp_bvh_download(hp_ctx* ctx, hp_bvh* bvh, void* nodes_host, void* woop
                           int32_t* tri_host, void* stream);
 hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh);
 /* SAH cost as HipBVH::getCost (sum over nodes of ct|ci*size times node area
- * over scene area); summed in a fixed order in double precision. Synchronous. */
+ * over scene area), computed on the device and summed in a fixed order in
+ * double precision, so repeated calls agree bit for bit. Synchronous. */
 hp_status hp_bvh_cost(hp_ctx* ctx, const hp_bvh* bvh, double* cost, void* stream);
-/* Structural validation as HipBVH::validate; *valid = 1 if consistent.
- * Synchronous (copies the BVH to the host). */
+
+/* Quality statistics of a built BVH (rt/bvh/HipBVH.cpp:346-442):
+ *   sah_cost              HipBVH::getCost
+ *   avg_leaf_size         HipBVH::getAvgLeafSize = sum_of_leaf_sizes / num_leaf
+ *   leaf_size_histogram   HipBVH::getLeafSizeHistogram: fraction of leaves
+ *                         holding s references, s = 0..HP_MAX_LEAF_SIZE_HIST
+ *                         (MAX_LEAF_SIZE, rt/bvh/HipBVHKernels.h:13); larger
+ *                         leaves are counted in num_leaf only. */
+#define HP_MAX_LEAF_SIZE_HIST 32
+typedef struct hp_bvh_stats {
+    double sah_cost;
+    double avg_leaf_size;
+    int64_t sum_of_leaf_sizes;
+    int32_t num_interior;
+    int32_t num_leaf;
+    float leaf_size_histogram[HP_MAX_LEAF_SIZE_HIST + 1];
+    int32_t pad;
+} hp_bvh_stats;
+/* One pass over the nodes on the device; synchronous. */
+hp_status hp_bvh_stats_get(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, void* stream);
+
+/* Structural validation as HipBVH::validate (rt/bvh/HipBVH.cpp:157-307);
+ * *valid = 1 if consistent, else 0 and hp_last_error names the first failed
+ * check. Runs on the device with every index bounds-checked; synchronous. */
 hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m,
                           int32_t* valid, void* stream);
 /* Refit-only update after vertex moves (HipBVH::update): re-woopify and

@@ -21,6 +21,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "hippie_b200.h"
 
@@ -131,6 +132,19 @@ public:
         double c = 0.0;
         check(hp_bvh_cost(ctx_.get(), &b_, &c, stream), "hp_bvh_cost");
         return c;
+    }
+    /* HipBVH::getAvgLeafSize. */
+    float getAvgLeafSize(void* stream = nullptr) const { return (float)stats(stream).avg_leaf_size; }
+    /* HipBVH::getLeafSizeHistogram: fraction of leaves of each size 0..32. */
+    std::vector<float> getLeafSizeHistogram(void* stream = nullptr) const {
+        const hp_bvh_stats st = stats(stream);
+        return std::vector<float>(st.leaf_size_histogram, st.leaf_size_histogram + HP_MAX_LEAF_SIZE_HIST + 1);
+    }
+    /* All of the above in one device pass. */
+    hp_bvh_stats stats(void* stream = nullptr) const {
+        hp_bvh_stats st;
+        check(hp_bvh_stats_get(ctx_.get(), &b_, &st, stream), "hp_bvh_stats_get");
+        return st;
     }
     /* HipBVH::validate. */
     bool validate(const hp_mesh& m, void* stream = nullptr) const {

@@ -8,6 +8,8 @@ from pathlib import Path
 
 import pytest
 
+import hippie_b200 as hp
+
 ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "hippie_b200" / "hippie_b200_bench"
 
@@ -76,13 +78,16 @@ def test_obj_scene(tmp_path):
     env.write_text(ENV.format(method="lbvh", scene=obj))
     d = json.loads(run(env, "--dry-run").stdout)
     assert (d["triangles"], d["vertices"]) == (5, 5)
+    # loaded as SceneLoader does: the geometry is cached beside the scene file
+    cached = hp.read_scene_bin(tmp_path / "quad.obj.bin")
+    assert cached.triangles.shape == (5, 3)
 
 
 def test_bad_input(tmp_path):
     env = tmp_path / "c.env"
     env.write_text(ENV.format(method="ploc", scene=tmp_path / "missing.obj"))
     r = run(env, "--dry-run")
-    assert r.returncode != 0 and "cannot open scene file" in r.stderr
+    assert r.returncode != 0 and "cannot open" in r.stderr
     bad = tmp_path / "bad.obj"
     bad.write_text("v 0 0 0\nf 1 2 3\n")
     env.write_text(ENV.format(method="ploc", scene=bad))

@@ -53,13 +53,20 @@ def test_cli_matches_python(ctx, tmp_path, method):
     assert r.returncode == 0, r.stderr
     d = json.loads(r.stdout)
     assert d["triangles"] == 3000 and d["valid"] is True
-    # the same build through the Python binding (vertices round-trip exactly through repr)
+    # the same build through the Python binding, on the scene as the CLI loaded it
+    # (vertices round-trip exactly through repr; then SceneLoader's normalisation)
+    scene = hp.load_scene(obj)
+    assert np.array_equal(scene.triangles, t)
+    assert np.array_equal(scene.vertices, hp.Scene(v, t).normalized().vertices)
     p = hp.Env().read_string(env.read_text()).build_params()
-    V, T = torch.from_numpy(v).cuda(), torch.from_numpy(t).cuda()
+    V, T = torch.from_numpy(scene.vertices).cuda(), torch.from_numpy(scene.triangles).cuda()
     bvh = ctx.build(V, T, p)
     bvh.sync()
     assert d["nodes"] == bvh.num_nodes
-    assert d["sah_cost"] == pytest.approx(bvh.cost(), rel=1e-9)
+    st = bvh.stats()
+    assert d["sah_cost"] == st["sah_cost"]
+    assert d["avg_leaf_size"] == st["avg_leaf_size"]
+    assert d["leaf_size_histogram"] == pytest.approx(st["leaf_size_histogram"], rel=1e-8)
     pos = np.array([0.5, 0.5, -1.5], np.float32)
     m = hp.camera_screen_to_world(pos, [0, 0, 1], 45.0, 256, 128, 0.01, 100.0)
     tbl = torch.from_numpy(hp.pixel_table(256, 128)).cuda()
