@@ -37,6 +37,12 @@ _SIGS = {
     "or_pixel_table": (C.c_int32, [C.c_int32, C.c_int32, _P]),
     "or_primary_rays": (None, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P, _P]),
     "or_ray_keys": (None, [_P, C.c_int64, _P, C.c_int32, _P]),
+    "or_collapse_wide": (C.c_int64, [C.c_int, _P, _P, _P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_int, _P, _P,
+                                      _P]),
+    "or_binary_tree": (None, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                              C.c_float, C.c_float, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "or_build_wide": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
     "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
@@ -203,6 +209,56 @@ def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1)):
     b = np.ascontiguousarray(box, np.float32)
     load().or_ray_keys(_p(np.ascontiguousarray(rays)), rays.shape[0], _p(b), bits, _p(keys))
     return keys
+
+
+METHODS = {"lbvh": 0, "ploc": 1, "atr": 2}
+
+
+def binary_tree(verts, tris, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, treelet=9,
+                iterations=2, ct=3.0, ci=2.0, scale=None):
+    """The binary tree a build collapses: dict of left, right, bmin4, bmax4 (2n-1 nodes),
+    sorted_tri, scene_box, scale."""
+    n = tris.shape[0]
+    nn = max(2 * n - 1, 1)
+    d = dict(left=np.zeros(nn, np.int32), right=np.zeros(nn, np.int32), bmin4=np.zeros((nn, 4), np.float32),
+             bmax4=np.zeros((nn, 4), np.float32), sorted_tri=np.zeros(n, np.int32), scene_box=np.zeros(6, np.float32),
+             scale=np.zeros(3, np.float32))
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    load().or_binary_tree(_p(verts), _p(tris), n, METHODS[method], bits, radius, max_radius, adaptive_r, treelet,
+                          iterations, ct, ci, _p(s_in), _p(d["left"]), _p(d["right"]), _p(d["bmin4"]),
+                          _p(d["bmax4"]), _p(d["sorted_tri"]), _p(d["scene_box"]), _p(d["scale"]))
+    return d
+
+
+def collapse_wide(n, left, right, bmin4, bmax4, sorted_tri, width, ct=3.0, ci=2.0, adaptive=1, max_leaf=8):
+    """BVH::collapseAdaptiveWide / collapseWide + BVHConverter::convert, restated:
+    (nodes [count, 8*width] int32, triangle order, (interior, leaves))."""
+    nodes = np.zeros((max(2 * n - 1, 2), 8 * width), np.int32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    c = load().or_collapse_wide(n, _p(np.ascontiguousarray(sorted_tri, np.int32)),
+                                _p(np.ascontiguousarray(left, np.int32)), _p(np.ascontiguousarray(right, np.int32)),
+                                _p(np.ascontiguousarray(bmin4, np.float32)),
+                                _p(np.ascontiguousarray(bmax4, np.float32)), width, ct, ci,
+                                0x7FFFFFFF if adaptive else max_leaf, _p(nodes), _p(tri), _p(counts))
+    return nodes[:c], tri[:n], (int(counts[0]), int(counts[1]))
+
+
+def build_wide(verts, tris, width, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, treelet=9,
+               iterations=2, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+    """Whole build into the Quad (4) or Oct (8) layout: dict of nodes, woop, tri_idx, counts, box, scale."""
+    n = tris.shape[0]
+    nodes = np.zeros((max(2 * n - 1, 2), 8 * width), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    c = load().or_build_wide(_p(verts), _p(tris), n, METHODS[method], bits, radius, max_radius, adaptive_r, treelet,
+                             iterations, ct, ci, adaptive, max_leaf, width, _p(s_in), _p(nodes), _p(woop), _p(tri),
+                             _p(counts), _p(box), _p(sc))
+    return dict(nodes=nodes[:c], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
 
 
 def cost(nodes, scene_box, ct=3.0, ci=2.0):

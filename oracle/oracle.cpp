@@ -959,6 +959,292 @@ int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int b
                            size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
 }
 
+// ---- wide layouts (Quad / Oct) ------------------------------------------------------
+// BVHCollapser::collapseAdaptive / collapse for layouts other than Bin
+// (rt/bvh/BVHCollapser.cpp:521-660): the binary tree becomes a host BVH whose
+// references are renumbered in left-first depth-first order (convert,
+// :339-413; writeTriangleIndices, :497-519), BVH::collapseAdaptiveWide(N) /
+// collapseWide(N, maxLeafSize) (rt/bvh/BVH.h:94-160, 228-292, 401-423) turns
+// it into an N-wide tree, and BVHConverter::convert (rt/bvh/BVHConverter.cpp:
+// 13-89) numbers it breadth first (interior nodes from 0, leaves after them).
+//
+// Cost model per binary node v and child budget j = 1..N-1 (recomputeCostsWide):
+//   leaf(v)    = ci * A(v) / A(root) * ceil(size/N) * N   (MAX_FLOAT if size > maxLeaf)
+//   cost[0]    = min(leaf(v), ct * A(v) / A(root) + min_k cost_l[k-1] + cost_r[N-k-1])
+//   cost[j-1]  = min(cost[j-2], min_k cost_l[k-1] + cost_r[j-k-1])        j >= 2
+// with the first minimum kept on ties and counts (k, j-k) or (-1, -1) for a
+// leaf. A = AABB::area, 2 * (dx*dy + dy*dz + dz*dx), evaluated as written.
+// collapseWide: a node with budget k starts from its two children with the
+// counts of count[k-1]; while it has fewer than N children, the first child
+// whose counts (l, r) are both positive with l + r < N is replaced by its
+// two children; children whose counts are (-1, -1) become leaves.
+// One deviation: when the root's best choice is a leaf (small meshes), the
+// reference reads count[-2] of the root's children (undefined); here the root
+// then takes its best interior split.
+namespace {
+
+inline float host_area(const float* mn, const float* mx) {
+    if (!(mn[0] <= mx[0] && mn[1] <= mx[1] && mn[2] <= mx[2])) return 0.0f;
+    const float dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+struct wide_dp {
+    std::vector<float> cost;   // [nn][N-1]
+    std::vector<int8_t> cl, cr; // counts, -1 for a leaf
+    std::vector<int8_t> bl, br; // best interior split of budget 1 (root fallback)
+};
+
+}  // namespace
+
+extern "C" {
+
+// nodes_out: count * 8 * width int32; tri_idx_out: n. Returns the node count.
+int64_t or_collapse_wide(int n, const int32_t* sorted_tri, const int32_t* left, const int32_t* right,
+                         const float* bmin4, const float* bmax4, int width, float ct, float ci, int max_leaf,
+                         int32_t* nodes_out, int32_t* tri_idx_out, int32_t* counts) {
+    const int N = width, W = 8 * width;
+    counts[0] = counts[1] = 0;
+    if (n < 1 || (N != 4 && N != 8)) return 0;
+    auto box = [&](int v, float* mn, float* mx) {
+        for (int a = 0; a < 3; ++a) { mn[a] = bmin4[4 * v + a]; mx[a] = bmax4[4 * v + a]; }
+    };
+    auto put_box = [&](int32_t* nd, int i, const float* mn, const float* mx) {
+        std::memcpy(&nd[4 * i + 0], &mn[0], 4); std::memcpy(&nd[4 * i + 1], &mx[0], 4);
+        std::memcpy(&nd[4 * i + 2], &mn[1], 4); std::memcpy(&nd[4 * i + 3], &mx[1], 4);
+        std::memcpy(&nd[4 * (N + i) + 0], &mn[2], 4); std::memcpy(&nd[4 * (N + i) + 1], &mx[2], 4);
+    };
+    if (n == 1) {  // root with the single triangle's leaf
+        tri_idx_out[0] = sorted_tri[0];
+        float mn[3], mx[3];
+        box(0, mn, mx);
+        int32_t* root = nodes_out;
+        int32_t* leaf = nodes_out + W;
+        std::memset(root, 0, 2 * W * 4);
+        const float dmx[3] = {mn[0], mn[1], mn[2]};
+        for (int i = 0; i < N; ++i) {
+            put_box(root, i, mn, i == 0 ? mx : dmx);
+            root[4 * (N + i) + 2] = ~1;
+            put_box(leaf, i, mn, mx);
+        }
+        root[8 * N - 9] = 1; root[8 * N - 5] = 1; root[8 * N - 1] = -1;
+        leaf[4 * N + 2] = 0; leaf[4 * N + 3] = 1; leaf[8 * N - 9] = 0; leaf[8 * N - 5] = ~1; leaf[8 * N - 1] = 0;
+        counts[0] = 1; counts[1] = 1;
+        return 2;
+    }
+    const int nn = 2 * n - 1;
+    // depth-first (left first) reference order: begin/end of every node
+    std::vector<int> beg(nn), end(nn), order;
+    order.reserve(nn);
+    {
+        int pos = 0;
+        std::vector<int> st{0};
+        while (!st.empty()) {
+            int v = st.back();
+            st.pop_back();
+            order.push_back(v);  // preorder
+            if (v >= n - 1) { tri_idx_out[pos] = sorted_tri[v - (n - 1)]; beg[v] = pos; end[v] = ++pos; continue; }
+            st.push_back(right[v]);
+            st.push_back(left[v]);
+        }
+        for (int k = nn - 1; k >= 0; --k) {
+            const int v = order[k];
+            if (v < n - 1) { beg[v] = beg[left[v]]; end[v] = end[right[v]]; }
+        }
+    }
+    // recomputeCostsWide, children before parents (reverse preorder)
+    const int J = N - 1;
+    wide_dp D;
+    D.cost.assign((size_t)nn * J, 0.0f);
+    D.cl.assign((size_t)nn * J, -1); D.cr.assign((size_t)nn * J, -1);
+    D.bl.assign(nn, -1); D.br.assign(nn, -1);
+    float rmn[3], rmx[3];
+    box(0, rmn, rmx);
+    const float root_area = host_area(rmn, rmx);
+    for (int k = nn - 1; k >= 0; --k) {
+        const int v = order[k];
+        float mn[3], mx[3];
+        box(v, mn, mx);
+        const float A = host_area(mn, mx);
+        const int size = end[v] - beg[v];
+        float* c = &D.cost[(size_t)v * J];
+        int8_t* xl = &D.cl[(size_t)v * J];
+        int8_t* xr = &D.cr[(size_t)v * J];
+        if (v >= n - 1) {
+            for (int j = 1; j < N; ++j) {
+                c[j - 1] = ci * A / root_area * (float)((size + N - 1) / N) * (float)N;
+                xl[j - 1] = xr[j - 1] = -1;
+            }
+            continue;
+        }
+        const float* c0 = &D.cost[(size_t)left[v] * J];
+        const float* c1 = &D.cost[(size_t)right[v] * J];
+        const float leaf_cost = size > max_leaf ? MAXF : ci * A / root_area * (float)((size + N - 1) / N) * (float)N;
+        float sub = ct * A / root_area;
+        float dist = MAXF;
+        int bk = 0;
+        for (int kk = 1; kk < N; ++kk) {
+            const float cc = c0[kk - 1] + c1[N - kk - 1];
+            if (dist > cc) { dist = cc; bk = kk; }
+        }
+        sub += dist;
+        D.bl[v] = (int8_t)bk;
+        D.br[v] = (int8_t)(N - bk);
+        if (leaf_cost > sub) { c[0] = sub; xl[0] = (int8_t)bk; xr[0] = (int8_t)(N - bk); }
+        else { c[0] = leaf_cost; xl[0] = xr[0] = -1; }
+        for (int j = 2; j < N; ++j) {
+            dist = MAXF;
+            for (int kk = 1; kk < j; ++kk) {
+                const float cc = c0[kk - 1] + c1[j - kk - 1];
+                if (dist > cc) { dist = cc; bk = kk; }
+            }
+            if (c[j - 2] <= dist) { c[j - 1] = c[j - 2]; xl[j - 1] = xl[j - 2]; xr[j - 1] = xr[j - 2]; }
+            else { c[j - 1] = dist; xl[j - 1] = (int8_t)bk; xr[j - 1] = (int8_t)(j - bk); }
+        }
+    }
+    // collapseWide: children (binary node, budget) of every wide interior node, breadth first
+    struct kid { int v, k; bool leaf; };
+    auto is_leaf_at = [&](int v, int k) { return D.cl[(size_t)v * J + k - 1] < 0; };
+    std::vector<std::vector<kid>> kids;
+    std::vector<int> wnode, wparent;  // binary node of each wide interior node, its wide parent
+    std::vector<std::pair<int, int>> queue{{0, 1}};
+    std::vector<int> qparent{-1};
+    for (size_t h = 0; h < queue.size(); ++h) {
+        const int v = queue[h].first, budget = queue[h].second;
+        int kl = D.cl[(size_t)v * J + budget - 1], kr = D.cr[(size_t)v * J + budget - 1];
+        if (kl < 0) { kl = D.bl[v]; kr = D.br[v]; }  // root whose best choice is a leaf
+        std::vector<int> cv{left[v], right[v]}, ck{kl, kr};
+        while ((int)cv.size() < N) {
+            int sidx = -1;
+            for (int i = 0; i < (int)cv.size(); ++i) {
+                const int lc = D.cl[(size_t)cv[i] * J + ck[i] - 1], rc = D.cr[(size_t)cv[i] * J + ck[i] - 1];
+                if (lc > 0 && rc > 0 && lc + rc < N) { sidx = i; break; }
+            }
+            if (sidx < 0) break;
+            const int x = cv[sidx], b = ck[sidx];
+            const int lc = D.cl[(size_t)x * J + b - 1], rc = D.cr[(size_t)x * J + b - 1];
+            cv[sidx] = left[x]; ck[sidx] = lc;
+            cv.insert(cv.begin() + sidx + 1, right[x]);
+            ck.insert(ck.begin() + sidx + 1, rc);
+        }
+        std::vector<kid> ks;
+        for (size_t i = 0; i < cv.size(); ++i) {
+            const bool lf = is_leaf_at(cv[i], ck[i]);
+            ks.push_back({cv[i], ck[i], lf});
+        }
+        kids.push_back(ks);
+        wnode.push_back(v);
+        wparent.push_back(qparent[h]);
+        for (const kid& c : ks)
+            if (!c.leaf) { queue.push_back({c.v, c.k}); qparent.push_back((int)h); }
+    }
+    // BVHConverter::convert: breadth-first numbering, interior nodes first
+    const int ni = (int)kids.size();
+    int nl = 0;
+    for (const auto& ks : kids)
+        for (const kid& c : ks) nl += c.leaf;
+    std::memset(nodes_out, 0, (size_t)(ni + nl) * W * 4);
+    int next_int = 1, next_leaf = ni;
+    for (int w = 0; w < ni; ++w) {
+        int32_t* nd = nodes_out + (size_t)w * W;
+        const auto& ks = kids[w];
+        for (int i = 0; i < (int)ks.size(); ++i) {
+            float mn[3], mx[3];
+            box(ks[i].v, mn, mx);
+            put_box(nd, i, mn, mx);
+            if (ks[i].leaf) {
+                const int li = next_leaf++;
+                nd[4 * (N + i) + 2] = ~li;
+                int32_t* lf = nodes_out + (size_t)li * W;
+                for (int q = 0; q < N; ++q) put_box(lf, q, mn, mx);
+                lf[4 * N + 2] = beg[ks[i].v];
+                lf[4 * N + 3] = end[ks[i].v];
+                lf[8 * N - 9] = 0;
+                lf[8 * N - 5] = ~(end[ks[i].v] - beg[ks[i].v]);
+                lf[8 * N - 1] = w;
+            } else {
+                nd[4 * (N + i) + 2] = next_int++;  // children are queued in this order
+            }
+        }
+        {  // unused slots: the degenerate box at child 0's minimum corner and child 0's
+           // index as getChildIndex returns it (decoded, also for a leaf child)
+            float mn0[3], mx0[3];
+            box(ks[0].v, mn0, mx0);
+            const int32_t d0 = nd[4 * N + 2];
+            for (int i = (int)ks.size(); i < N; ++i) {
+                put_box(nd, i, mn0, mn0);
+                nd[4 * (N + i) + 2] = d0 < 0 ? ~d0 : d0;
+            }
+        }
+        nd[8 * N - 9] = (int)ks.size();
+        nd[8 * N - 5] = end[wnode[w]] - beg[wnode[w]];
+        nd[8 * N - 1] = wparent[w];
+    }
+    counts[0] = ni;
+    counts[1] = nl;
+    return (int64_t)ni + nl;
+}
+
+}  // extern "C"
+
+// The final binary tree of a build (method 0 LBVH, 1 PLOC, 2 ATR) before its
+// collapse: children, refitted boxes and the sorted reference order.
+void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int method, int bits, int radius,
+                    int max_radius, int adaptive_r, int treelet, int iterations, float ct, float ci,
+                    const float* scale_in, int32_t* left, int32_t* right, float* nbmin4, float* nbmax4,
+                    int32_t* sorted_tri, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    or_sort(n, keys.data(), bits, skeys.data(), sorted_tri);
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), size(nn), state(nn);
+    std::vector<float> cost(nn);
+    if (n == 1) {
+        tri_box(verts, tris, sorted_tri[0], nbmin4, nbmax4);
+        nbmin4[3] = nbmax4[3] = 0.0f;
+        left[0] = 0;
+        right[0] = 1;
+        return;
+    }
+    if (method == 1) {
+        or_ploc(n, verts, tris, sorted_tri, radius, max_radius, adaptive_r, ct, ci, 1, 8, parent.data(), left, right,
+                nbmin4, nbmax4, size.data(), cost.data(), state.data());
+        return;
+    }
+    or_karras(n, skeys.data(), parent.data(), left, right);
+    or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
+             cost.data(), state.data());
+    if (method == 2) {
+        or_atr(n, treelet, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
+        or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
+                 cost.data(), state.data());
+    }
+}
+
+// Whole build into an N-wide layout: the binary tree of the method, the wide
+// collapse, then the Woop triangles in the collapsed reference order.
+int64_t or_build_wide(const float* verts, const int32_t* tris, int64_t n64, int method, int bits, int radius,
+                      int max_radius, int adaptive_r, int treelet, int iterations, float ct, float ci, int adaptive,
+                      int max_leaf, int width, const float* scale_in, int32_t* nodes_out, float* woop4,
+                      int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    counts[0] = counts[1] = 0;
+    if (n == 0) return 0;
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> left(nn), right(nn), sorted(n);
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn);
+    or_binary_tree(verts, tris, n64, method, bits, radius, max_radius, adaptive_r, treelet, iterations, ct, ci,
+                   scale_in, left.data(), right.data(), nbmin.data(), nbmax.data(), sorted.data(), scene_box,
+                   scale_out);
+    const int64_t c = or_collapse_wide(n, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
+                                       width, ct, ci, adaptive ? 0x7fffffff : max_leaf, nodes_out, tri_idx, counts);
+    or_woopify(n, verts, tris, tri_idx, woop4);
+    return c;
+}
+
 // ---- ray generation and ray keys ---------------------------------------------------
 // PixelTable::recalculate (rt/ray/PixelTable.cpp:10-80), walked as the reference
 // does: Morton indices over a square of block coordinates whose side is the

@@ -33,6 +33,9 @@ def load():
         lib.hpref_trace.argtypes = [_P, _P, _P, _P, C.c_int, _P, C.c_int, C.POINTER(C.c_double)]
         lib.hpref_last_error.restype = C.c_char_p
         lib.hpref_last_error.argtypes = []
+        lib.hpref_wide_collapse.restype = C.c_int
+        lib.hpref_wide_collapse.argtypes = [C.c_int, _P, _P, _P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_int,
+                                            C.c_int, _P, _P, _P]
         lib.hpref_bvh_cost.restype = C.c_float
         lib.hpref_bvh_cost.argtypes = [_P, C.c_int, C.c_float, C.c_float, C.c_float]
         _lib = lib
@@ -97,3 +100,21 @@ def trace(nodes, woop, tri_idx, R, any_hit=False):
 
 def cost(nodes, num_nodes, scene_area, ct=3.0, ci=2.0):
     return float(load().hpref_bvh_cost(_p(nodes), num_nodes, scene_area, ct, ci))
+
+
+def wide_collapse(n, left, right, bmin4, bmax4, sorted_tri, width, ct=3.0, ci=2.0, adaptive=1, max_leaf=8):
+    """BVH::collapseAdaptiveWide / collapseWide of the reference (host code, rt/bvh/BVH.h)
+    on a binary tree given as host arrays; returns (nodes [count, 8*width] int32,
+    triangle order, (interior, leaves)), or None when the root's best choice is a leaf."""
+    def p(a):
+        return np.ascontiguousarray(a).ctypes.data_as(C.c_void_p)
+    arrs = [np.ascontiguousarray(a) for a in (left, right, bmin4, bmax4, sorted_tri)]
+    nodes = np.zeros((max(2 * n - 1, 2), 8 * width), np.int32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    c = load().hpref_wide_collapse(n, *[a.ctypes.data_as(C.c_void_p) for a in arrs], width, ct, ci, adaptive,
+                                   max_leaf, nodes.ctypes.data_as(C.c_void_p), tri.ctypes.data_as(C.c_void_p),
+                                   counts.ctypes.data_as(C.c_void_p))
+    if c < 0:
+        return None
+    return nodes[:c], tri[:n], (int(counts[0]), int(counts[1]))
