@@ -43,6 +43,8 @@ class BuildParams:
         for k, v in kw.items():
             if k == "method" and isinstance(v, str):
                 v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR}[v]
+            if k == "layout" and isinstance(v, str):
+                v = {"bin": 2, "quad": 4, "oct": 8}[v]
             setattr(self.c, k, v)
 
     def __getattr__(self, k):
@@ -97,7 +99,8 @@ class Env:
 
 
 class BVH:
-    """A built BVH (HipBVH): 64-byte binary nodes, Woop triangles, triangle indices."""
+    """A built BVH (HipBVH): nodes of its layout (64-byte binary, or Quad / Oct
+    records of 32 * N bytes), Woop triangles, triangle indices."""
 
     def __init__(self, ctx: "Context"):
         self.ctx = ctx
@@ -114,6 +117,11 @@ class BVH:
     @property
     def num_nodes(self):
         return self.c.num_interior + self.c.num_leaf
+
+    @property
+    def layout(self) -> int:
+        """Children per node: 2 (bin), 4 (quad) or 8 (oct)."""
+        return self.c.layout or 2
 
     def cost(self, stream=None) -> float:
         v = C.c_double()
@@ -137,7 +145,7 @@ class BVH:
     def download(self, stream=None):
         """Copy nodes (N x 16 int32), woop (n x 12 float32) and triangle indices to the host."""
         self.sync(stream)
-        nodes = np.zeros((self.num_nodes, 16), np.int32)
+        nodes = np.zeros((self.num_nodes, 8 * self.layout), np.int32)
         woop = np.zeros((self.c.num_refs, 12), np.float32)
         tri = np.zeros(self.c.num_refs, np.int32)
         check(load().hp_bvh_download(self.ctx.h, C.byref(self.c), nodes.ctypes.data, woop.ctypes.data,

@@ -18,6 +18,7 @@ STATUS_NAMES = {0: "HP_OK", 1: "HP_ERR_CUDA", 2: "HP_ERR_ARG", 3: "HP_ERR_OOM", 
 HP_METHOD_LBVH, HP_METHOD_PLOC, HP_METHOD_ATR = 0, 1, 2
 HP_TRACE_ANY_HIT, HP_TRACE_STATS = 1, 2
 HP_BATCH_NO_GRAPH = 0x100
+HP_LAYOUT_BIN, HP_LAYOUT_QUAD, HP_LAYOUT_OCT = 2, 4, 8
 
 
 class hp_mesh(C.Structure):
@@ -30,14 +31,15 @@ class hp_build_params(C.Structure):
                 ("ploc_max_radius", C.c_int32), ("ploc_adaptive", C.c_int32),
                 ("atr_iterations", C.c_int32), ("atr_treelet", C.c_int32), ("ct", C.c_float),
                 ("ci", C.c_float), ("max_leaf_size", C.c_int32), ("adaptive_leaf", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("layout", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class hp_bvh(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("woop", C.c_void_p), ("tri_indices", C.c_void_p),
                 ("num_refs", C.c_int64), ("capacity_refs", C.c_int64), ("num_interior", C.c_int32),
                 ("num_leaf", C.c_int32), ("scene_box", C.c_float * 6), ("morton_scale", C.c_float * 3),
-                ("method", C.c_int32), ("ct", C.c_float), ("ci", C.c_float), ("impl", C.c_void_p)]
+                ("method", C.c_int32), ("ct", C.c_float), ("ci", C.c_float), ("impl", C.c_void_p),
+                ("layout", C.c_int32), ("node_bytes", C.c_int32)]
 
 
 class hp_bvh_stats(C.Structure):

@@ -99,12 +99,17 @@ hp_status check_params(const hp_build_params* p) {
     } else if (p->method != HP_METHOD_LBVH) {
         return hp_fail(HP_ERR_ARG, "unknown build method");
     }
+    if (p->layout != 0 && p->layout != HP_LAYOUT_BIN && p->layout != HP_LAYOUT_QUAD && p->layout != HP_LAYOUT_OCT)
+        return hp_fail(HP_ERR_ARG, "layout must be 2 (bin), 4 (quad) or 8 (oct)");
     return HP_OK;
 }
 
-hp_status bvh_alloc(hp_bvh* out, int64_t n) {
+// Nodes of a tree over n references: at most 2n - 1 (3 for a single reference).
+hp_status bvh_alloc(hp_bvh* out, int64_t n, int layout) {
     hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
-    if (b && b->capacity >= n && b->nodes) return HP_OK;
+    const size_t node_bytes = 32 * (size_t)layout;
+    const size_t need_nodes = (size_t)std::max<int64_t>(2 * std::max<int64_t>(n, 2) - 1, 3) * node_bytes;
+    if (b && b->capacity >= n && b->nodes && b->node_capacity >= need_nodes) return HP_OK;
     if (b) {
         cudaFree(b->nodes);
         cudaFree(b->woop);
@@ -118,8 +123,9 @@ hp_status bvh_alloc(hp_bvh* out, int64_t n) {
     *b = hp_bvh_impl();
     const int64_t cap = std::max<int64_t>(n, 2);
     const int64_t max_nodes = std::max<int64_t>(2 * cap - 1, 3);
+    const size_t node_cap = (size_t)max_nodes * std::max<size_t>(node_bytes, sizeof(hp_node_bin));
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaMalloc(&b->nodes, max_nodes * sizeof(hp_node_bin));
+    if (e == cudaSuccess) e = cudaMalloc(&b->nodes, node_cap);
     if (e == cudaSuccess) e = cudaMalloc(&b->woop, 3 * cap * sizeof(float4));
     if (e == cudaSuccess) e = cudaMalloc(&b->tri_idx, cap * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->counters, cap * sizeof(int32_t));
@@ -132,6 +138,7 @@ hp_status bvh_alloc(hp_bvh* out, int64_t n) {
     }
     HP_CUDA(cudaMemset(b->info, 0, sizeof(hp_bvh_info)));
     b->capacity = cap;
+    b->node_capacity = node_cap;
     out->nodes = b->nodes;
     out->woop = b->woop;
     out->tri_indices = b->tri_idx;
@@ -252,6 +259,7 @@ void hp_build_params_default(hp_build_params* p) {
     p->ci = 2.0f;
     p->max_leaf_size = 8;
     p->adaptive_leaf = 1;
+    p->layout = HP_LAYOUT_BIN;
 }
 
 hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh* out,
@@ -263,8 +271,12 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
     const int64_t n = m->num_triangles;
     if (out->impl && reinterpret_cast<hp_bvh_impl*>(out->impl)->view)
         return hp_fail(HP_ERR_ARG, "hp_build: the output is a view into a batch");
-    HP_TRY(bvh_alloc(out, n));
+    const int layout = hp_layout_of(p);
+    HP_TRY(bvh_alloc(out, n, layout));
     hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
+    b->layout = layout;
+    out->layout = layout;
+    out->node_bytes = 32 * layout;
     out->num_refs = n;
     out->method = p->method;
     out->ct = p->ct;
@@ -299,7 +311,8 @@ hp_status hp_bvh_download(hp_ctx* ctx, hp_bvh* bvh, void* nodes_host, void* woop
     const int64_t count = (int64_t)bvh->num_interior + bvh->num_leaf;
     const int64_t n = bvh->num_refs;
     if (nodes_host && count > 0)
-        HP_CUDA(cudaMemcpy(nodes_host, bvh->nodes, count * sizeof(hp_node_bin), cudaMemcpyDeviceToHost));
+        HP_CUDA(cudaMemcpy(nodes_host, bvh->nodes, count * (size_t)(bvh->node_bytes > 0 ? bvh->node_bytes : 64),
+                           cudaMemcpyDeviceToHost));
     if (woop_host && n > 0)
         HP_CUDA(cudaMemcpy(woop_host, bvh->woop, n * 3 * sizeof(float4), cudaMemcpyDeviceToHost));
     if (tri_host && n > 0)
@@ -363,6 +376,8 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
     if (m->num_triangles != bvh->num_refs) return hp_fail(HP_ERR_ARG, "hp_refit: mesh does not match the BVH");
     if (reinterpret_cast<hp_bvh_impl*>(bvh->impl)->view)
         return hp_fail(HP_ERR_UNSUPPORTED, "hp_refit: a BVH of a batch is rebuilt with hp_batch_build");
+    if (reinterpret_cast<hp_bvh_impl*>(bvh->impl)->layout != HP_LAYOUT_BIN)
+        return hp_fail(HP_ERR_UNSUPPORTED, "hp_refit: only the binary layout is refitted in place (rebuild wide BVHs)");
     return hp_refit_launch(ctx, reinterpret_cast<hp_bvh_impl*>(bvh->impl), bvh->num_refs, m,
                            reinterpret_cast<cudaStream_t>(stream));
 }

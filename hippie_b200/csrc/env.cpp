@@ -349,8 +349,10 @@ hp_status hp_env_build_params(const hp_env* env, hp_build_params* p) {
     char layout[64] = {0};
     HP_TRY(hp_env_get_string(env, "Bvh.method", method, sizeof(method)));
     HP_TRY(hp_env_get_string(env, "Bvh.layout", layout, sizeof(layout)));
-    if (std::strcmp(layout, "bin") != 0)
-        return hp_fail(HP_ERR_UNSUPPORTED, std::string("Bvh.layout ") + layout + " is not supported (bin only)");
+    // HipBVH::HipBVH (rt/bvh/HipBVH.cpp:317-325): "bin", "quad", anything else Oct
+    if (!std::strcmp(layout, "bin")) p->layout = HP_LAYOUT_BIN;
+    else if (!std::strcmp(layout, "quad")) p->layout = HP_LAYOUT_QUAD;
+    else p->layout = HP_LAYOUT_OCT;
     const char* bits_key;
     if (!std::strcmp(method, "lbvh")) { p->method = HP_METHOD_LBVH; bits_key = "Bvh.lbvhMortonCodeBits"; }
     else if (!std::strcmp(method, "ploc")) { p->method = HP_METHOD_PLOC; bits_key = "Bvh.plocMortonCodeBits"; }

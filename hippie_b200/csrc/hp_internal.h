@@ -39,6 +39,8 @@ struct hp_bvh_impl {
     int32_t* counters = nullptr;   // refit termination counters [capacity]
     hp_bvh_info* info = nullptr;   // device
     int64_t capacity = 0;          // references
+    size_t node_capacity = 0;      // bytes of the node buffer
+    int layout = 2;                // children per node: 2, 4 or 8
     bool view = false;             // storage owned by a batch (hp_batch_bvh)
 };
 
@@ -83,6 +85,32 @@ struct hp_carve {
     }
     static size_t pad(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 };
+
+// ---- N-wide layouts (k_wide.cu, k_trace_wide.cu) -------------------------------
+// The final binary tree of a build (root 0, leaf n-1+p holding sorted position p).
+struct hp_wide_in {
+    int n = 0;
+    int width = 4;
+    const int* parent = nullptr;     // [2n-1]
+    const int* left = nullptr;       // interior nodes
+    const int* right = nullptr;
+    const float4* nbmin = nullptr;   // [2n-1], xyz used
+    const float4* nbmax = nullptr;
+    const int32_t* sorted_tri = nullptr;  // sorted position -> triangle
+    bool reorder = true;             // write references (and Woop) in depth-first order
+    float ct = 3.0f, ci = 2.0f;
+    int max_leaf = 0x7fffffff;       // INT_MAX: adaptive leaves
+    const float* verts = nullptr;
+    int64_t nv = 0;
+    const int32_t* tris = nullptr;
+};
+size_t hp_wide_scratch_bytes(int64_t n, int width);
+hp_status hp_wide_collapse(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, void* scratch, cudaStream_t s);
+hp_status hp_wide_single(hp_ctx* ctx, const hp_mesh* m, int width, hp_bvh_impl* out, cudaStream_t s);
+hp_status hp_trace_wide_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                               int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
+                               unsigned long long* counter, const int32_t* order, cudaStream_t s);
+inline int hp_layout_of(const hp_build_params* p) { return p->layout == 0 ? 2 : p->layout; }
 
 // ---- BVH statistics and validation (k_stats.cu) ------------------------------
 hp_status hp_bvh_stats_run(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, cudaStream_t s);
@@ -136,7 +164,7 @@ hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
 size_t hp_ploc_scratch_bytes(int64_t n);
 hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax,
-                        void* scratch, cudaStream_t stream);
+                        void* scratch, void* wide_scratch, cudaStream_t stream);
 // Depth-first collapse of a binary tree (interior nodes 0..n-2, leaves n-1..2n-2,
 // sorted reference p at leaf n-1+p) into 64-byte nodes, the triangle order and
 // Woop triangles. nbmax.w holds each node's size; counts the surviving interior
@@ -162,7 +190,7 @@ size_t hp_atr_scratch_bytes(int64_t n);
 hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out, int n,
                        const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
                        float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
-                       cudaStream_t stream);
+                       void* wide_scratch, cudaStream_t stream);
 hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
                           cudaStream_t stream);
 

@@ -473,7 +473,7 @@ size_t hp_atr_scratch_bytes(int64_t n) {
 hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out, int n,
                        const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
                        float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
-                       cudaStream_t s) {
+                       void* wide_scratch, cudaStream_t s) {
     const int64_t nn = 2 * (int64_t)n - 1;
     const int T = p->atr_treelet;
     if (T < 3 || T > TMAX) return hp_fail(HP_ERR_ARG, "ATR treelet size must be in [3, 32]");
@@ -519,6 +519,25 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
     k_atr_finish<<<hp_div_up(n, 256), 256, 0, s>>>(F);
     HP_CUDA(cudaGetLastError());
     hp_mark(ctx, s, "atr_finish");
+    if (hp_layout_of(p) != 2) {  // N-wide layouts: the final climb has set every box
+        hp_wide_in W;
+        W.n = n;
+        W.width = hp_layout_of(p);
+        W.parent = parent;
+        W.left = left;
+        W.right = right;
+        W.nbmin = nbmin;
+        W.nbmax = nbmax;
+        W.sorted_tri = sorted_tri;
+        W.reorder = true;
+        W.ct = p->ct;
+        W.ci = p->ci;
+        W.max_leaf = p->adaptive_leaf ? 0x7fffffff : p->max_leaf_size;
+        W.verts = m->vertices;
+        W.nv = m->num_vertices;
+        W.tris = m->triangles;
+        return hp_wide_collapse(ctx, W, out, wide_scratch, s);
+    }
     k_size_keys<<<hp_div_up(n, 256), 256, 0, s>>>(n, nbmax, keys);
     k_leaf_order<<<hp_div_up(n, 256), 256, 0, s>>>(n, order);
     HP_CUDA(cudaGetLastError());

@@ -645,6 +645,8 @@ hp_status hp_batch_create(hp_ctx* ctx, const hp_mesh* meshes, int32_t num_meshes
     *out = nullptr;
     if (p->method != HP_METHOD_LBVH)
         return hp_fail(HP_ERR_UNSUPPORTED, "batched builds use the LBVH method");
+    if (p->layout != 0 && p->layout != HP_LAYOUT_BIN)
+        return hp_fail(HP_ERR_UNSUPPORTED, "batched builds use the binary layout");
     if (p->morton_bits < 6 || p->morton_bits > 60) return hp_fail(HP_ERR_ARG, "morton_bits must be in [6,60]");
     if (p->ct <= 0.0f || p->ci <= 0.0f) return hp_fail(HP_ERR_ARG, "ct and ci must be positive");
     if (p->max_leaf_size <= 0 || p->max_leaf_size > 1024) return hp_fail(HP_ERR_ARG, "max_leaf_size must be in (0,1024]");
@@ -799,5 +801,7 @@ hp_status hp_batch_bvh(hp_batch* b, int32_t mesh, hp_bvh* out) {
     out->ct = b->params.ct;
     out->ci = b->params.ci;
     out->impl = &v;
+    out->layout = HP_LAYOUT_BIN;
+    out->node_bytes = 64;
     return HP_OK;
 }

@@ -396,7 +396,10 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
     const bool atr = p->method == HP_METHOD_ATR;
+    const int layout = hp_layout_of(p);
+    const bool wide = layout != 2;
     size_t need = 0;
+    if (wide) need += hp_carve::pad(hp_wide_scratch_bytes(n, layout));
     need += 2 * hp_carve::pad(n * 16);                  // triangle boxes
     need += 2 * hp_carve::pad(n * sizeof(K));           // keys, sorted keys
     need += hp_carve::pad(plan.scratch_bytes);
@@ -422,6 +425,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     K* skeys = cv.take<K>(n);
     void* sort_scratch = cv.take<char>(plan.scratch_bytes);
     uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    void* wide_scratch = wide ? cv.take<char>(hp_wide_scratch_bytes(n, layout)) : nullptr;
     int* err = ctx->d_status;
     hp_bvh_info* info = out->info;
     const int grid_n = hp_div_up(n, TB);
@@ -440,7 +444,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         hp_mark(ctx, s, "morton");
         hp_sort_args sa{keys, nullptr, skeys, sorted_refs, sort_scratch, hist, true, err, ctx};
         HP_TRY(hp_sort_run(plan, sa, s));
-        HP_TRY(hp_ploc_stage(ctx, m, p, out, sorted_refs, tbmin, tbmax, ploc_scratch, s));
+        HP_TRY(hp_ploc_stage(ctx, m, p, out, sorted_refs, tbmin, tbmax, ploc_scratch, wide_scratch, s));
         if (taps) {
             if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
             if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
@@ -477,7 +481,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         hp_count_launch();
         hp_mark(ctx, s, "karras");
         HP_TRY(hp_atr_stage(ctx, m, p, out, (int)n, sorted_refs, parent, left, right, nbmin, nbmax, counters,
-                            tbmin, tbmax, atr_scratch, s));
+                            tbmin, tbmax, atr_scratch, wide_scratch, s));
         if (taps) {
             if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
             if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);
@@ -532,6 +536,25 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                   max_hi, state, p->ct, p->ci, p->adaptive_leaf, p->max_leaf_size, err);
     hp_count_launch();
     hp_mark(ctx, s, "climb");
+    if (wide) {  // N-wide layouts: references stay in sorted (= depth-first) order
+        hp_wide_in W;
+        W.n = (int)n;
+        W.width = layout;
+        W.parent = parent;
+        W.left = left;
+        W.right = right;
+        W.nbmin = nbmin;
+        W.nbmax = nbmax;
+        W.sorted_tri = out->tri_idx;
+        W.reorder = false;
+        W.ct = p->ct;
+        W.ci = p->ci;
+        W.max_leaf = p->adaptive_leaf ? 0x7fffffff : p->max_leaf_size;
+        W.verts = m->vertices;
+        W.nv = m->num_vertices;
+        W.tris = m->triangles;
+        HP_TRY(hp_wide_collapse(ctx, W, out, wide_scratch, s));
+    } else {
     hp_scan_max_excl(max_hi, n, reach, scan_a, err, s);
     k_collapse_flags<<<hp_div_up(nn, TB), TB, 0, s>>>((int)n, left, range, state, max_hi, reach,
                                                      flag_int, flag_leaf);
@@ -542,6 +565,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     HP_CUDA(cudaGetLastError());
     hp_count_launch(2);
     hp_mark(ctx, s, "collapse");
+    }
 
     if (taps) {
         if (taps->morton_keys)
@@ -567,6 +591,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
 hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const hp_build_taps* taps, cudaStream_t s) {
     const int64_t n = m->num_triangles;
+    if (n == 1 && hp_layout_of(p) != 2) return hp_wide_single(ctx, m, hp_layout_of(p), out, s);
     if (n == 1) {
         k_single<<<1, 32, 0, s>>>(m->vertices, m->num_vertices, m->triangles, out->nodes, out->woop,
                                   out->tri_idx, out->info, ctx->d_status);

@@ -623,7 +623,7 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
 
 hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax, void* scratch,
-                        cudaStream_t s) {
+                        void* wide_scratch, cudaStream_t s) {
     const int n = (int)m->num_triangles;
     const int64_t nn = 2 * (int64_t)n - 1;
     const int r_max = p->ploc_adaptive ? p->ploc_max_radius : p->ploc_radius;
@@ -682,6 +682,25 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "ploc_tail");
+    if (hp_layout_of(p) != 2) {  // N-wide layouts
+        hp_wide_in W;
+        W.n = n;
+        W.width = hp_layout_of(p);
+        W.parent = A.parent;
+        W.left = A.left;
+        W.right = A.right;
+        W.nbmin = A.nbmin;
+        W.nbmax = A.nbmax;
+        W.sorted_tri = sorted_tri;
+        W.reorder = true;
+        W.ct = p->ct;
+        W.ci = p->ci;
+        W.max_leaf = p->adaptive_leaf ? 0x7fffffff : p->max_leaf_size;
+        W.verts = m->vertices;
+        W.nv = m->num_vertices;
+        W.tris = m->triangles;
+        return hp_wide_collapse(ctx, W, out, wide_scratch, s);
+    }
     td_args T{};
     T.n = n;
     T.left = A.left;

@@ -44,24 +44,40 @@ struct stats_out {
     unsigned hist[MAX_LEAF + 1];
 };
 
-__device__ __forceinline__ void node_union(const hp_node_bin& n, float* mn, float* mx) {
-    mn[0] = fminf(n.c0xy.x, n.c1xy.x); mx[0] = fmaxf(n.c0xy.y, n.c1xy.y);
-    mn[1] = fminf(n.c0xy.z, n.c1xy.z); mx[1] = fmaxf(n.c0xy.w, n.c1xy.w);
-    mn[2] = fminf(n.cz.x, n.cz.z);     mx[2] = fmaxf(n.cz.y, n.cz.w);
+// A node of width N (HipBVHNodeN<N>, rt/bvh/HipBVHNode.h): N = 2 is the 64-byte
+// binary record, N = 4 / 8 the wide records.
+template <int N>
+struct node_ref {
+    const int* c;
+    __device__ __forceinline__ float lo(int i, int a) const {
+        const int k = a == 0 ? 4 * i : (a == 1 ? 4 * i + 2 : (N == 2 ? 8 + 2 * i : 4 * (N + i)));
+        return __int_as_float(__ldg(c + k));
+    }
+    __device__ __forceinline__ float hi(int i, int a) const {
+        const int k = a == 0 ? 4 * i + 1 : (a == 1 ? 4 * i + 3 : (N == 2 ? 9 + 2 * i : 4 * (N + i) + 1));
+        return __int_as_float(__ldg(c + k));
+    }
+    __device__ __forceinline__ int child(int i) const { return __ldg(c + (N == 2 ? 12 + i : 4 * (N + i) + 2)); }
+    __device__ __forceinline__ int size() const { return __ldg(c + (N == 2 ? 14 : 8 * N - 5)); }
+    __device__ __forceinline__ int parent() const { return __ldg(c + (N == 2 ? 15 : 8 * N - 1)); }
+    __device__ __forceinline__ int count() const { return N == 2 ? 2 : __ldg(c + 8 * N - 9); }
+    __device__ __forceinline__ int begin() const { return __ldg(c + (N == 2 ? 12 : 4 * N + 2)); }
+    __device__ __forceinline__ int end() const { return __ldg(c + (N == 2 ? 13 : 4 * N + 3)); }
+    // HipBVHNodeN::getBoundingBox: the union of all N stored child boxes
+    __device__ __forceinline__ void box(float* mn, float* mx) const {
+        for (int a = 0; a < 3; ++a) { mn[a] = lo(0, a); mx[a] = hi(0, a); }
+        for (int i = 1; i < N; ++i)
+            for (int a = 0; a < 3; ++a) { mn[a] = fminf(mn[a], lo(i, a)); mx[a] = fmaxf(mx[a], hi(i, a)); }
+    }
+};
+
+template <int N>
+__device__ __forceinline__ node_ref<N> node_at(const int* nodes, int64_t i) {
+    return node_ref<N>{nodes + (size_t)i * 8 * N};
 }
 
-__device__ __forceinline__ hp_node_bin load_bin(const hp_node_bin* nodes, int64_t i) {
-    const float4* p = reinterpret_cast<const float4*>(nodes + i);
-    hp_node_bin n;
-    n.c0xy = __ldg(p + 0);
-    n.c1xy = __ldg(p + 1);
-    n.cz = __ldg(p + 2);
-    const float4 m = __ldg(p + 3);
-    n.meta = make_int4(__float_as_int(m.x), __float_as_int(m.y), __float_as_int(m.z), __float_as_int(m.w));
-    return n;
-}
-
-__global__ void __launch_bounds__(SB) k_node_stats(const hp_node_bin* __restrict__ nodes,
+template <int N>
+__global__ void __launch_bounds__(SB) k_node_stats(const int* __restrict__ nodes,
                                                    const hp_bvh_info* __restrict__ info, float ct, float ci,
                                                    double* part_cost, long long* part_leaf, stats_out* out) {
     __shared__ unsigned s_hist[MAX_LEAF + 1];
@@ -77,13 +93,16 @@ __global__ void __launch_bounds__(SB) k_node_stats(const hp_node_bin* __restrict
     double c = 0.0;
     long long leaf = 0;
     for (int64_t i = blockIdx.x * (int64_t)SB + threadIdx.x; i < count; i += (int64_t)SGRID * SB) {
-        const hp_node_bin nd = load_bin(nodes, i);
+        const node_ref<N> nd = node_at<N>(nodes, i);
         float mn[3], mx[3];
-        node_union(nd, mn, mx);
+        nd.box(mn, mx);
         const double a = (double)hp_area(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]) / scene;
-        if (nd.meta.z < 0) {
-            const int size = ~nd.meta.z;
-            c += (double)ci * a * (double)size;
+        const int sz = nd.size();
+        if (sz < 0) {
+            const int size = ~sz;
+            // computeCost: leaves of wide layouts count ceil(size / N) * N references
+            const int billed = N > 2 ? (size + N - 1) / N * N : size;
+            c += (double)ci * a * (double)billed;
             if (i >= num_int) {
                 leaf += size;
                 if (size <= MAX_LEAF) atomicAdd(&s_hist[size], 1u);
@@ -136,7 +155,7 @@ __device__ __forceinline__ void v_fail(int* err, int code, int64_t node) {
 }
 
 struct val_args {
-    const hp_node_bin* nodes;
+    const int* nodes;
     const hp_bvh_info* info;
     const int32_t* tri_idx;
     int64_t n;  // references
@@ -149,6 +168,7 @@ struct val_args {
     int* err;        // [2]
 };
 
+template <int N>
 __global__ void __launch_bounds__(256) k_validate_nodes(val_args V) {
     const int64_t num_int = V.info->num_interior;
     const int64_t count = num_int + V.info->num_leaf;
@@ -159,43 +179,44 @@ __global__ void __launch_bounds__(256) k_validate_nodes(val_args V) {
         return;
     }
     if (i >= count) return;
-    const hp_node_bin nd = load_bin(V.nodes, i);
+    const node_ref<N> nd = node_at<N>(V.nodes, i);
+    const int nsz = nd.size();
     if (i == 0) {
-        if (nd.meta.w != -1) v_fail(V.err, V_ROOT_PARENT, 0);
-        const int64_t rs = nd.meta.z < 0 ? ~nd.meta.z : nd.meta.z;
+        if (nd.parent() != -1) v_fail(V.err, V_ROOT_PARENT, 0);
+        const int64_t rs = nsz < 0 ? ~nsz : nsz;
         if (rs != V.n) v_fail(V.err, V_ROOT_SIZE, 0);
     }
-    if (nd.meta.z >= 0) {
+    if (nsz >= 0) {
         if (i >= num_int) { v_fail(V.err, V_INTERIOR_IN_LEAF_RANGE, i); return; }
+        const int nch = nd.count();
+        if (nch < 1 || nch > N || (nch < 2 && V.n > 1)) { v_fail(V.err, V_CHILD_RANGE, i); return; }
         int64_t size = 0;
-        for (int c = 0; c < 2; ++c) {
-            const int raw = c == 0 ? nd.meta.x : nd.meta.y;
+        for (int c = 0; c < nch; ++c) {
+            const int raw = nd.child(c);
             const int64_t ch = raw < 0 ? ~(int64_t)raw : raw;
             if (ch <= 0 || ch >= count) { v_fail(V.err, V_CHILD_RANGE, i); return; }
-            const hp_node_bin cn = load_bin(V.nodes, ch);
-            if ((raw < 0) != (cn.meta.z < 0)) { v_fail(V.err, V_CHILD_FLAG, i); return; }
-            if (cn.meta.w != i) { v_fail(V.err, V_PARENT, i); return; }
-            size += cn.meta.z < 0 ? ~cn.meta.z : cn.meta.z;
+            const node_ref<N> cn = node_at<N>(V.nodes, ch);
+            const int csz = cn.size();
+            if ((raw < 0) != (csz < 0)) { v_fail(V.err, V_CHILD_FLAG, i); return; }
+            if (cn.parent() != i) { v_fail(V.err, V_PARENT, i); return; }
+            size += csz < 0 ? ~csz : csz;
             atomicAdd(V.node_refs + ch, 1);
-            const bool empty_child = cn.meta.z < 0 && cn.meta.x == cn.meta.y;
+            const bool empty_child = csz < 0 && cn.begin() == cn.end();
             if (!empty_child) {
                 float cmn[3], cmx[3];
-                node_union(cn, cmn, cmx);
-                const float4 xy = c == 0 ? nd.c0xy : nd.c1xy;
-                const float bmn[3] = {xy.x, xy.z, c == 0 ? nd.cz.x : nd.cz.z};
-                const float bmx[3] = {xy.y, xy.w, c == 0 ? nd.cz.y : nd.cz.w};
+                cn.box(cmn, cmx);
                 for (int a = 0; a < 3; ++a)
-                    if (cmn[a] < bmn[a] || cmx[a] > bmx[a]) { v_fail(V.err, V_CHILD_BOX, i); return; }
+                    if (cmn[a] < nd.lo(c, a) || cmx[a] > nd.hi(c, a)) { v_fail(V.err, V_CHILD_BOX, i); return; }
             }
         }
-        if (size != nd.meta.z) v_fail(V.err, V_SIZE, i);
+        if (size != nsz) v_fail(V.err, V_SIZE, i);
     } else {
         if (i < num_int) { v_fail(V.err, V_LEAF_IN_INTERIOR_RANGE, i); return; }
-        const int64_t b = nd.meta.x, e = nd.meta.y;
+        const int64_t b = nd.begin(), e = nd.end();
         if (b > e || b < 0 || e > V.n || (b == e && V.n != 1)) { v_fail(V.err, V_LEAF_BOUNDS, i); return; }
-        if (e - b != ~nd.meta.z) { v_fail(V.err, V_LEAF_SIZE, i); return; }
+        if (e - b != ~nsz) { v_fail(V.err, V_LEAF_SIZE, i); return; }
         float mn[3], mx[3];
-        node_union(nd, mn, mx);
+        nd.box(mn, mx);
         for (int64_t r = b; r < e; ++r) {
             const int32_t t = __ldg(V.tri_idx + r);
             if (t < 0 || t >= V.n) { v_fail(V.err, V_TRI_INDEX, i); return; }
@@ -257,8 +278,10 @@ hp_status hp_bvh_stats_run(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, cu
     stats_out* so = cv.take<stats_out>(1);
     hp_bvh_info* inf = cv.take<hp_bvh_info>(1);
     HP_CUDA(cudaMemsetAsync(so, 0, sizeof(stats_out), s));
-    k_node_stats<<<SGRID, SB, 0, s>>>(reinterpret_cast<const hp_node_bin*>(bvh->nodes), b->info, bvh->ct, bvh->ci,
-                                      pc, pl, so);
+    const int* nodes = reinterpret_cast<const int*>(bvh->nodes);
+    if (b->layout == 4) k_node_stats<4><<<SGRID, SB, 0, s>>>(nodes, b->info, bvh->ct, bvh->ci, pc, pl, so);
+    else if (b->layout == 8) k_node_stats<8><<<SGRID, SB, 0, s>>>(nodes, b->info, bvh->ct, bvh->ci, pc, pl, so);
+    else k_node_stats<2><<<SGRID, SB, 0, s>>>(nodes, b->info, bvh->ct, bvh->ci, pc, pl, so);
     k_stats_final<<<1, 32, 0, s>>>(pc, pl, so);
     HP_CUDA(cudaGetLastError());
     hp_count_launch(2);
@@ -281,13 +304,13 @@ hp_status hp_bvh_stats_run(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, cu
 hp_status hp_bvh_validate_run(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, int32_t* valid, cudaStream_t s) {
     const hp_bvh_impl* b = reinterpret_cast<const hp_bvh_impl*>(bvh->impl);
     const int64_t n = bvh->num_refs;
-    const int64_t cap_nodes = 2 * n + 1;  // 2n - 1, or 3 for a single reference (root + two leaves)
+    const int64_t cap_nodes = 2 * n + 1;  // 2n - 1, or 3 for a single binary reference (root + two leaves)
     const size_t need = hp_carve::pad(cap_nodes * 4) + hp_carve::pad(std::max<int64_t>(n, 1) * 4) +
                         hp_carve::pad(2 * sizeof(int));
     HP_TRY(hp_ctx_reserve(ctx, need, s));
     hp_carve cv(ctx->arena);
     val_args V{};
-    V.nodes = reinterpret_cast<const hp_node_bin*>(bvh->nodes);
+    V.nodes = reinterpret_cast<const int*>(bvh->nodes);
     V.info = b->info;
     V.tri_idx = bvh->tri_indices;
     V.n = n;
@@ -300,7 +323,9 @@ hp_status hp_bvh_validate_run(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, 
     V.err = cv.take<int>(2);
     HP_CUDA(cudaMemsetAsync(ctx->arena, 0, cv.off, s));
     const int64_t grid = hp_div_up(cap_nodes, 256);
-    k_validate_nodes<<<(unsigned)grid, 256, 0, s>>>(V);
+    if (b->layout == 4) k_validate_nodes<4><<<(unsigned)grid, 256, 0, s>>>(V);
+    else if (b->layout == 8) k_validate_nodes<8><<<(unsigned)grid, 256, 0, s>>>(V);
+    else k_validate_nodes<2><<<(unsigned)grid, 256, 0, s>>>(V);
     k_validate_refs<<<(unsigned)grid, 256, 0, s>>>(V);
     HP_CUDA(cudaGetLastError());
     hp_count_launch(2);

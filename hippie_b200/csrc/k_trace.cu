@@ -368,6 +368,8 @@ hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, con
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
     HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     hp_mark(ctx, s, "trace_begin");
+    if (b->layout != 2)
+        return hp_trace_wide_launch(ctx, b, n_refs, rays, num_rays, results, stats, flags, counter, order, s);
     const bool any = flags & HP_TRACE_ANY_HIT, st = (flags & HP_TRACE_STATS) && stats;
     if (any && st) return launch_st<true, true>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);
     if (any) return launch_st<true, false>(ctx, b, n_refs, rays, num_rays, results, stats, counter, order, s);

@@ -40,7 +40,7 @@
 extern "C" {
 #endif
 
-#define HP_ABI_VERSION 1
+#define HP_ABI_VERSION 2
 
 typedef enum hp_status {
     HP_OK = 0,
@@ -58,6 +58,14 @@ typedef enum hp_method {
     HP_METHOD_PLOC = 1,       /* Bvh.method ploc */
     HP_METHOD_ATR = 2         /* Bvh.method atr  (LBVH + agglomerative treelet restructuring) */
 } hp_method;
+
+/* Node layouts: children per node (HipBVH::Layout, rt/bvh/HipBVH.h:23-27). A
+ * node of layout L is 32*L bytes (HipBVHNodeN<L>, rt/bvh/HipBVHNode.h:14-218). */
+typedef enum hp_layout {
+    HP_LAYOUT_BIN = 2,
+    HP_LAYOUT_QUAD = 4,
+    HP_LAYOUT_OCT = 8
+} hp_layout;
 
 /* Trace flags (HipTracer: `anyHit` kernel argument and the traceStats variant). */
 #define HP_TRACE_ANY_HIT 1u
@@ -86,7 +94,8 @@ typedef struct hp_build_params {
     float ci;                 /* > 0                           Bvh.ci              */
     int32_t max_leaf_size;    /* (0,1024]                      Bvh.maxLeafSize     */
     int32_t adaptive_leaf;    /* 0/1                           Bvh.adaptiveLeafSize */
-    int32_t reserved[5];
+    int32_t layout;           /* hp_layout; 0 means Bin        Bvh.layout          */
+    int32_t reserved[4];
 } hp_build_params;
 
 /* A built BVH. Device pointers are owned by the library; release with
@@ -99,6 +108,14 @@ typedef struct hp_build_params {
  *            leaf), [15] parent index (-1 at the root).
  * Interior nodes occupy [0, num_interior) with the root at 0; leaf nodes
  * occupy [num_interior, num_interior + num_leaf).
+ * With layout Quad (N = 4) or Oct (N = 8) a node is HipBVHNodeN<N>
+ * (rt/bvh/HipBVHNode.h:14-114), int[8N]: [4i..4i+3] child i {lo.x, hi.x, lo.y,
+ * hi.y}; [4(N+i)], [4(N+i)+1] child i lo.z, hi.z; [4(N+i)+2] child i's index
+ * (~index for a leaf); [8N-9] child count, [8N-5] size (~size in a leaf),
+ * [8N-1] parent; a leaf holds its box in every child slot and its range
+ * [begin, end) at [4N+2], [4N+3]. Nodes are numbered breadth first, interior
+ * nodes from 0 and leaves after them (BVHConverter::convert). Unused child
+ * slots hold child 0's minimum corner as an empty box and child 0's index.
  * woop holds 3 float4 per leaf-ordered reference (rt/bvh/HipBVHKernels.cu:35-65),
  * tri_indices maps a leaf-ordered reference to its scene triangle. */
 typedef struct hp_bvh {
@@ -114,6 +131,8 @@ typedef struct hp_bvh {
     int32_t method;
     float ct, ci;
     void* impl;               /* library private                              */
+    int32_t layout;           /* hp_layout of the nodes                       */
+    int32_t node_bytes;       /* 32 * layout                                  */
 } hp_bvh;
 
 /* Optional device buffers that receive intermediate results of an LBVH build

@@ -1024,7 +1024,7 @@ int64_t or_collapse_wide(int n, const int32_t* sorted_tri, const int32_t* left, 
         const float dmx[3] = {mn[0], mn[1], mn[2]};
         for (int i = 0; i < N; ++i) {
             put_box(root, i, mn, i == 0 ? mx : dmx);
-            root[4 * (N + i) + 2] = ~1;
+            root[4 * (N + i) + 2] = i == 0 ? ~1 : 1;  // unused slots: child 0's decoded index
             put_box(leaf, i, mn, mx);
         }
         root[8 * N - 9] = 1; root[8 * N - 5] = 1; root[8 * N - 1] = -1;

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(_lib.exported_symbols()) <= set(declared)
-    assert lib.hp_abi_version() == 1
+    assert lib.hp_abi_version() == 2
 
 
 def test_bad_arguments_are_rejected():

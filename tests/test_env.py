@@ -98,7 +98,8 @@ def test_method_and_layout_support():
     with pytest.raises(HPError) as ei:
         hp.Env().read_string("Bvh { method hlbvh }").build_params()
     assert ei.value.status == 6
-    with pytest.raises(HPError):
-        hp.Env().read_string("Bvh { layout quad }").build_params()
+    # HipBVH: "bin", "quad", anything else Oct
+    for text, want in (("bin", 2), ("quad", 4), ("oct", 8), ("octree", 8)):
+        assert hp.Env().read_string("Bvh { layout %s }" % text).build_params().layout == want
     p = hp.Env().read_string("Bvh { method atr\n atrTreeletSize 9\n atrIterations 2 }").build_params()
     assert p.method == hp.HP_METHOD_ATR and p.atr_treelet == 9 and p.atr_iterations == 2
