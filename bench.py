@@ -434,6 +434,50 @@ def extra_large(ctx, steps=3, seed=SEED + 4):
             "rays_total": 2 * w * h}
 
 
+def extra_wide(ctx, cfg, V, T, R, RES, steps=3):
+    """The headline scene in the Quad and Oct layouts (Bvh.layout quad / oct):
+    build time, SAH cost, leaf statistics and trace rate of the same rays, with
+    the hits checked against the binary layout's."""
+    import torch
+    import hippie_b200 as hp
+    s = torch.cuda.current_stream()
+    n, nr = T.shape[0], R.shape[0]
+    kw = dict(method=cfg["method"], morton_bits=cfg["bits"])
+    if cfg["method"] == "ploc":
+        kw.update(ploc_radius=16, ploc_max_radius=256, ploc_adaptive=0)
+    base = ctx.build(V, T, hp.BuildParams(**kw))
+    ctx.trace(base, R, results=RES)
+    torch.cuda.synchronize()
+    want = RES[:, :2].clone()
+    out = {"workload": cfg["workload"] + ", same rays"}
+    for name, layout in (("quad", 4), ("oct", 8)):
+        p = hp.BuildParams(layout=layout, **kw)
+        bvh = ctx.build(V, T, p)
+        ctx.trace(bvh, R, results=RES)
+        torch.cuda.synchronize()
+        same = bool(torch.equal(RES[:, :2], want))
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        for k in range(steps):
+            ev[k][0].record(s)
+            ctx.build(V, T, p, bvh=bvh)
+            ev[k][1].record(s)
+            ctx.trace(bvh, R, results=RES)
+            ev[k][2].record(s)
+        torch.cuda.synchronize()
+        ctx.check()
+        tb = float(np.median([e[0].elapsed_time(e[1]) for e in ev]))
+        tt = float(np.median([e[1].elapsed_time(e[2]) for e in ev]))
+        st = bvh.stats()
+        out[name] = {"build_ms": tb, "build_mtris_s": n / tb / 1e3, "trace_ms": tt,
+                     "trace_mrays_s": nr / tt / 1e3, "sah_cost": st["sah_cost"],
+                     "avg_leaf_size": st["avg_leaf_size"], "nodes": st["num_interior"] + st["num_leaf"],
+                     "hits_equal_binary": same}
+        del bvh
+    out["binary_sah_cost"] = base.cost()
+    del base
+    return out
+
+
 def run_reference(args, cfg, rank):
     """CPU restatement of the path, timed on the host cores (rank 0 only)."""
     if rank != 0:
@@ -700,6 +744,8 @@ def main(argv=None):
         line["reference_kernels_gpu"] = reference_kernels(cfg, V, T, R, v)
     ctx.reset_tune()  # the other workloads run with the default launch choices
     if args.extras:
+        if world == 1:
+            line["wide"] = extra_wide(ctx, cfg, V, T, R, RES)
         del V, T, R, RES
         torch.cuda.empty_cache()
         line["batched"] = extra_batched(ctx, rank=rank, world=world)
