@@ -42,7 +42,7 @@ class BuildParams:
         load().hp_build_params_default(C.byref(self.c))
         for k, v in kw.items():
             if k == "method" and isinstance(v, str):
-                v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR}[v]
+                v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR, "tr": 3}[v]
             if k == "layout" and isinstance(v, str):
                 v = {"bin": 2, "quad": 4, "oct": 8}[v]
             setattr(self.c, k, v)
@@ -201,11 +201,12 @@ class Context:
         check(load().hp_refit(self.h, C.byref(bvh.c), C.byref(m), _stream_ptr(stream)))
 
     def trace(self, bvh: BVH, rays, results=None, stats=None, any_hit=False, stream=None):
-        """rays: float32 (R, 8) CUDA tensor. Returns int32 (R, 4) results (and stats if given)."""
+        """rays: float32 (R, 8) CUDA tensor. Returns int32 (R, 4) results (and stats if given).
+        A miss writes only {-1, tmax}; a buffer allocated here starts zeroed."""
         import torch
         n = rays.shape[0]
         if results is None:
-            results = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+            results = torch.zeros((n, 4), dtype=torch.int32, device=rays.device)
         flags = (HP_TRACE_ANY_HIT if any_hit else 0) | (HP_TRACE_STATS if stats is not None else 0)
         check(load().hp_trace(self.h, C.byref(bvh.c), _ptr(rays), n, _ptr(results), _ptr(stats), flags,
                               _stream_ptr(stream)))
@@ -217,7 +218,7 @@ class Context:
         import torch
         n = rays.shape[0]
         if results is None:
-            results = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+            results = torch.zeros((n, 4), dtype=torch.int32, device=rays.device)
         flags = (HP_TRACE_ANY_HIT if any_hit else 0) | (HP_TRACE_STATS if stats is not None else 0)
         check(load().hp_trace_sorted(self.h, C.byref(bvh.c), _ptr(rays), n, _ptr(results), _ptr(stats), flags,
                                      bits, _ptr(order), _stream_ptr(stream)))

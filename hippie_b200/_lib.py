@@ -19,6 +19,7 @@ HP_METHOD_LBVH, HP_METHOD_PLOC, HP_METHOD_ATR = 0, 1, 2
 HP_TRACE_ANY_HIT, HP_TRACE_STATS = 1, 2
 HP_BATCH_NO_GRAPH = 0x100
 HP_LAYOUT_BIN, HP_LAYOUT_QUAD, HP_LAYOUT_OCT = 2, 4, 8
+HP_METHOD_TR = 3
 
 
 class hp_mesh(C.Structure):

@@ -94,7 +94,9 @@ T* to_device(const std::vector<T>& h) {
     return d;
 }
 
-const char* method_name(int m) { return m == HP_METHOD_PLOC ? "ploc" : (m == HP_METHOD_ATR ? "atr" : "lbvh"); }
+const char* method_name(int m) {
+    return m == HP_METHOD_PLOC ? "ploc" : (m == HP_METHOD_ATR ? "atr" : (m == HP_METHOD_TR ? "tr" : "lbvh"));
+}
 
 int run(int argc, char** argv) {
     if (argc < 2 || !std::strcmp(argv[1], "--help")) {

@@ -96,6 +96,8 @@ hp_status check_params(const hp_build_params* p) {
     } else if (p->method == HP_METHOD_ATR) {
         if (p->atr_iterations < 0 || p->atr_iterations > 25) return hp_fail(HP_ERR_ARG, "atr_iterations must be in [0,25]");
         if (p->atr_treelet < 4 || p->atr_treelet > 30) return hp_fail(HP_ERR_ARG, "atr_treelet must be in [4,30]");
+    } else if (p->method == HP_METHOD_TR) {
+        if (p->atr_iterations < 0 || p->atr_iterations > 25) return hp_fail(HP_ERR_ARG, "iterations must be in [0,25]");
     } else if (p->method != HP_METHOD_LBVH) {
         return hp_fail(HP_ERR_ARG, "unknown build method");
     }

@@ -357,6 +357,7 @@ hp_status hp_env_build_params(const hp_env* env, hp_build_params* p) {
     if (!std::strcmp(method, "lbvh")) { p->method = HP_METHOD_LBVH; bits_key = "Bvh.lbvhMortonCodeBits"; }
     else if (!std::strcmp(method, "ploc")) { p->method = HP_METHOD_PLOC; bits_key = "Bvh.plocMortonCodeBits"; }
     else if (!std::strcmp(method, "atr")) { p->method = HP_METHOD_ATR; bits_key = "Bvh.atrMortonCodeBits"; }
+    else if (!std::strcmp(method, "tr")) { p->method = HP_METHOD_TR; bits_key = "Bvh.trMortonCodeBits"; }
     else return hp_fail(HP_ERR_UNSUPPORTED, std::string("Bvh.method ") + method + " is not supported");
     if (hp_env_get_int(env, "Bvh.maxLeafSize", &iv) == HP_OK) {
         if (iv > 0 && iv <= 1024) p->max_leaf_size = iv;
@@ -378,7 +379,8 @@ hp_status hp_env_build_params(const hp_env* env, hp_build_params* p) {
         else p->ploc_radius = iv;
     }
     if (hp_env_get_bool(env, "Bvh.plocAdaptive", &iv) == HP_OK) p->ploc_adaptive = iv;
-    if (hp_env_get_int(env, "Bvh.atrIterations", &iv) == HP_OK) {
+    // TRBuilder::setIterations (rt/bvh/TRBuilder.cpp:331-334) / ATRBuilder's: [0,25]
+    if (hp_env_get_int(env, p->method == HP_METHOD_TR ? "Bvh.trIterations" : "Bvh.atrIterations", &iv) == HP_OK) {
         if (iv < 0 || iv > 25) warn("Number of iterations must be in range [0,25].");
         else p->atr_iterations = iv;
     }

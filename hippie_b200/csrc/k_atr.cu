@@ -38,6 +38,7 @@
 // A parent is larger than its children and usually far larger, so the waits
 // rarely chain. The output is numbered in left-first preorder.
 #include <algorithm>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include "hp_device.cuh"
 #include "hp_internal.h"
@@ -121,6 +122,22 @@ struct atr_smem {
     float d[DMAX];
 };
 
+// TRBVH (treelet of 7 leaves): per-warp subset boxes, costs and best splits.
+constexpr int TR_T = 7;
+constexpr int TR_SUB = 1 << TR_T;
+struct tr_smem {
+    float4 smn[TR_SUB];  // subset boxes (w unused)
+    float4 smx[TR_SUB];
+    float cost[TR_SUB];
+    uint8_t mask[TR_SUB];
+    int refs[TR_T];      // reference counts of the treelet leaves
+};
+
+// Subsets of 2..5 of the 7 treelet leaves, by size (21, 35, 35, 21): each size
+// depends only on smaller ones.
+__constant__ uint8_t c_tr_subsets[112];
+__constant__ int c_tr_size_off[5];
+
 __device__ __forceinline__ box6 box_of(const float4& lo, const float4& hi) {
     box6 b;
     b.mn[0] = lo.x; b.mn[1] = lo.y; b.mn[2] = lo.z;
@@ -139,16 +156,20 @@ __device__ __forceinline__ void load_node(const atr_args& A, int v, box6& b, flo
 __device__ __forceinline__ bool interior_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(A.n - 1); }
 __device__ __forceinline__ bool node_ok(const atr_args& A, int v) { return (unsigned)v < (unsigned)(2 * A.n - 1); }
 
-// Restructure the treelet rooted at `root` with children l0, r0 (whole warp,
-// converged). root_cost is the cost the climb just computed for the root.
-// Lane k holds treelet leaf k: its node, box, cost, refs and, for an interior
-// node, its two children, fetched together so that each expansion costs one
-// dependent round trip to memory.
-__device__ void atr_treelet(const atr_args& A, int root, float root_cost, int l0, int r0, atr_smem& W,
-                            const uint16_t* rc_of) {
+// formTreelet (TRBuilderUtil.h:141-216) for a treelet of T leaves rooted at
+// `root` with children l0, r0 (whole warp, converged): lane k ends with
+// treelet leaf k (node, box, cost in lo.w, refs in hi.w) and internal node k
+// (the root is internal node 0). Each lane fetches a new treelet leaf together
+// with its children, so an expansion costs one dependent round trip. Returns
+// false (after reporting) on an index out of range.
+struct treelet_lane {
+    int tl, ti;
+    float4 lo, hi;
+};
+
+__device__ bool form_treelet(const atr_args& A, int T, int root, int l0, int r0, treelet_lane& L) {
     const int lane = threadIdx.x & 31;
-    const int T = A.T, n = A.n;
-    // ---- formTreelet: lane k holds treelet leaf k and internal node k
+    const int n = A.n;
     int tl = lane == 0 ? l0 : (lane == 1 ? r0 : -1);
     int ti = lane == 0 ? root : -1;
     int kl = -1, kr = -1;
@@ -198,8 +219,26 @@ __device__ void atr_treelet(const atr_args& A, int root, float root_cost, int l0
     }
     if (bad) {
         if (lane == 0) hp_report(A.err, HP_DEV_BAD_INDEX, root);
-        return;
+        return false;
     }
+    L.tl = tl;
+    L.ti = ti;
+    L.lo = lo;
+    L.hi = hi;
+    return true;
+}
+
+// Restructure the treelet rooted at `root` with children l0, r0 (whole warp,
+// converged) by agglomerative merging. root_cost is the cost the climb just
+// computed for the root.
+__device__ void atr_treelet(const atr_args& A, int root, float root_cost, int l0, int r0, atr_smem& W,
+                            const uint16_t* rc_of) {
+    const int lane = threadIdx.x & 31;
+    const int T = A.T;
+    treelet_lane L;
+    if (!form_treelet(A, T, root, l0, r0, L)) return;
+    const int tl = L.tl, ti = L.ti;
+    const float4 lo = L.lo, hi = L.hi;
     // ---- slots and the distance matrix
     if (lane < T) {
         W.lo[lane] = lo;
@@ -281,15 +320,169 @@ __device__ void atr_treelet(const atr_args& A, int root, float root_cost, int l0
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
-    __shared__ atr_smem s_w[AW];
-    __shared__ uint16_t s_rc[DMAX];  // packed triangle index -> (row << 8) | col
-    for (int e = threadIdx.x; e < DMAX; e += AB) {
-        int row, col;
-        tri_decode(e, row, col);
-        s_rc[e] = (uint16_t)((row << 8) | col);
+// TRBVH treelet optimisation (TRBuilderKernels.cu:12-300) for the treelet at
+// `root` (whole warp, converged): subset boxes and areas, the dynamic
+// programme over subsets in the kernel's partition order and tie rules, and
+// the top-down rebuild when the best cost is below the root's. root_refs is
+// the root's reference count (the leaf term of every subset uses it, as the
+// kernel does), root_cost the cost the climb computed for it. The root keeps
+// its cost; a new internal node takes cost(split of its parent's subset) —
+// for a right child as well, as the kernel stores it.
+__device__ void tr_treelet(const atr_args& A, int root, float root_cost, int root_refs, int l0, int r0, tr_smem& W) {
+    const int lane = threadIdx.x & 31;
+    constexpr int T = TR_T, FULL = TR_SUB - 1;
+    treelet_lane L;
+    if (!form_treelet(A, T, root, l0, r0, L)) return;
+    // subset boxes and areas: lane l builds subsets 4l .. 4l+3
+    box6 leaf[T];
+#pragma unroll
+    for (int i = 0; i < T; ++i) leaf[i] = shfl_box(box_of(L.lo, L.hi), i);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int sub = 4 * lane + q;
+        box6 b;
+        for (int a = 0; a < 3; ++a) { b.mn[a] = MAXF; b.mx[a] = -MAXF; }
+#pragma unroll
+        for (int i = 0; i < T; ++i)
+            if (sub & (1 << i)) b = join(b, leaf[i]);
+        W.smn[sub] = make_float4(b.mn[0], b.mn[1], b.mn[2], 0.0f);
+        W.smx[sub] = make_float4(b.mx[0], b.mx[1], b.mx[2], 0.0f);
+        W.cost[sub] = area_of(b);
+        W.mask[sub] = 0;
     }
-    __syncthreads();
+    __syncwarp();
+    if (lane < T) {
+        W.cost[1 << lane] = L.lo.w;
+        W.refs[lane] = __float_as_int(L.hi.w);
+    }
+    __syncwarp();
+    const float refs = (float)root_refs;
+    auto finish = [&](int sub, float opt, int p) {
+        const float a = W.cost[sub];
+        W.cost[sub] = fminf(__fmaf_rn(A.ct, a, opt), __fmul_rn(__fmul_rn(A.ci, a), refs));
+        W.mask[sub] = (uint8_t)p;
+    };
+    // sizes 2 .. T-2 (processSchedule): partitions (-delta)&s, then (p - delta)&s
+    for (int size = 0; size < 4; ++size) {
+        const int off = c_tr_size_off[size], cnt = c_tr_size_off[size + 1] - off;
+        for (int b0 = 0; b0 < cnt; b0 += 32) {
+            if (b0 + lane < cnt) {
+                const int sub = c_tr_subsets[off + b0 + lane];
+                const int delta = (sub - 1) & sub;
+                int p = (-delta) & sub;
+                float opt = MAXF;
+                int optp = 0;
+                while (p != 0) {
+                    const float c = __fadd_rn(W.cost[p], W.cost[p ^ sub]);
+                    if (c < opt) { opt = c; optp = p; }
+                    p = (p - delta) & sub;
+                }
+                finish(sub, opt, optp);
+            }
+        }
+        __syncwarp();
+    }
+    // size T-1 (processSubsets): four lanes per subset, reduced q0:q2, q1:q3, then 0:1
+    {
+        const int k = lane >> 2, q = lane & 3;
+        const int sub = FULL & ~(1 << k);
+        float opt = MAXF;
+        int optp = 0;
+        if (lane < 4 * T) {
+            const int lm = -(1 << max(k - 1, 0));
+            int base = q + 1;
+            int p = (((base & lm) << 1) | (base & ~lm)) << 1;
+            for (int j = q; j < (1 << (T - 2)) - 1; j += 4) {
+                const float c = __fadd_rn(W.cost[p], W.cost[p ^ sub]);
+                if (c < opt) { opt = c; optp = p; }
+                base += 4;
+                p = (((base & lm) << 1) | (base & ~lm)) << 1;
+            }
+        }
+        for (int i = 2; i > 0; i >>= 1) {
+            const float oo = __shfl_down_sync(HP_FULL_MASK, opt, i);
+            const int op = __shfl_down_sync(HP_FULL_MASK, optp, i);
+            if (oo < opt) { opt = oo; optp = op; }
+        }
+        if (lane < 4 * T && q == 0) finish(sub, opt, optp);
+    }
+    __syncwarp();
+    // the full set: lane l takes 2(l+1) and 2(l+1) + 64, reduced over the warp
+    {
+        float opt = MAXF;
+        int optp = 0;
+        int p = (lane + 1) * 2;
+        for (int j = lane; j < (1 << (T - 1)) - 1; j += 32) {
+            const float c = __fadd_rn(W.cost[p], W.cost[p ^ FULL]);
+            if (c < opt) { opt = c; optp = p; }
+            p += 64;
+        }
+#pragma unroll
+        for (int i = 16; i > 0; i >>= 1) {
+            const float oo = __shfl_down_sync(HP_FULL_MASK, opt, i);
+            const int op = __shfl_down_sync(HP_FULL_MASK, optp, i);
+            if (oo < opt) { opt = oo; optp = op; }
+        }
+        if (lane == 0) finish(FULL, opt, optp);
+    }
+    __syncwarp();
+    // updateTreelet: top-down rebuild by lane 0, rounds of left children then right children
+    int ti_all[T - 1], tl_all[T];
+#pragma unroll
+    for (int i = 0; i < T - 1; ++i) ti_all[i] = __shfl_sync(HP_FULL_MASK, L.ti, i);
+#pragma unroll
+    for (int i = 0; i < T; ++i) tl_all[i] = __shfl_sync(HP_FULL_MASK, L.tl, i);
+    if (lane == 0 && W.cost[FULL] < root_cost) {
+        int rn[T - 1], rs[T - 1], nr = 1, next = 1;
+        rn[0] = root;
+        rs[0] = FULL;
+        while (nr > 0) {
+            int on[T - 1], os[T - 1], no = 0;
+            for (int side = 0; side < 2; ++side)
+                for (int e = 0; e < nr; ++e) {
+                    const int node = rn[e], sub = rs[e];
+                    const int p = W.mask[sub];
+                    const int cs = side == 0 ? p : (p ^ sub);
+                    int child;
+                    if (__popc(cs) > 1) {
+                        if (next >= T - 1 || no >= T - 1) { hp_report(A.err, HP_DEV_BAD_INDEX, root); return; }
+                        child = ti_all[next++];
+                        int r = 0;
+                        for (int i = 0; i < T; ++i)
+                            if (cs & (1 << i)) r += W.refs[i];
+                        const float4 mn = W.smn[cs], mx = W.smx[cs];
+                        __stcg(A.nbmin + child, make_float4(mn.x, mn.y, mn.z, W.cost[p]));
+                        __stcg(A.nbmax + child, make_float4(mx.x, mx.y, mx.z, __int_as_float(r)));
+                        on[no] = child;
+                        os[no] = cs;
+                        ++no;
+                    } else {
+                        child = tl_all[__ffs(cs) - 1];
+                    }
+                    __stcg((side == 0 ? A.left : A.right) + node, child);
+                    __stcg(A.parent + child, node);
+                }
+            for (int e = 0; e < no; ++e) { rn[e] = on[e]; rs[e] = os[e]; }
+            nr = no;
+        }
+    }
+    __threadfence();
+    __syncwarp();
+}
+
+template <bool TR>
+__global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
+    using wsmem = typename std::conditional<TR, tr_smem, atr_smem>::type;
+    __shared__ wsmem s_w[AW];
+    __shared__ uint16_t s_rc[DMAX];  // packed triangle index -> (row << 8) | col
+    if (!TR) {
+        for (int e = threadIdx.x; e < DMAX; e += AB) {
+            int row, col;
+            tri_decode(e, row, col);
+            s_rc[e] = (uint16_t)((row << 8) | col);
+        }
+        __syncthreads();
+    }
     const int warp = threadIdx.x >> 5;
     const int p = blockIdx.x * AB + threadIdx.x;
     const int n = A.n;
@@ -355,7 +548,12 @@ __global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
             const int root = __shfl_sync(HP_FULL_MASK, cur, src);
             const float rc = __shfl_sync(HP_FULL_MASK, cost, src);
             const int l0 = __shfl_sync(HP_FULL_MASK, l, src), r0 = __shfl_sync(HP_FULL_MASK, r, src);
-            atr_treelet(A, root, rc, l0, r0, s_w[warp], s_rc);
+            if constexpr (TR) {
+                const int rr = __shfl_sync(HP_FULL_MASK, refs, src);
+                tr_treelet(A, root, rc, rr, l0, r0, s_w[warp]);
+            } else {
+                atr_treelet(A, root, rc, l0, r0, s_w[warp], s_rc);
+            }
             vote &= vote - 1;
         }
         cur = arrived ? up : -1;
@@ -470,13 +668,37 @@ size_t hp_atr_scratch_bytes(int64_t n) {
     return b;
 }
 
+// The subset table of the TRBVH kernel: subsets of 2..5 of 7 leaves by size,
+// uploaded once per device.
+hp_status tr_tables() {
+    static bool done[64] = {};
+    int dev = 0;
+    HP_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return HP_OK;
+    uint8_t subs[112];
+    int off[5] = {0, 0, 0, 0, 0}, k = 0;
+    for (int size = 2; size <= TR_T - 2; ++size) {
+        off[size - 2] = k;
+        for (int sub = 1; sub < TR_SUB - 1; ++sub)
+            if (__builtin_popcount(sub) == size) subs[k++] = (uint8_t)sub;
+    }
+    off[4] = k;
+    if (k != 112) return hp_fail(HP_ERR_ARG, "TRBVH subset table");
+    HP_CUDA(cudaMemcpyToSymbol(c_tr_subsets, subs, sizeof(subs)));
+    HP_CUDA(cudaMemcpyToSymbol(c_tr_size_off, off, sizeof(off)));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return HP_OK;
+}
+
 hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out, int n,
                        const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
                        float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
                        void* wide_scratch, cudaStream_t s) {
     const int64_t nn = 2 * (int64_t)n - 1;
-    const int T = p->atr_treelet;
+    const bool tr = p->method == HP_METHOD_TR;  // TRBVH: dynamic programming over treelets of 7
+    const int T = tr ? TR_T : p->atr_treelet;
     if (T < 3 || T > TMAX) return hp_fail(HP_ERR_ARG, "ATR treelet size must be in [3, 32]");
+    if (tr) HP_TRY(tr_tables());
     if (p->atr_iterations < 0) return hp_fail(HP_ERR_ARG, "ATR iterations must be >= 0");
     hp_carve cv(reinterpret_cast<char*>(scratch));
     uint8_t* state = cv.take<uint8_t>(nn);
@@ -502,10 +724,11 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
         A.gamma = gamma;
         A.init = (i == 0);
         HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
-        k_atr_iter<<<hp_div_up(n, AB), AB, 0, s>>>(A);
+        if (tr) k_atr_iter<true><<<hp_div_up(n, AB), AB, 0, s>>>(A);
+        else k_atr_iter<false><<<hp_div_up(n, AB), AB, 0, s>>>(A);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
-        hp_mark(ctx, s, "atr_iteration");
+        hp_mark(ctx, s, tr ? "tr_iteration" : "atr_iteration");
         ++runs;
         gamma *= 2;
         if (gamma > n) break;

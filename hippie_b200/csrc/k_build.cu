@@ -395,7 +395,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits, ctx->tune.sort_block);
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
-    const bool atr = p->method == HP_METHOD_ATR;
+    const bool atr = p->method == HP_METHOD_ATR || p->method == HP_METHOD_TR;  // treelet restructuring
     const int layout = hp_layout_of(p);
     const bool wide = layout != 2;
     size_t need = 0;

@@ -56,7 +56,9 @@ typedef enum hp_status {
 typedef enum hp_method {
     HP_METHOD_LBVH = 0,       /* Bvh.method lbvh */
     HP_METHOD_PLOC = 1,       /* Bvh.method ploc */
-    HP_METHOD_ATR = 2         /* Bvh.method atr  (LBVH + agglomerative treelet restructuring) */
+    HP_METHOD_ATR = 2,        /* Bvh.method atr  (LBVH + agglomerative treelet restructuring) */
+    HP_METHOD_TR = 3          /* Bvh.method tr   (LBVH + treelet restructuring by dynamic programming,
+                                 treelet 7: TRBuilder) */
 } hp_method;
 
 /* Node layouts: children per node (HipBVH::Layout, rt/bvh/HipBVH.h:23-27). A
@@ -88,7 +90,7 @@ typedef struct hp_build_params {
     int32_t ploc_radius;      /* [1,ploc_max_radius]           Bvh.plocRadius      */
     int32_t ploc_max_radius;  /* >= 1                          Bvh.plocMaxRadius   */
     int32_t ploc_adaptive;    /* 0/1                           Bvh.plocAdaptive    */
-    int32_t atr_iterations;   /* [0,25]                        Bvh.atrIterations   */
+    int32_t atr_iterations;   /* [0,25]                        Bvh.atrIterations (tr: Bvh.trIterations) */
     int32_t atr_treelet;      /* [4,30]                        Bvh.atrTreeletSize  */
     float ct;                 /* > 0                           Bvh.ct              */
     float ci;                 /* > 0                           Bvh.ci              */

@@ -37,6 +37,9 @@ _SIGS = {
     "or_pixel_table": (C.c_int32, [C.c_int32, C.c_int32, _P]),
     "or_primary_rays": (None, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P, _P]),
     "or_ray_keys": (None, [_P, C.c_int64, _P, C.c_int32, _P]),
+    "or_tr": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
+    "or_build_tr": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, _P, _P,
+                                _P, _P, _P, _P, _P]),
     "or_collapse_wide": (C.c_int64, [C.c_int, _P, _P, _P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_int, _P, _P,
                                       _P]),
     "or_binary_tree": (None, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -172,6 +175,27 @@ def build_atr(verts, tris, bits=60, treelet=9, iterations=2, ct=3.0, ci=2.0, ada
     return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
 
 
+def build_tr(verts, tris, bits=60, iterations=2, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+    """LBVH + TRBVH treelet restructuring (treelet 7) + depth-first collapse (TRBuilder::build)."""
+    n = tris.shape[0]
+    cap = max(2 * n - 1, 3)
+    nodes = np.zeros((cap, 16), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    cnt = load().or_build_tr(_p(verts), _p(tris), n, bits, iterations, ct, ci, adaptive, max_leaf, _p(s_in),
+                             _p(nodes), _p(woop), _p(tri), _p(counts), _p(box), _p(sc))
+    return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
+
+
+def tr(n, parent, left, right, bmin4, bmax4, iterations=2, ct=3.0, ci=2.0):
+    """TRBVH iterations in place on a refitted binary tree (arrays over 2n-1 nodes)."""
+    return load().or_tr(n, iterations, ct, ci, _p(parent), _p(left), _p(right), _p(bmin4), _p(bmax4))
+
+
 def atr(n, parent, left, right, bmin4, bmax4, treelet=9, iterations=2, ct=3.0, ci=2.0):
     """ATR iterations in place on a refitted binary tree (arrays over 2n-1 nodes)."""
     return load().or_atr(n, treelet, iterations, ct, ci, _p(parent), _p(left), _p(right), _p(bmin4), _p(bmax4))
@@ -211,7 +235,7 @@ def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1)):
     return keys
 
 
-METHODS = {"lbvh": 0, "ploc": 1, "atr": 2}
+METHODS = {"lbvh": 0, "ploc": 1, "atr": 2, "tr": 3}
 
 
 def binary_tree(verts, tris, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, treelet=9,

@@ -931,6 +931,233 @@ int or_atr(int n, int treelet, int iterations, float ct, float ci, int32_t* pare
     return done;
 }
 
+// ---- TRBVH: treelet restructuring by dynamic programming over subsets
+// (TRBuilder::optimize, rt/bvh/TRBuilder.cpp:137-205; kernel optimize with
+// calculateSubsetSurfaceAreas, processSchedule, processSubsets, updateTreelet,
+// rt/bvh/TRBuilderKernels.cu:12-470; formTreelet, TRBuilderUtil.h:141-216).
+//
+// The climb is ATR's (refs, cost = ct*A + cost(l) + cost(r), leaves ci*A; a
+// node with refs >= gamma is a treelet root, gamma = 7 doubled per
+// iteration). A treelet has T = 7 leaves formed as in ATR. Every subset s of
+// them gets the box of its leaves and A(s); singletons cost their node's cost;
+// then, by increasing size, cost(s) = min(ct*A(s) + best split, ci*A(s)*R)
+// with R the treelet root's reference count, the best split over partitions
+// (p, s^p) in the kernel's enumeration order, first strict minimum kept:
+//   * sizes 2..T-2: p runs over (−delta)&s, then (p − delta)&s, delta =
+//     (s−1)&s;
+//   * size T-1 (bit k cleared): four lanes q take bases q+1, q+5, ..., each
+//     mapped to ((b & m) << 1 | (b & ~m)) << 1, m = −(1 << max(k−1, 0)); the
+//     lanes' minima are reduced q0:q2, q1:q3, then the two winners;
+//   * the full set: lane l takes p = 2(l+1) and p + 64 (while below 127), the
+//     32 minima reduced by shuffle-down halving, the lower lane winning ties.
+// If cost(full) < the root's cost, the treelet is rebuilt top-down from the
+// splits: internal nodes are reused in the order the rounds hand them out
+// (all left children of a round, then all right children), each takes its
+// subset's box, and its cost becomes cost(split) — for a right child as well:
+// the kernel stores costs[partition], not costs[partition ^ subset], and that
+// value feeds later treelets, so it is kept. The root keeps its cost.
+namespace {
+
+void tr_treelet(atr_state& S, int root) {
+    const int T = 7, n = S.n, FULL = (1 << T) - 1;
+    auto box = [&](int v, float* mn, float* mx) {
+        for (int a = 0; a < 3; ++a) { mn[a] = S.bmin4[4 * v + a]; mx[a] = S.bmax4[4 * v + a]; }
+    };
+    auto node_area = [&](int v) {
+        float mn[3], mx[3];
+        box(v, mn, mx);
+        return atr_area(mn, mx);
+    };
+    // formTreelet
+    int tl[T], ti[T - 1];
+    float ta[T];
+    tl[0] = S.left[root];
+    tl[1] = S.right[root];
+    ta[0] = node_area(tl[0]);
+    ta[1] = node_area(tl[1]);
+    ti[0] = root;
+    for (int it = 0; it < T - 2; ++it) {
+        const int m = it + 2;
+        float a[32];
+        for (int k = 0; k < m; ++k) a[k] = tl[k] >= n - 1 ? -MAXF : ta[k];
+        const int idx = warp_argmax(a, m);
+        const int rep = tl[idx];
+        ti[it + 1] = rep;
+        tl[idx] = S.left[rep];
+        tl[m] = S.right[rep];
+        ta[idx] = node_area(tl[idx]);
+        ta[m] = node_area(tl[m]);
+    }
+    // subset boxes and areas
+    float smn[128][3], smx[128][3], cost[128];
+    int mask[128];
+    for (int s = 0; s <= FULL; ++s) {
+        for (int a = 0; a < 3; ++a) { smn[s][a] = MAXF; smx[s][a] = -MAXF; }
+        for (int i = 0; i < T; ++i)
+            if (s & (1 << i)) {
+                float mn[3], mx[3];
+                box(tl[i], mn, mx);
+                for (int a = 0; a < 3; ++a) {
+                    smn[s][a] = std::min(smn[s][a], mn[a]);
+                    smx[s][a] = std::max(smx[s][a], mx[a]);
+                }
+            }
+        cost[s] = atr_area(smn[s], smx[s]);
+        mask[s] = 0;
+    }
+    float area[128];
+    std::memcpy(area, cost, sizeof(area));
+    for (int i = 0; i < T; ++i) cost[1 << i] = S.cost[tl[i]];
+    const float refs = (float)S.refs[root];
+    auto finish = [&](int s, float opt, int p) {
+        cost[s] = std::min(std::fmaf(S.ct, area[s], opt), (S.ci * area[s]) * refs);
+        mask[s] = p;
+    };
+    // sizes 2 .. T-2
+    for (int size = 2; size <= T - 2; ++size)
+        for (int s = 1; s < FULL; ++s) {
+            if (__builtin_popcount(s) != size) continue;
+            float opt = MAXF;
+            int optp = 0;
+            const int delta = (s - 1) & s;
+            int p = (-delta) & s;
+            while (p != 0) {
+                const float c = cost[p] + cost[p ^ s];
+                if (c < opt) { opt = c; optp = p; }
+                p = (p - delta) & s;
+            }
+            finish(s, opt, optp);
+        }
+    // size T-1
+    for (int k = 0; k < T; ++k) {
+        const int s = FULL & ~(1 << k);
+        const int lm = -(1 << std::max(k - 1, 0));
+        const int np = (1 << (T - 2)) - 1;
+        float qo[4];
+        int qp[4];
+        for (int q = 0; q < 4; ++q) {
+            int base = q + 1;
+            float opt = MAXF;
+            int optp = 0;
+            int p = (((base & lm) << 1) | (base & ~lm)) << 1;
+            for (int j = q; j < np; j += 4) {
+                const float c = cost[p] + cost[p ^ s];
+                if (c < opt) { opt = c; optp = p; }
+                base += 4;
+                p = (((base & lm) << 1) | (base & ~lm)) << 1;
+            }
+            qo[q] = opt;
+            qp[q] = optp;
+        }
+        for (int q = 0; q < 2; ++q)
+            if (qo[q + 2] < qo[q]) { qo[q] = qo[q + 2]; qp[q] = qp[q + 2]; }
+        if (qo[1] < qo[0]) { qo[0] = qo[1]; qp[0] = qp[1]; }
+        finish(s, qo[0], qp[0]);
+    }
+    // the full set
+    {
+        float lo[32];
+        int lp[32];
+        const int np = (1 << (T - 1)) - 1;
+        for (int l = 0; l < 32; ++l) {
+            float opt = MAXF;
+            int optp = 0;
+            int p = (l + 1) * 2;
+            for (int j = l; j < np; j += 32) {
+                const float c = cost[p] + cost[p ^ FULL];
+                if (c < opt) { opt = c; optp = p; }
+                p += 64;
+            }
+            lo[l] = opt;
+            lp[l] = optp;
+        }
+        for (int off = 16; off > 0; off >>= 1)
+            for (int l = 0; l < 32; ++l)
+                if (l + off < 32 && lo[l + off] < lo[l]) { lo[l] = lo[l + off]; lp[l] = lp[l + off]; }
+        finish(FULL, lo[0], lp[0]);
+    }
+    // updateTreelet
+    if (!(cost[FULL] < S.cost[root])) return;
+    std::vector<std::pair<int, int>> round{{root, FULL}};
+    int next = 1;
+    auto leaf_refs = [&](int s) {
+        int r = 0;
+        for (int i = 0; i < T; ++i)
+            if (s & (1 << i)) r += S.refs[tl[i]];
+        return r;
+    };
+    auto place = [&](int node, int s, int from, bool left_side, std::vector<std::pair<int, int>>& out) {
+        int child;
+        if (__builtin_popcount(s) > 1) {
+            child = ti[next++];
+            for (int a = 0; a < 3; ++a) { S.bmin4[4 * child + a] = smn[s][a]; S.bmax4[4 * child + a] = smx[s][a]; }
+            S.cost[child] = cost[from];
+            S.refs[child] = leaf_refs(s);
+            out.push_back({child, s});
+        } else {
+            child = tl[__builtin_ctz(s)];
+        }
+        (left_side ? S.left : S.right)[node] = child;
+        S.parent[child] = node;
+    };
+    while (!round.empty()) {
+        std::vector<std::pair<int, int>> out;
+        for (auto [node, s] : round) place(node, mask[s], mask[s], true, out);
+        for (auto [node, s] : round) place(node, mask[s] ^ s, mask[s], false, out);
+        round.swap(out);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// TRBVH iterations (treelet 7) on a refitted LBVH in place; returns the count run.
+int or_tr(int n, int iterations, float ct, float ci, int32_t* parent, int32_t* left, int32_t* right, float* bmin4,
+          float* bmax4) {
+    const int T = 7;
+    if (n < 2) return 0;
+    atr_state S;
+    S.n = n; S.T = T; S.ct = ct; S.ci = ci;
+    S.parent = parent; S.left = left; S.right = right; S.bmin4 = bmin4; S.bmax4 = bmax4;
+    S.cost.assign(2 * n - 1, 0.0f);
+    S.refs.assign(2 * n - 1, 0);
+    for (int p = 0; p < n; ++p) {
+        const int j = n - 1 + p;
+        S.cost[j] = ci * atr_area(&bmin4[4 * j], &bmax4[4 * j]);
+        S.refs[j] = 1;
+    }
+    int gamma = T, done = 0;
+    for (int i = 0; i < iterations; ++i) {
+        ++done;
+        std::vector<std::pair<int, bool>> st{{0, false}};
+        while (!st.empty()) {
+            auto [v, expanded] = st.back();
+            if (v >= n - 1) { st.pop_back(); continue; }
+            if (!expanded) {
+                st.back().second = true;
+                st.push_back({right[v], false});
+                st.push_back({left[v], false});
+                continue;
+            }
+            st.pop_back();
+            const int l = left[v], r = right[v];
+            for (int a = 0; a < 3; ++a) {
+                bmin4[4 * v + a] = std::min(bmin4[4 * l + a], bmin4[4 * r + a]);
+                bmax4[4 * v + a] = std::max(bmax4[4 * l + a], bmax4[4 * r + a]);
+            }
+            S.refs[v] = S.refs[l] + S.refs[r];
+            S.cost[v] = std::fmaf(ct, atr_area(&bmin4[4 * v], &bmax4[4 * v]), S.cost[l]) + S.cost[r];
+            if (S.refs[v] >= gamma) tr_treelet(S, v);
+        }
+        gamma *= 2;
+        if (gamma > n) break;
+    }
+    return done;
+}
+
+}  // extern "C"
+
 // Whole ATR build (ATRBuilder::build, rt/bvh/ATRBuilder.cpp:180-236): the LBVH
 // stages, the ATR iterations, then the collapse of the restructured tree.
 int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int bits, int treelet, int iterations,
@@ -953,6 +1180,34 @@ int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int b
     or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
              nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
     or_atr(n, treelet, iterations, ct, ci, parent.data(), left.data(), right.data(), nbmin.data(), nbmax.data());
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    return or_collapse_dfs(n, verts, tris, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
+                           size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
+}
+
+// Whole TRBVH build (TRBuilder::build, rt/bvh/TRBuilder.cpp:207-260): the LBVH
+// stages, the TR iterations, then the collapse of the restructured tree.
+int64_t or_build_tr(const float* verts, const int32_t* tris, int64_t n64, int bits, int iterations, float ct,
+                    float ci, int adaptive, int max_leaf, const float* scale_in, void* nodes_out, float* woop4,
+                    int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    if (n < 2)
+        return or_build_lbvh(verts, tris, n64, bits, ct, ci, adaptive, max_leaf, scale_in, nodes_out, woop4,
+                             tri_idx, counts, scene_box, scale_out);
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    std::vector<int32_t> sorted(n);
+    or_sort(n, keys.data(), bits, skeys.data(), sorted.data());
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), left(nn), right(nn), size(nn), state(nn);
+    or_karras(n, skeys.data(), parent.data(), left.data(), right.data());
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn), cost(nn);
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    or_tr(n, iterations, ct, ci, parent.data(), left.data(), right.data(), nbmin.data(), nbmax.data());
     or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
              nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
     return or_collapse_dfs(n, verts, tris, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
@@ -1187,7 +1442,7 @@ int64_t or_collapse_wide(int n, const int32_t* sorted_tri, const int32_t* left, 
 
 }  // extern "C"
 
-// The final binary tree of a build (method 0 LBVH, 1 PLOC, 2 ATR) before its
+// The final binary tree of a build (method 0 LBVH, 1 PLOC, 2 ATR, 3 TRBVH) before its
 // collapse: children, refitted boxes and the sorted reference order.
 void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int method, int bits, int radius,
                     int max_radius, int adaptive_r, int treelet, int iterations, float ct, float ci,
@@ -1217,8 +1472,9 @@ void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int me
     or_karras(n, skeys.data(), parent.data(), left, right);
     or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
              cost.data(), state.data());
-    if (method == 2) {
-        or_atr(n, treelet, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
+    if (method == 2 || method == 3) {
+        if (method == 2) or_atr(n, treelet, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
+        else or_tr(n, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
         or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
                  cost.data(), state.data());
     }
