@@ -183,85 +183,6 @@ int ref_atr(timer& T, int n, int treelet, int iterations, float ct, float ci, in
     return 0;
 }
 
-// TRBuilder::generateSchedule (rt/bvh/TRBuilder.cpp:59-121): subsets of 2..T-2
-// treelet leaves in rounds of at most 32, each round only after the rounds of
-// the subsets it is built from; rounds run smallest subsets first. The order of
-// subsets inside a round does not change any result (each is independent).
-std::vector<int> tr_schedule(int T) {
-    const int full = (1 << T) - 1;
-    std::vector<std::vector<int>> rounds;
-    std::vector<int> round_of(full + 1, -1);
-    for (int size = 2; size <= T - 2; ++size) {
-        for (int s = 1; s < full; ++s) {
-            if (__builtin_popcount(s) != size) continue;
-            int r = 0;
-            for (int p = (s - 1) & s; p; p = (p - 1) & s)  // every proper non-empty sub-mask
-                if (__builtin_popcount(p) >= 2) r = std::max(r, round_of[p] + 1);
-            while ((int)rounds.size() <= r) rounds.emplace_back();
-            while ((int)rounds[r].size() == 32) {
-                ++r;
-                while ((int)rounds.size() <= r) rounds.emplace_back();
-            }
-            rounds[r].push_back(s);
-            round_of[s] = r;
-        }
-    }
-    std::vector<int> flat;
-    for (auto& rr : rounds) {
-        rr.resize(32, 0);
-        flat.insert(flat.end(), rr.begin(), rr.end());
-    }
-    return flat;
-}
-
-// TRBuilder::computeSurfaceAreas + optimize on a refitted LBVH (treelet 7),
-// with the buffers of TRBuilder::allocate (rt/bvh/TRBuilder.cpp:10-25).
-int ref_tr(timer& T, int n, int iterations, float ct, float ci, int* parent, int* left, int* right, float4* nbmin,
-           float4* nbmax) {
-    const int treelet = 7, nn = 2 * n - 1;
-    const std::vector<int> hs = tr_schedule(treelet);
-    const int rounds = (int)hs.size() / 32;
-    int* schedule = dalloc<int>(hs.size());
-    cudaMemcpy(schedule, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice);
-    const int warps = (n + 31) / 32;
-    const size_t subsets = (size_t)(1 << treelet) * warps;
-    float* areas = dalloc<float>(nn);
-    float* costs = dalloc<float>(nn);
-    int* refs = dalloc<int>(nn);
-    int* counters = dalloc<int>(n);
-    float* subset_areas = dalloc<float>(subsets);
-    float4* subset_min = dalloc<float4>(subsets);
-    float4* subset_max = dalloc<float4>(subsets);
-    int* stack_node = dalloc<int>((size_t)(treelet - 1) * warps);
-    char* stack_mask = dalloc<char>((size_t)(treelet - 1) * warps);
-    int* stack_size = dalloc<int>(warps);
-    int* current = dalloc<int>(warps);
-    T.run([&] { hpref_tr_areas(nn, areas, nbmin, nbmax); });
-    int gamma = treelet, rc = 0;
-    for (int i = 0; i < iterations; ++i) {
-        cudaMemset(counters, 0, n * 4);
-        T.run([&] { hpref_tr_optimize(n, rounds, treelet, gamma, ci, ct, costs, areas, left, right, nbmin, nbmax,
-                                      counters, parent, refs, subset_areas, subset_min, subset_max, schedule, current,
-                                      stack_node, stack_size, stack_mask); });
-        // The next launch climbs parent links with no bound: it only runs on a
-        // tree that is still valid.
-        if (!valid_tree(n, parent, left, right)) {
-            std::fprintf(stderr, "reference TRBVH produced an invalid tree (iteration %d)\n", i);
-            rc = 4;
-            break;
-        }
-        gamma *= 2;
-        if (gamma > n) break;
-    }
-    cudaError_t e = cudaDeviceSynchronize();
-    cudaFree(schedule); cudaFree(areas); cudaFree(costs); cudaFree(refs); cudaFree(counters);
-    cudaFree(subset_areas); cudaFree(subset_min); cudaFree(subset_max); cudaFree(stack_node); cudaFree(stack_mask);
-    cudaFree(stack_size); cudaFree(current);
-    if (rc) return rc;
-    if (e != cudaSuccess) return fail(9, "after TRBVH optimize");
-    return 0;
-}
-
 }  // namespace
 
 extern "C" {
@@ -270,7 +191,7 @@ const char* hpref_last_error(void) { return g_err; }
 
 // Build a BVH with the reference's kernels. method 0 = LBVH, 1 = PLOC, 2 = ATR
 // (LBVH + treelet restructuring; radius carries the treelet size, max_radius
-// the iteration count), 3 = TRBVH (max_radius carries the iteration count).
+// the iteration count).
 // Device inputs: verts, tris. Device outputs: nodes (64 B x (2n-1)), woop
 // (48 B x n), tri_idx (n). Optional device taps (null to skip): morton keys
 // (u64 n) before sorting, sorted keys, sorted reference indices, and the
@@ -350,7 +271,7 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     if (tap_refs) cudaMemcpy(tap_refs, refs0, n * 4, cudaMemcpyDeviceToDevice);
     T.run([&] { hpref_setup_leaves(n, refs0, refs1, tri0, tri1, left, right, nbmin, nbmax, rbmin, rbmax); });
     int iters = 0;
-    if (method == 0 || method == 2 || method == 3) {
+    if (method == 0 || method == 2) {
         T.run([&] { hpref_construct60(n, parent, left, right, keys0); });
         if (!valid_tree(n, parent, left, right)) {
             std::fprintf(stderr, "reference construct60 produced an invalid tree\n");
@@ -360,10 +281,6 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
         cudaMemset(counters, 0, n * 4);
         T.run([&] { hpref_refit(nn, counters, parent, left, right, nbmin, nbmax); });
         cudaFree(counters);
-        if (method == 3) {
-            const int rc = ref_tr(T, n, max_radius, ct, ci, parent, left, right, nbmin, nbmax);
-            if (rc) return rc;
-        }
         if (method == 2) {
             const int rc = ref_atr(T, n, radius, max_radius, ct, ci, parent, left, right, nbmin, nbmax);
             if (rc) return rc;

@@ -46,13 +46,6 @@ void hpref_atr_optimize(int n, int treelet, int schedule_size, int dist_size, in
                         float* costs, float* areas, float* dist_mats, int* left, int* right, float4* nbmin,
                         float4* nbmax, int* counters, int* parent, int* subtree_refs, int* schedule, int smem);
 
-// w_tr.cu
-void hpref_tr_areas(int nodes, float* areas, float4* nbmin, float4* nbmax);
-void hpref_tr_optimize(int n, int rounds, int treelet, int gamma, float ci, float ct, float* costs, float* areas,
-                       int* left, int* right, float4* nbmin, float4* nbmax, int* counters, int* parent,
-                       int* subtree_refs, float* subset_areas, float4* subset_min, float4* subset_max, int* schedule,
-                       int* current_internal, int* stack_node, int* stack_size, char* stack_mask);
-
 // w_bvh.cu
 void hpref_woopify(int n, int* tri_idx, const int* tris, const float* verts, float4* woop);
 float hpref_cost(int nodes, float scene_area, float ct, float ci, void* bin_nodes);

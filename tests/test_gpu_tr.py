@@ -1,14 +1,13 @@
 """TRBVH (treelet restructuring by dynamic programming over 7-leaf treelets,
-TRBuilder) on the GPU: against the CPU oracle (bit-exact nodes, triangle order
-and Woop triangles) and against the reference's own TRBVH kernels (canonical
-trees), sm_100a."""
+TRBuilder) on the GPU against the CPU oracle: bit-exact nodes, triangle order
+and Woop triangles, sm_100a. (The reference's own TRBVH kernels are not run:
+see the parity notes of the design document.)"""
 import numpy as np
 import pytest
 import torch
 
 import hippie_b200 as hp
 import oracle
-from oracle import ref_harness as R
 
 pytestmark = pytest.mark.gpu
 
@@ -90,17 +89,3 @@ def test_tr_wide_layouts(ctx, layout):
     ref = oracle.build_wide(v, t, layout, method="tr", bits=60, iterations=2,
                             scale=np.array(bvh.c.morton_scale, np.float32))
     np.testing.assert_array_equal(bvh.download()[0], ref["nodes"])
-
-
-@pytest.mark.skipif(not R.available(), reason="reference harness not built (needs /root/reference)")
-@pytest.mark.parametrize("kind,n,bits", [("uniform", 65536, 30), ("clustered", 131072, 60), ("mixed", 100000, 60)])
-def test_tr_matches_reference_kernels(ctx, kind, n, bits):
-    v, t = _mesh(kind, n, 400 + n)
-    V, T = dev(v), dev(t)
-    bvh = ctx.build(V, T, hp.BuildParams(method="tr", morton_bits=bits, atr_iterations=2))
-    bvh.sync()
-    box = np.array(bvh.c.scene_box, np.float32)
-    ref = R.build(V, T, box, method="tr", bits=bits, iterations=2)
-    nodes, woop, tri = bvh.download()
-    assert (bvh.c.num_interior, bvh.c.num_leaf) == tuple(ref["counts"].tolist())
-    assert canonical(nodes, tri) == canonical(ref["nodes"], ref["tri_idx"])
