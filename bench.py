@@ -478,6 +478,47 @@ def extra_wide(ctx, cfg, V, T, R, RES, steps=3):
     return out
 
 
+def extra_methods(ctx, cfg, V, T, R, RES, steps=3):
+    """The headline scene built by the other builders of the path (Bvh.method lbvh,
+    hlbvh, atr, tr; 60-bit keys, the reference's defaults): build time, SAH cost
+    and trace rate of the same rays, with the hits checked against the headline
+    build's."""
+    import torch
+    import hippie_b200 as hp
+    s = torch.cuda.current_stream()
+    n, nr = T.shape[0], R.shape[0]
+    kw = dict(method=cfg["method"], morton_bits=cfg["bits"])
+    if cfg["method"] == "ploc":
+        kw.update(ploc_radius=16, ploc_max_radius=256, ploc_adaptive=0)
+    base = ctx.build(V, T, hp.BuildParams(**kw))
+    ctx.trace(base, R, results=RES)
+    torch.cuda.synchronize()
+    want = RES[:, :2].clone()
+    out = {"workload": cfg["workload"] + ", same rays", "headline_sah_cost": base.cost()}
+    del base
+    for method in ("lbvh", "hlbvh", "atr", "tr"):
+        p = hp.BuildParams(method=method, morton_bits=60)
+        bvh = ctx.build(V, T, p)
+        ctx.trace(bvh, R, results=RES)
+        torch.cuda.synchronize()
+        same = bool(torch.equal(RES[:, :2], want))
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        for k in range(steps):
+            ev[k][0].record(s)
+            ctx.build(V, T, p, bvh=bvh)
+            ev[k][1].record(s)
+            ctx.trace(bvh, R, results=RES)
+            ev[k][2].record(s)
+        torch.cuda.synchronize()
+        ctx.check()
+        tb = float(np.median([e[0].elapsed_time(e[1]) for e in ev]))
+        tt = float(np.median([e[1].elapsed_time(e[2]) for e in ev]))
+        out[method] = {"build_ms": tb, "build_mtris_s": n / tb / 1e3, "trace_ms": tt,
+                       "trace_mrays_s": nr / tt / 1e3, "sah_cost": bvh.cost(), "hits_equal_headline": same}
+        del bvh
+    return out
+
+
 def run_reference(args, cfg, rank):
     """CPU restatement of the path, timed on the host cores (rank 0 only)."""
     if rank != 0:
@@ -746,6 +787,7 @@ def main(argv=None):
     if args.extras:
         if world == 1:
             line["wide"] = extra_wide(ctx, cfg, V, T, R, RES)
+            line["methods"] = extra_methods(ctx, cfg, V, T, R, RES)
         del V, T, R, RES
         torch.cuda.empty_cache()
         line["batched"] = extra_batched(ctx, rank=rank, world=world)

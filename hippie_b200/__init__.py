@@ -42,7 +42,7 @@ class BuildParams:
         load().hp_build_params_default(C.byref(self.c))
         for k, v in kw.items():
             if k == "method" and isinstance(v, str):
-                v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR, "tr": 3}[v]
+                v = {"lbvh": HP_METHOD_LBVH, "ploc": HP_METHOD_PLOC, "atr": HP_METHOD_ATR, "tr": 3, "hlbvh": 4}[v]
             if k == "layout" and isinstance(v, str):
                 v = {"bin": 2, "quad": 4, "oct": 8}[v]
             setattr(self.c, k, v)

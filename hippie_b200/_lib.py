@@ -20,6 +20,7 @@ HP_TRACE_ANY_HIT, HP_TRACE_STATS = 1, 2
 HP_BATCH_NO_GRAPH = 0x100
 HP_LAYOUT_BIN, HP_LAYOUT_QUAD, HP_LAYOUT_OCT = 2, 4, 8
 HP_METHOD_TR = 3
+HP_METHOD_HLBVH = 4
 
 
 class hp_mesh(C.Structure):
@@ -32,7 +33,7 @@ class hp_build_params(C.Structure):
                 ("ploc_max_radius", C.c_int32), ("ploc_adaptive", C.c_int32),
                 ("atr_iterations", C.c_int32), ("atr_treelet", C.c_int32), ("ct", C.c_float),
                 ("ci", C.c_float), ("max_leaf_size", C.c_int32), ("adaptive_leaf", C.c_int32),
-                ("layout", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("layout", C.c_int32), ("hlbvh_sah_bits", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class hp_bvh(C.Structure):

@@ -95,7 +95,13 @@ T* to_device(const std::vector<T>& h) {
 }
 
 const char* method_name(int m) {
-    return m == HP_METHOD_PLOC ? "ploc" : (m == HP_METHOD_ATR ? "atr" : (m == HP_METHOD_TR ? "tr" : "lbvh"));
+    switch (m) {
+    case HP_METHOD_PLOC: return "ploc";
+    case HP_METHOD_ATR: return "atr";
+    case HP_METHOD_TR: return "tr";
+    case HP_METHOD_HLBVH: return "hlbvh";
+    default: return "lbvh";
+    }
 }
 
 int run(int argc, char** argv) {

@@ -98,6 +98,13 @@ hp_status check_params(const hp_build_params* p) {
         if (p->atr_treelet < 4 || p->atr_treelet > 30) return hp_fail(HP_ERR_ARG, "atr_treelet must be in [4,30]");
     } else if (p->method == HP_METHOD_TR) {
         if (p->atr_iterations < 0 || p->atr_iterations > 25) return hp_fail(HP_ERR_ARG, "iterations must be in [0,25]");
+    } else if (p->method == HP_METHOD_HLBVH) {
+        // HLBVHBuilder::setMortonCodeSAHBits (rt/bvh/HLBVHBuilder.cpp:431-435) takes [6,15] up to the Morton
+        // bits; only multiples of 3 give every axis whole bins, so the others are not supported.
+        if (p->hlbvh_sah_bits < 6 || p->hlbvh_sah_bits > 15 || p->hlbvh_sah_bits > p->morton_bits)
+            return hp_fail(HP_ERR_ARG, "hlbvh_sah_bits must be in [6,15] and at most morton_bits");
+        if (p->hlbvh_sah_bits % 3 != 0)
+            return hp_fail(HP_ERR_UNSUPPORTED, "hlbvh_sah_bits must be a multiple of 3 (6, 9, 12 or 15)");
     } else if (p->method != HP_METHOD_LBVH) {
         return hp_fail(HP_ERR_ARG, "unknown build method");
     }
@@ -262,6 +269,7 @@ void hp_build_params_default(hp_build_params* p) {
     p->max_leaf_size = 8;
     p->adaptive_leaf = 1;
     p->layout = HP_LAYOUT_BIN;
+    p->hlbvh_sah_bits = 15;
 }
 
 hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh* out,

@@ -358,6 +358,7 @@ hp_status hp_env_build_params(const hp_env* env, hp_build_params* p) {
     else if (!std::strcmp(method, "ploc")) { p->method = HP_METHOD_PLOC; bits_key = "Bvh.plocMortonCodeBits"; }
     else if (!std::strcmp(method, "atr")) { p->method = HP_METHOD_ATR; bits_key = "Bvh.atrMortonCodeBits"; }
     else if (!std::strcmp(method, "tr")) { p->method = HP_METHOD_TR; bits_key = "Bvh.trMortonCodeBits"; }
+    else if (!std::strcmp(method, "hlbvh")) { p->method = HP_METHOD_HLBVH; bits_key = "Bvh.hlbvhMortonCodeBits"; }
     else return hp_fail(HP_ERR_UNSUPPORTED, std::string("Bvh.method ") + method + " is not supported");
     if (hp_env_get_int(env, "Bvh.maxLeafSize", &iv) == HP_OK) {
         if (iv > 0 && iv <= 1024) p->max_leaf_size = iv;
@@ -369,6 +370,12 @@ hp_status hp_env_build_params(const hp_env* env, hp_build_params* p) {
     if (hp_env_get_int(env, bits_key, &iv) == HP_OK) {
         if (iv < 6 || iv > 60) warn("Morton code bits must be in range [6,60].");
         else p->morton_bits = iv;
+    }
+    // HLBVHBuilder::setMortonCodeSAHBits (rt/bvh/HLBVHBuilder.cpp:431-435)
+    if (hp_env_get_int(env, "Bvh.hlbvhMortonCodeSAHBits", &iv) == HP_OK) {
+        if (iv < 6 || iv > 15) warn("Morton code SAH bits must be in range [6,15].");
+        else if (p->morton_bits < iv) warn("Morton code SAH bits must be less than Morton bits.");
+        else p->hlbvh_sah_bits = iv;
     }
     if (hp_env_get_int(env, "Bvh.plocMaxRadius", &iv) == HP_OK) {
         if (iv < 1) warn("Max. radius must be positive.");

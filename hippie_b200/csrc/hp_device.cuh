@@ -41,6 +41,39 @@ __device__ __forceinline__ int hp_arrive(int* counter) {
     return old;
 }
 
+// Bounded grid barrier for cooperative launches: bar[0] counts arrivals,
+// bar[1] is the generation (both zero before the launch). Every thread of every
+// CTA calls it. Returns false, with HP_DEV_SPIN_LIMIT reported, when the wait
+// gave up: after `limit` polls, or early once another CTA has reported an
+// error; the caller then leaves the kernel.
+__device__ __forceinline__ bool hp_grid_barrier(unsigned* bar, int* err, unsigned limit) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        const unsigned gen = *((volatile unsigned*)(bar + 1));
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*((volatile unsigned*)(bar + 1)) == gen) {
+                if (++spins > limit || ((spins & 255u) == 0 && *((volatile int*)err) != 0)) {
+                    hp_report(err, HP_DEV_SPIN_LIMIT, -1);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // ---- float <-> order-preserving uint (for atomicMin/atomicMax on floats) ----
 __device__ __forceinline__ uint32_t hp_f2ord(float f) {
     uint32_t u = __float_as_uint(f);

@@ -191,6 +191,15 @@ hp_status hp_atr_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, 
                        const int32_t* sorted_tri, int* parent, int* left, int* right, float4* nbmin,
                        float4* nbmax, int* counters, const float4* tbmin, const float4* tbmax, void* scratch,
                        void* wide_scratch, cudaStream_t stream);
+// HLBVH top-level rebuild of a Karras tree over its sorted keys (method
+// HP_METHOD_HLBVH): refits the LBVH boxes, finds the clusters below the top
+// hlbvh_sah_bits of the key and rebuilds the tree above them by binned SAH.
+// The tree is then refitted and collapsed by hp_atr_stage with no iterations.
+size_t hp_hlbvh_scratch_bytes(int64_t n, int sah_bits);
+hp_status hp_hlbvh_stage(hp_ctx* ctx, const hp_build_params* p, int n, const void* skeys, int key_bytes,
+                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax, int* parent, int* left,
+                         int* right, const int2* range, float4* nbmin, float4* nbmax, int* counters, void* scratch,
+                         cudaStream_t stream);
 hp_status hp_refit_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m,
                           cudaStream_t stream);
 

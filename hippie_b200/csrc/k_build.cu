@@ -395,7 +395,8 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits, ctx->tune.sort_block);
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
-    const bool atr = p->method == HP_METHOD_ATR || p->method == HP_METHOD_TR;  // treelet restructuring
+    const bool hlbvh = p->method == HP_METHOD_HLBVH;  // binned SAH above the clusters, then the ATR collapse
+    const bool atr = p->method == HP_METHOD_ATR || p->method == HP_METHOD_TR || hlbvh;  // treelet restructuring
     const int layout = hp_layout_of(p);
     const bool wide = layout != 2;
     size_t need = 0;
@@ -410,7 +411,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         need += hp_carve::pad(n * 4);                                                     // sorted references
         need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
         need += 2 * hp_carve::pad(nn * 16) + hp_carve::pad(n * 4);                        // node boxes, counters
-        need += hp_atr_scratch_bytes(n);
+        need += std::max(hp_atr_scratch_bytes(n), hlbvh ? hp_hlbvh_scratch_bytes(n, p->hlbvh_sah_bits) : 0);
     } else {
         need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
         need += 2 * hp_carve::pad(nn * 16);                   // node boxes
@@ -464,7 +465,8 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         float4* nbmin = cv.take<float4>(nn);
         float4* nbmax = cv.take<float4>(nn);
         int* counters = cv.take<int>(n);
-        void* atr_scratch = cv.take<char>(hp_atr_scratch_bytes(n));
+        void* atr_scratch =
+            cv.take<char>(std::max(hp_atr_scratch_bytes(n), hlbvh ? hp_hlbvh_scratch_bytes(n, p->hlbvh_sah_bits) : 0));
         k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
         k_tri_boxes<<<grid_red, TB, 0, s>>>(m->vertices, m->num_vertices, m->triangles, n, tbmin, tbmax,
                                             info->box_ord, err);
@@ -480,7 +482,15 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(ctx, s, "karras");
-        HP_TRY(hp_atr_stage(ctx, m, p, out, (int)n, sorted_refs, parent, left, right, nbmin, nbmax, counters,
+        hp_build_params q = *p;
+        if (hlbvh) {  // the top-level rebuild; the ATR stage with no iterations refits and collapses
+            HP_TRY(hp_hlbvh_stage(ctx, p, (int)n, skeys, (int)sizeof(K), sorted_refs, tbmin, tbmax, parent, left,
+                                  right, range, nbmin, nbmax, counters, atr_scratch, s));
+            q.method = HP_METHOD_ATR;
+            q.atr_iterations = 0;
+            q.atr_treelet = 9;
+        }
+        HP_TRY(hp_atr_stage(ctx, m, &q, out, (int)n, sorted_refs, parent, left, right, nbmin, nbmax, counters,
                             tbmin, tbmax, atr_scratch, wide_scratch, s));
         if (taps) {
             if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);

@@ -90,33 +90,7 @@ __device__ __forceinline__ int radius_at(const ploc_args& a, int it) {
 }
 
 // Bounded grid barrier (generation counter). Returns false if it gave up.
-__device__ bool grid_barrier(unsigned* bar, int* err) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        s_ok = 1;
-        unsigned gen = ld_vol_u32(bar + 1);
-        __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned spins = 0;
-            while (ld_vol_u32(bar + 1) == gen) {
-                if (++spins > SPIN || ((spins & 255u) == 0 && *((volatile int*)err) != 0)) {
-                    hp_report(err, HP_DEV_SPIN_LIMIT, -1);
-                    s_ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) { return hp_grid_barrier(bar, err, SPIN); }
 
 // Create node `node` = merge of clusters with node ids a (left) and b (right).
 __device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a, int b) {

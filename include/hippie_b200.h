@@ -57,8 +57,10 @@ typedef enum hp_method {
     HP_METHOD_LBVH = 0,       /* Bvh.method lbvh */
     HP_METHOD_PLOC = 1,       /* Bvh.method ploc */
     HP_METHOD_ATR = 2,        /* Bvh.method atr  (LBVH + agglomerative treelet restructuring) */
-    HP_METHOD_TR = 3          /* Bvh.method tr   (LBVH + treelet restructuring by dynamic programming,
+    HP_METHOD_TR = 3,         /* Bvh.method tr   (LBVH + treelet restructuring by dynamic programming,
                                  treelet 7: TRBuilder) */
+    HP_METHOD_HLBVH = 4       /* Bvh.method hlbvh (LBVH clusters below the top Morton bits, binned SAH
+                                 above them: HLBVHBuilder) */
 } hp_method;
 
 /* Node layouts: children per node (HipBVH::Layout, rt/bvh/HipBVH.h:23-27). A
@@ -86,7 +88,7 @@ typedef struct hp_mesh {
  * (environment/AppEnvironment.cpp:52-75) plus Bvh.atrTreeletSize. */
 typedef struct hp_build_params {
     int32_t method;           /* hp_method                     Bvh.method          */
-    int32_t morton_bits;      /* [6,60]                        Bvh.{lbvh,ploc,atr}MortonCodeBits */
+    int32_t morton_bits;      /* [6,60]                        Bvh.{lbvh,ploc,atr,tr,hlbvh}MortonCodeBits */
     int32_t ploc_radius;      /* [1,ploc_max_radius]           Bvh.plocRadius      */
     int32_t ploc_max_radius;  /* >= 1                          Bvh.plocMaxRadius   */
     int32_t ploc_adaptive;    /* 0/1                           Bvh.plocAdaptive    */
@@ -97,7 +99,8 @@ typedef struct hp_build_params {
     int32_t max_leaf_size;    /* (0,1024]                      Bvh.maxLeafSize     */
     int32_t adaptive_leaf;    /* 0/1                           Bvh.adaptiveLeafSize */
     int32_t layout;           /* hp_layout; 0 means Bin        Bvh.layout          */
-    int32_t reserved[4];
+    int32_t hlbvh_sah_bits;   /* 6, 9, 12 or 15, <= morton_bits Bvh.hlbvhMortonCodeSAHBits */
+    int32_t reserved[3];
 } hp_build_params;
 
 /* A built BVH. Device pointers are owned by the library; release with

@@ -37,15 +37,18 @@ _SIGS = {
     "or_pixel_table": (C.c_int32, [C.c_int32, C.c_int32, _P]),
     "or_primary_rays": (None, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P, _P]),
     "or_ray_keys": (None, [_P, C.c_int64, _P, C.c_int32, _P]),
+    "or_build_hlbvh": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, _P,
+                                   _P, _P, _P, _P, _P, _P]),
     "or_tr": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
     "or_build_tr": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, _P, _P,
                                 _P, _P, _P, _P, _P]),
     "or_collapse_wide": (C.c_int64, [C.c_int, _P, _P, _P, _P, _P, C.c_int, C.c_float, C.c_float, C.c_int, _P, _P,
                                       _P]),
     "or_binary_tree": (None, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                              C.c_float, C.c_float, _P, _P, _P, _P, _P, _P, _P, _P]),
+                              C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P, _P, _P, _P]),
     "or_build_wide": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
-                                  C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P, _P]),
+                                  C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P,
+                                  _P]),
     "or_trace": (None, [_P, _P, _P, C.c_int64, _P, C.c_int64, _P, _P, C.c_int]),
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
@@ -191,6 +194,25 @@ def build_tr(verts, tris, bits=60, iterations=2, ct=3.0, ci=2.0, adaptive=1, max
     return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
 
 
+def build_hlbvh(verts, tris, bits=60, sah_bits=15, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+    """HLBVH (HLBVHBuilder::build): LBVH clusters below the top sah_bits Morton bits, a
+    binned-SAH top tree above them, then the depth-first collapse."""
+    n = tris.shape[0]
+    cap = max(2 * n - 1, 3)
+    nodes = np.zeros((cap, 16), np.int32)
+    woop = np.zeros((max(n, 1), 12), np.float32)
+    tri = np.zeros(max(n, 1), np.int32)
+    counts = np.zeros(2, np.int32)
+    box = np.zeros(6, np.float32)
+    sc = np.zeros(3, np.float32)
+    s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
+    cnt = load().or_build_hlbvh(_p(verts), _p(tris), n, bits, sah_bits, ct, ci, adaptive, max_leaf, _p(s_in),
+                                _p(nodes), _p(woop), _p(tri), _p(counts), _p(box), _p(sc))
+    if cnt < 0:
+        raise ValueError("sah_bits must be a multiple of 3 in [6, 15] and at most bits")
+    return dict(nodes=nodes[:cnt], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
+
+
 def tr(n, parent, left, right, bmin4, bmax4, iterations=2, ct=3.0, ci=2.0):
     """TRBVH iterations in place on a refitted binary tree (arrays over 2n-1 nodes)."""
     return load().or_tr(n, iterations, ct, ci, _p(parent), _p(left), _p(right), _p(bmin4), _p(bmax4))
@@ -235,11 +257,11 @@ def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1)):
     return keys
 
 
-METHODS = {"lbvh": 0, "ploc": 1, "atr": 2, "tr": 3}
+METHODS = {"lbvh": 0, "ploc": 1, "atr": 2, "tr": 3, "hlbvh": 4}
 
 
 def binary_tree(verts, tris, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, treelet=9,
-                iterations=2, ct=3.0, ci=2.0, scale=None):
+                iterations=2, ct=3.0, ci=2.0, scale=None, sah_bits=15):
     """The binary tree a build collapses: dict of left, right, bmin4, bmax4 (2n-1 nodes),
     sorted_tri, scene_box, scale."""
     n = tris.shape[0]
@@ -249,7 +271,7 @@ def binary_tree(verts, tris, method="lbvh", bits=60, radius=16, max_radius=256, 
              scale=np.zeros(3, np.float32))
     s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
     load().or_binary_tree(_p(verts), _p(tris), n, METHODS[method], bits, radius, max_radius, adaptive_r, treelet,
-                          iterations, ct, ci, _p(s_in), _p(d["left"]), _p(d["right"]), _p(d["bmin4"]),
+                          iterations, sah_bits, ct, ci, _p(s_in), _p(d["left"]), _p(d["right"]), _p(d["bmin4"]),
                           _p(d["bmax4"]), _p(d["sorted_tri"]), _p(d["scene_box"]), _p(d["scale"]))
     return d
 
@@ -269,7 +291,7 @@ def collapse_wide(n, left, right, bmin4, bmax4, sorted_tri, width, ct=3.0, ci=2.
 
 
 def build_wide(verts, tris, width, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, treelet=9,
-               iterations=2, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None):
+               iterations=2, ct=3.0, ci=2.0, adaptive=1, max_leaf=8, scale=None, sah_bits=15):
     """Whole build into the Quad (4) or Oct (8) layout: dict of nodes, woop, tri_idx, counts, box, scale."""
     n = tris.shape[0]
     nodes = np.zeros((max(2 * n - 1, 2), 8 * width), np.int32)
@@ -280,7 +302,7 @@ def build_wide(verts, tris, width, method="lbvh", bits=60, radius=16, max_radius
     sc = np.zeros(3, np.float32)
     s_in = None if scale is None else np.ascontiguousarray(scale, np.float32)
     c = load().or_build_wide(_p(verts), _p(tris), n, METHODS[method], bits, radius, max_radius, adaptive_r, treelet,
-                             iterations, ct, ci, adaptive, max_leaf, width, _p(s_in), _p(nodes), _p(woop), _p(tri),
+                             iterations, sah_bits, ct, ci, adaptive, max_leaf, width, _p(s_in), _p(nodes), _p(woop), _p(tri),
                              _p(counts), _p(box), _p(sc))
     return dict(nodes=nodes[:c], woop=woop[:n], tri_idx=tri[:n], counts=counts, box=box, scale=sc)
 

@@ -19,6 +19,7 @@
 // pinned by known-answer vectors derived by hand from the reference formulas
 // (tests/golden/) and by structural invariants; see the tests.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -1186,6 +1187,252 @@ int64_t or_build_atr(const float* verts, const int32_t* tris, int64_t n64, int b
                            size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
 }
 
+// ---- HLBVH: LBVH clusters below the top Morton bits, binned SAH above them
+// (HLBVHBuilder::build, rt/bvh/HLBVHBuilder.cpp:330-395; kernels
+// computeNodeStates, computeLeafClusterIndices, computeClusters, binClusters,
+// split, distributeClusters, rt/bvh/HLBVHBuilderKernels.cu:35-704).
+//
+// An interior LBVH node whose split prefix delta(g, g+1) is at least
+// 64 - bits + sahBits lies inside a cluster (state 0; leaves too); the clusters
+// are the highest state-0 nodes below the root. Each cluster is binned by the
+// (x, y, z) coordinates of its top sahBits Morton bits (2^(sahBits/3) bins
+// per axis). The top tree is built top-down over the clusters: per task and
+// axis the bins are swept from the left against suffix unions from the
+// right; a split needs clusters on both sides and costs
+// count_l * A_l + count_r * A_r (the kernel's fused form
+// fma(count_l, A_l, count_r * A_r), A = 2 * fma(y, z, fma(x, y, x * z))), the
+// first strictly lowest cost over (axis, bin) wins, clusters at or below the
+// split bin go left; a side with one cluster takes the cluster's subtree. With
+// sahBits a multiple of 3 every cluster has its own cell except a leaf
+// cluster at the last sorted position, which the kernel bins with key 0's
+// cell (below); that leaf and the cluster holding position 0 are never
+// separated by a bin split and end as the two clusters of the kernel's
+// object-median fallback. The new top nodes reuse the indices of the LBVH's
+// state-1 nodes in increasing order (the root stays 0). When the root itself
+// lies inside a cluster (every key shares the top sahBits) the LBVH is kept.
+// Bin boxes are float min / max; the kernel's integer atomics on float bits
+// agree with them for non-negative coordinates (the reference's scene loader
+// scales scenes into [0, 1]^3, rt/scene/SceneLoader.cpp:136-140), not for
+// negative ones.
+namespace {
+
+inline void morton_coords(uint32_t code, int* c) {
+    c[0] = c[1] = c[2] = 0;
+    for (int i = 0; i < 10; ++i) {
+        c[0] += ((code >> (3 * i + 0)) & 1) << i;
+        c[1] += ((code >> (3 * i + 1)) & 1) << i;
+        c[2] += ((code >> (3 * i + 2)) & 1) << i;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// HLBVH top-level rebuild in place on a Karras LBVH (parent / left / right /
+// refitted boxes over 2n-1 nodes) with its sorted keys. Returns the number of
+// clusters, or -1 for an unsupported sahBits.
+int or_hlbvh(int n, const uint64_t* skeys, int bits, int sah_bits, int32_t* parent, int32_t* left, int32_t* right,
+             float* bmin4, float* bmax4) {
+    if (sah_bits % 3 != 0 || sah_bits < 6 || sah_bits > 15 || sah_bits > bits) return -1;
+    if (n < 2) return 0;
+    const int nn = 2 * n - 1, off = 64 - bits + sah_bits, NB = 1 << (sah_bits / 3);
+    std::vector<int> state(nn, 0), gamma(n - 1, 0), last(nn, 0);
+    // split position of each interior node: the last sorted position of its left child
+    for (int p = 0; p < n; ++p) last[n - 1 + p] = p;
+    {
+        std::vector<int> st{0};
+        std::vector<char> ex(nn, 0);
+        while (!st.empty()) {
+            const int v = st.back();
+            if (v >= n - 1) { st.pop_back(); continue; }
+            if (!ex[v]) { ex[v] = 1; st.push_back(right[v]); st.push_back(left[v]); continue; }
+            st.pop_back();
+            last[v] = last[right[v]];
+            gamma[v] = last[left[v]];
+        }
+    }
+    for (int v = 0; v < n - 1; ++v) state[v] = delta(skeys, n, gamma[v], gamma[v] + 1) >= off ? 0 : 1;
+    // clusters, in order of their first sorted position
+    std::vector<int> clusters;
+    {
+        std::vector<int> st{0};
+        while (!st.empty()) {
+            const int v = st.back();
+            st.pop_back();
+            if (v != 0 && state[v] == 0) { clusters.push_back(v); continue; }
+            st.push_back(right[v]);
+            st.push_back(left[v]);
+        }
+    }
+    const int C = (int)clusters.size();
+    std::vector<int> free_idx;  // state-1 interior nodes, root first
+    for (int v = 0; v < n - 1; ++v)
+        if (state[v] == 1) free_idx.push_back(v);
+    if (C < 2 || free_idx.empty() || free_idx[0] != 0) return C;
+    // computeClusters reads the key at the node's left index with leaf indices
+    // mapped by subtracting n-1; a leaf's left index is its sorted position, so
+    // the leaf at the last position n-1 reads key 0 (rt/bvh/HLBVHBuilderKernels.cu:
+    // 325-327 with setupLeaves, rt/bvh/LBVHBuilderKernels.cu:186).
+    std::vector<std::array<int, 3>> coord(C);
+    for (int c = 0; c < C; ++c) {
+        const int v = clusters[c];
+        int pos = v >= n - 1 ? v - (n - 1) : gamma[v];
+        if (v == 2 * n - 2) pos = 0;
+        morton_coords((uint32_t)((skeys[pos] >> (bits - sah_bits)) & ((1u << sah_bits) - 1)), coord[c].data());
+    }
+    struct bin {
+        float mn[3], mx[3];
+        int cnt;
+        void reset() { for (int a = 0; a < 3; ++a) { mn[a] = MAXF; mx[a] = -MAXF; } cnt = 0; }
+        void add(const float* bmn, const float* bmx, int k) {
+            for (int a = 0; a < 3; ++a) { mn[a] = std::min(mn[a], bmn[a]); mx[a] = std::max(mx[a], bmx[a]); }
+            cnt += k;
+        }
+        float cost() const {
+            return (float)cnt * atr_area(mn, mx);  // only the product; the sum below is fused
+        }
+    };
+    auto area = [](const bin& b) { return atr_area(b.mn, b.mx); };
+    // tasks: (node to write, parent), each with its clusters (in cluster order)
+    std::vector<int> task_node{0}, task_parent{-1};
+    std::vector<int> task_of(C, 0);
+    size_t next_free = 1;
+    std::vector<int> node_of_task(1, 0);
+    while (!task_node.empty()) {
+        const int T = (int)task_node.size();
+        std::vector<bin> bins((size_t)T * 3 * NB);
+        for (auto& b : bins) b.reset();
+        for (int c = 0; c < C; ++c) {
+            const int t = task_of[c];
+            if (t < 0) continue;
+            const int v = clusters[c];
+            for (int a = 0; a < 3; ++a) bins[((size_t)t * 3 + a) * NB + coord[c][a]].add(&bmin4[4 * v], &bmax4[4 * v], 1);
+        }
+        std::vector<int> new_node, new_parent;
+        std::vector<int> best_axis(T, -1), best_bin(T, -1), left_task(T, -1), right_task(T, -1);
+        std::vector<int> left_cnt(T, 0), right_cnt(T, 0), total(T, 0), rank(T, 0);
+        for (int c = 0; c < C; ++c)
+            if (task_of[c] >= 0) ++total[task_of[c]];
+        for (int t = 0; t < T; ++t) {
+            float best = MAXF;
+            bin bl{}, br{};
+            for (int a = 0; a < 3; ++a) {
+                const bin* B = &bins[((size_t)t * 3 + a) * NB];
+                std::vector<bin> suffix(NB);
+                suffix[NB - 1] = B[NB - 1];
+                for (int b = NB - 2; b >= 0; --b) {
+                    suffix[b] = suffix[b + 1];
+                    suffix[b].add(B[b].mn, B[b].mx, B[b].cnt);
+                }
+                bin lft = B[0];
+                for (int b = 0; b < NB - 1; ++b) {
+                    if (lft.cnt > 0 && suffix[b + 1].cnt > 0) {
+                        const float cost = std::fmaf((float)lft.cnt, area(lft), (float)suffix[b + 1].cnt * area(suffix[b + 1]));
+                        if (cost < best) {
+                            best = cost;
+                            best_axis[t] = a;
+                            best_bin[t] = b;
+                            bl = lft;
+                            br = suffix[b + 1];
+                        }
+                    }
+                    lft.add(B[b + 1].mn, B[b + 1].mx, B[b + 1].cnt);
+                }
+            }
+            if (best_axis[t] < 0) {
+                // Every cluster in one bin (only the leaf above and the cluster of
+                // key 0 share a cell): an object median, the first half of the
+                // clusters left. The kernel orders them by atomic arrival; here
+                // they go in sorted order.
+                best_axis[t] = 3;
+                best_bin[t] = total[t] / 2;
+                bl.reset();
+                br.reset();
+                int k = 0;
+                for (int c = 0; c < C; ++c) {
+                    if (task_of[c] != t) continue;
+                    const int v = clusters[c];
+                    (k++ < best_bin[t] ? bl : br).add(&bmin4[4 * v], &bmax4[4 * v], 1);
+                }
+            }
+            const int node = task_node[t];
+            for (int a = 0; a < 3; ++a) {
+                bmin4[4 * node + a] = std::min(bl.mn[a], br.mn[a]);
+                bmax4[4 * node + a] = std::max(bl.mx[a], br.mx[a]);
+            }
+            parent[node] = task_parent[t];
+            left_cnt[t] = bl.cnt;
+            right_cnt[t] = br.cnt;
+            // interior children take the next free indices, left then right
+            if (bl.cnt > 1) {
+                left_task[t] = (int)new_node.size();
+                new_node.push_back(free_idx[next_free++]);
+                new_parent.push_back(node);
+                left[node] = new_node.back();
+            }
+            if (br.cnt > 1) {
+                right_task[t] = (int)new_node.size();
+                new_node.push_back(free_idx[next_free++]);
+                new_parent.push_back(node);
+                right[node] = new_node.back();
+            }
+        }
+        // distribute the clusters; a single cluster becomes its side's child
+        for (int c = 0; c < C; ++c) {
+            const int t = task_of[c];
+            if (t < 0) continue;
+            const bool go_left =
+                best_axis[t] == 3 ? rank[t]++ < best_bin[t] : coord[c][best_axis[t]] <= best_bin[t];
+            const int nt = go_left ? left_task[t] : right_task[t];
+            if (nt >= 0) {
+                task_of[c] = nt;
+            } else {
+                const int node = task_node[t], v = clusters[c];
+                (go_left ? left : right)[node] = v;
+                parent[v] = node;
+                task_of[c] = -1;
+            }
+        }
+        task_node.swap(new_node);
+        task_parent.swap(new_parent);
+    }
+    return C;
+}
+
+// Whole HLBVH build: the LBVH stages, the top-level rebuild, then the collapse.
+int64_t or_build_hlbvh(const float* verts, const int32_t* tris, int64_t n64, int bits, int sah_bits, float ct, float ci,
+                       int adaptive, int max_leaf, const float* scale_in, void* nodes_out, float* woop4,
+                       int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
+    const int n = (int)n64;
+    if (n < 2)
+        return or_build_lbvh(verts, tris, n64, bits, ct, ci, adaptive, max_leaf, scale_in, nodes_out, woop4,
+                             tri_idx, counts, scene_box, scale_out);
+    std::vector<float> bmin(4 * (size_t)n), bmax(4 * (size_t)n);
+    or_tri_boxes(verts, tris, n, bmin.data(), bmax.data(), scene_box);
+    std::vector<uint64_t> keys(n), skeys(n);
+    or_morton(n, bmin.data(), bmax.data(), scene_box, scale_in, bits, keys.data(), scale_out);
+    std::vector<int32_t> sorted(n);
+    or_sort(n, keys.data(), bits, skeys.data(), sorted.data());
+    const int nn = 2 * n - 1;
+    std::vector<int32_t> parent(nn), left(nn), right(nn), size(nn), state(nn);
+    or_karras(n, skeys.data(), parent.data(), left.data(), right.data());
+    std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn), cost(nn);
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    if (or_hlbvh(n, skeys.data(), bits, sah_bits, parent.data(), left.data(), right.data(), nbmin.data(),
+                 nbmax.data()) < 0) {
+        counts[0] = counts[1] = 0;
+        return -1;
+    }
+    or_refit(n, verts, tris, sorted.data(), parent.data(), left.data(), right.data(), ct, ci, adaptive, max_leaf,
+             nbmin.data(), nbmax.data(), size.data(), cost.data(), state.data());
+    return or_collapse_dfs(n, verts, tris, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
+                           size.data(), state.data(), nodes_out, tri_idx, woop4, counts);
+}
+
+}  // extern "C"
+
 // Whole TRBVH build (TRBuilder::build, rt/bvh/TRBuilder.cpp:207-260): the LBVH
 // stages, the TR iterations, then the collapse of the restructured tree.
 int64_t or_build_tr(const float* verts, const int32_t* tris, int64_t n64, int bits, int iterations, float ct,
@@ -1442,10 +1689,10 @@ int64_t or_collapse_wide(int n, const int32_t* sorted_tri, const int32_t* left, 
 
 }  // extern "C"
 
-// The final binary tree of a build (method 0 LBVH, 1 PLOC, 2 ATR, 3 TRBVH) before its
+// The final binary tree of a build (method 0 LBVH, 1 PLOC, 2 ATR, 3 TRBVH, 4 HLBVH) before its
 // collapse: children, refitted boxes and the sorted reference order.
 void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int method, int bits, int radius,
-                    int max_radius, int adaptive_r, int treelet, int iterations, float ct, float ci,
+                    int max_radius, int adaptive_r, int treelet, int iterations, int sah_bits, float ct, float ci,
                     const float* scale_in, int32_t* left, int32_t* right, float* nbmin4, float* nbmax4,
                     int32_t* sorted_tri, float* scene_box, float* scale_out) {
     const int n = (int)n64;
@@ -1472,9 +1719,10 @@ void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int me
     or_karras(n, skeys.data(), parent.data(), left, right);
     or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
              cost.data(), state.data());
-    if (method == 2 || method == 3) {
+    if (method == 2 || method == 3 || method == 4) {
         if (method == 2) or_atr(n, treelet, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
-        else or_tr(n, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
+        else if (method == 3) or_tr(n, iterations, ct, ci, parent.data(), left, right, nbmin4, nbmax4);
+        else or_hlbvh(n, skeys.data(), bits, sah_bits, parent.data(), left, right, nbmin4, nbmax4);
         or_refit(n, verts, tris, sorted_tri, parent.data(), left, right, ct, ci, 1, 8, nbmin4, nbmax4, size.data(),
                  cost.data(), state.data());
     }
@@ -1483,7 +1731,8 @@ void or_binary_tree(const float* verts, const int32_t* tris, int64_t n64, int me
 // Whole build into an N-wide layout: the binary tree of the method, the wide
 // collapse, then the Woop triangles in the collapsed reference order.
 int64_t or_build_wide(const float* verts, const int32_t* tris, int64_t n64, int method, int bits, int radius,
-                      int max_radius, int adaptive_r, int treelet, int iterations, float ct, float ci, int adaptive,
+                      int max_radius, int adaptive_r, int treelet, int iterations, int sah_bits, float ct, float ci,
+                      int adaptive,
                       int max_leaf, int width, const float* scale_in, int32_t* nodes_out, float* woop4,
                       int32_t* tri_idx, int32_t* counts, float* scene_box, float* scale_out) {
     const int n = (int)n64;
@@ -1492,8 +1741,8 @@ int64_t or_build_wide(const float* verts, const int32_t* tris, int64_t n64, int 
     const int nn = 2 * n - 1;
     std::vector<int32_t> left(nn), right(nn), sorted(n);
     std::vector<float> nbmin(4 * (size_t)nn), nbmax(4 * (size_t)nn);
-    or_binary_tree(verts, tris, n64, method, bits, radius, max_radius, adaptive_r, treelet, iterations, ct, ci,
-                   scale_in, left.data(), right.data(), nbmin.data(), nbmax.data(), sorted.data(), scene_box,
+    or_binary_tree(verts, tris, n64, method, bits, radius, max_radius, adaptive_r, treelet, iterations, sah_bits, ct,
+                   ci, scale_in, left.data(), right.data(), nbmin.data(), nbmax.data(), sorted.data(), scene_box,
                    scale_out);
     const int64_t c = or_collapse_wide(n, sorted.data(), left.data(), right.data(), nbmin.data(), nbmax.data(),
                                        width, ct, ci, adaptive ? 0x7fffffff : max_leaf, nodes_out, tri_idx, counts);

@@ -98,6 +98,9 @@ void ref_collapse(timer& T, int n, int* parent, int* left, int* right, float4* n
     int* node_idx = dalloc<int>(n);
     int* ref_off = dalloc<int>(nn);
     cudaMemset(counters, 0, n * 4);
+    // computeNodeOffsets writes the offsets of children only; the compaction
+    // reads the root's, which the reference's fresh buffer holds as 0.
+    cudaMemset(node_off, 0, nn * 4);
     T.run([&] { hpref_collapse_sizes(nn, counters, parent, left, right, sizes); });
     cudaMemset(counters, 0, n * 4);
     T.run([&] { hpref_collapse_states(n, ci, ct, counters, costs, parent, left, right, sizes, states, nbmin, nbmax); });
@@ -183,6 +186,90 @@ int ref_atr(timer& T, int n, int treelet, int iterations, float ct, float ci, in
     return 0;
 }
 
+// HLBVHBuilder::build after construct (rt/bvh/HLBVHBuilder.cpp:359-391) and
+// HLBVHBuilder::split (rt/bvh/HLBVHBuilder.cpp:237-328) on a Karras tree
+// (parent / left / right, leaf boxes set) and its sorted keys. Writes the
+// HLBVH topology into hparent / hleft / hright and its boxes into nbmin /
+// nbmax. Only run where the reference's index bookkeeping holds: Morton SAH
+// bits a multiple of 3 (else its bin coordinates run past their axis) and the
+// root outside every cluster (else its compaction and its top-level node
+// counter hand out the same indices).
+int ref_hlbvh(timer& T, int n, int bits, int sah, int* parent, int* left, int* right, unsigned long long* keys,
+              float4* nbmin, float4* nbmax, int* hparent, int* hleft, int* hright) {
+    if (sah % 3 != 0 || sah < 6 || sah > 15 || sah > bits) {
+        std::snprintf(g_err, sizeof(g_err), "HLBVH: Morton SAH bits must be 6, 9, 12 or 15 and at most the bits");
+        return 10;
+    }
+    unsigned long long k0 = 0, k1 = 0;
+    if (cudaMemcpy(&k0, keys, 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&k1, keys + (n - 1), 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(10, "reading the sorted keys");
+    if (((k0 ^ k1) >> (bits - sah)) == 0) {
+        std::snprintf(g_err, sizeof(g_err), "HLBVH: every key shares the top Morton SAH bits (root in a cluster)");
+        return 11;
+    }
+    const int nn = 2 * n - 1;
+    int* counters = dalloc<int>(n);
+    int* states = dalloc<int>(nn);
+    int* offsets = dalloc<int>(n);
+    int* leaf_cluster = dalloc<int>(n);
+    int* cl_tasks = dalloc<int>(n);
+    int* cl_nodes = dalloc<int>(n);
+    int4* cl_bins = dalloc<int4>(n);
+    cudaMemset(cl_bins, 0, (size_t)n * 16);
+    cudaMemset(counters, 0, (size_t)n * 4);
+    T.run([&] { hpref_hl_node_states(n, bits, sah, counters, parent, left, right, states, keys); });
+    T.run([&] { hpref_hl_leaf_clusters(n, leaf_cluster, parent, states); });
+    cudaMemset(counters, 0, (size_t)n * 4);
+    T.run([&] { hpref_hl_invalidate(n, counters, leaf_cluster, parent, states); });
+    hpref_hl_set_counter(0);
+    T.run([&] { hpref_hl_node_offsets(n, offsets, states); });
+    T.run([&] { hpref_hl_compact(n, offsets, states, parent, left, right, hparent, hleft, hright); });
+    hpref_hl_set_counter(0);
+    T.run([&] { hpref_hl_clusters(n, bits, sah, states, offsets, left, cl_nodes, cl_bins, keys); });
+    const int C = hpref_hl_counter();
+    int rc = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = fail(9, "after the HLBVH cluster kernels");
+    else if (C < 2 || C > n) rc = fail(12, "HLBVH cluster count out of range");
+    if (!rc) {
+        cudaMemset(counters, 0, (size_t)n * 4);
+        T.run([&] { hpref_refit(nn, counters, hparent, hleft, hright, nbmin, nbmax); });
+        cudaMemset(cl_tasks, 0, (size_t)n * 4);
+        hpref_hl_set_counter(1);
+        const int NB = 1 << (sah / 3);
+        float4* bmin = dalloc<float4>((size_t)3 * C * NB);
+        float4* bmax = dalloc<float4>((size_t)3 * C * NB);
+        int* new_tasks = dalloc<int>(C);
+        int* split_idx = dalloc<int>(C);
+        int2* q[2] = {dalloc<int2>(C), dalloc<int2>(C)};
+        int* out_size = dalloc<int>(1);
+        const int2 root = make_int2(0, -1);
+        cudaMemcpy(q[0], &root, sizeof(root), cudaMemcpyHostToDevice);
+        int in = 1, cur = 0, levels = 0;
+        while (in > 0) {
+            if (++levels > 2 * C + 2) { rc = fail(13, "HLBVH split did not terminate"); break; }
+            cudaMemset(out_size, 0, 4);
+            T.run([&] { hpref_hl_reset_bins(3 * in * NB, bmin, bmax); });
+            T.run([&] { hpref_hl_bin(in, NB, C, cl_tasks, cl_nodes, cl_bins, nbmin, nbmax, bmin, bmax); });
+            T.run([&] { hpref_hl_split(NB, in, out_size, new_tasks, split_idx, hparent, hleft, hright, nbmin, nbmax,
+                                       bmin, bmax, q[cur], q[cur ^ 1]); });
+            T.run([&] { hpref_hl_distribute(in, NB, C, new_tasks, split_idx, hparent, hleft, hright, cl_tasks,
+                                            cl_nodes, cl_bins, bmin, bmax, q[cur]); });
+            if (cudaMemcpy(&in, out_size, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                rc = fail(9, "after an HLBVH split level");
+                break;
+            }
+            if (in < 0 || in > C) { rc = fail(12, "HLBVH task count out of range"); break; }
+            cur ^= 1;
+        }
+        cudaFree(bmin); cudaFree(bmax); cudaFree(new_tasks); cudaFree(split_idx); cudaFree(q[0]); cudaFree(q[1]);
+        cudaFree(out_size);
+    }
+    cudaFree(counters); cudaFree(states); cudaFree(offsets); cudaFree(leaf_cluster); cudaFree(cl_tasks);
+    cudaFree(cl_nodes); cudaFree(cl_bins);
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -191,7 +278,7 @@ const char* hpref_last_error(void) { return g_err; }
 
 // Build a BVH with the reference's kernels. method 0 = LBVH, 1 = PLOC, 2 = ATR
 // (LBVH + treelet restructuring; radius carries the treelet size, max_radius
-// the iteration count).
+// the iteration count), 3 = HLBVH (radius carries the Morton SAH bits).
 // Device inputs: verts, tris. Device outputs: nodes (64 B x (2n-1)), woop
 // (48 B x n), tri_idx (n). Optional device taps (null to skip): morton keys
 // (u64 n) before sorting, sorted keys, sorted reference indices, and the
@@ -271,7 +358,28 @@ int hpref_build(int method, const float* verts, const int* tris, int n, const fl
     if (tap_refs) cudaMemcpy(tap_refs, refs0, n * 4, cudaMemcpyDeviceToDevice);
     T.run([&] { hpref_setup_leaves(n, refs0, refs1, tri0, tri1, left, right, nbmin, nbmax, rbmin, rbmax); });
     int iters = 0;
-    if (method == 0 || method == 2) {
+    if (method == 3) {  // HLBVH: radius carries the Morton SAH bits
+        T.run([&] { hpref_construct60(n, parent, left, right, keys0); });
+        if (!valid_tree(n, parent, left, right)) {
+            std::fprintf(stderr, "reference construct60 produced an invalid tree\n");
+            return 4;
+        }
+        int* hparent = dalloc<int>(nn);
+        int* hleft = dalloc<int>(nn);
+        int* hright = dalloc<int>(nn);
+        const int rc = ref_hlbvh(T, n, bits, radius, parent, left, right, keys0, nbmin, nbmax, hparent, hleft, hright);
+        if (!rc) {
+            cudaMemcpy(parent, hparent, nn * 4, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(left, hleft, nn * 4, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(right, hright, nn * 4, cudaMemcpyDeviceToDevice);
+        }
+        cudaFree(hparent); cudaFree(hleft); cudaFree(hright);
+        if (rc) return rc;
+        if (!valid_tree(n, parent, left, right)) {
+            std::fprintf(stderr, "reference HLBVH produced an invalid tree\n");
+            return 4;
+        }
+    } else if (method == 0 || method == 2) {
         T.run([&] { hpref_construct60(n, parent, left, right, keys0); });
         if (!valid_tree(n, parent, left, right)) {
             std::fprintf(stderr, "reference construct60 produced an invalid tree\n");

@@ -46,6 +46,27 @@ void hpref_atr_optimize(int n, int treelet, int schedule_size, int dist_size, in
                         float* costs, float* areas, float* dist_mats, int* left, int* right, float4* nbmin,
                         float4* nbmax, int* counters, int* parent, int* subtree_refs, int* schedule, int smem);
 
+// w_hlbvh.cu
+void hpref_hl_node_states(int n, int bits, int sah, int* counters, int* parent, int* left, int* right, int* states,
+                          unsigned long long* keys);
+void hpref_hl_leaf_clusters(int n, int* leaf_cluster, int* parent, int* states);
+void hpref_hl_invalidate(int n, int* counters, int* leaf_cluster, int* parent, int* states);
+void hpref_hl_set_counter(int v);
+int hpref_hl_counter(void);
+void hpref_hl_node_offsets(int n, int* offsets, int* states);
+void hpref_hl_compact(int n, int* offsets, int* states, int* in_parent, int* in_left, int* in_right, int* out_parent,
+                      int* out_left, int* out_right);
+void hpref_hl_clusters(int n, int bits, int sah, int* states, int* offsets, int* lbvh_left, int* cluster_nodes,
+                       int4* cluster_bins, unsigned long long* keys);
+void hpref_hl_reset_bins(int all_bins, float4* bmin, float4* bmax);
+void hpref_hl_bin(int tasks, int bins, int clusters, int* cluster_tasks, int* cluster_nodes, int4* cluster_bins,
+                  float4* nbmin, float4* nbmax, float4* bmin, float4* bmax);
+void hpref_hl_split(int bins, int tasks, int* out_size, int* new_tasks, int* split_idx, int* parent, int* left,
+                    int* right, float4* nbmin, float4* nbmax, float4* bmin, float4* bmax, int2* in_q, int2* out_q);
+void hpref_hl_distribute(int tasks, int bins, int clusters, int* new_tasks, int* split_idx, int* parent, int* left,
+                         int* right, int* cluster_tasks, int* cluster_nodes, int4* cluster_bins, float4* bmin,
+                         float4* bmax, int2* in_q);
+
 // w_bvh.cu
 void hpref_woopify(int n, int* tri_idx, const int* tris, const float* verts, float4* woop);
 float hpref_cost(int nodes, float scene_area, float ct, float ci, void* bin_nodes);

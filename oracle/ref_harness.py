@@ -47,11 +47,11 @@ def _p(t):
 
 
 def build(V, T, scene_box, method="lbvh", bits=60, radius=16, max_radius=256, adaptive_r=0, ct=3.0, ci=2.0,
-          taps=False, treelet=20, iterations=2):
+          taps=False, treelet=20, iterations=2, sah_bits=15):
     """Run the reference's build on device tensors V (float32 [v,3]) and T (int32 [n,3]).
 
-    method: "lbvh", "ploc" (radius / max_radius / adaptive_r) or "atr" (treelet /
-    iterations)."""
+    method: "lbvh", "ploc" (radius / max_radius / adaptive_r), "atr" (treelet /
+    iterations) or "hlbvh" (sah_bits)."""
     import torch
     n = T.shape[0]
     nn = 2 * n - 1
@@ -70,9 +70,11 @@ def build(V, T, scene_box, method="lbvh", bits=60, radius=16, max_radius=256, ad
     secs = C.c_double()
     iters = np.zeros(1, np.int32)
     box = np.ascontiguousarray(scene_box, np.float32)
-    code = {"lbvh": 0, "ploc": 1, "atr": 2}[method]
+    code = {"lbvh": 0, "ploc": 1, "atr": 2, "hlbvh": 3}[method]
     if method == "atr":
         radius, max_radius = treelet, iterations
+    elif method == "hlbvh":
+        radius = sah_bits
     rc = load().hpref_build(code, _p(V), _p(T), n, box.ctypes.data, bits, radius, max_radius,
                             adaptive_r, ct, ci, _p(nodes), _p(woop), _p(tri), _p(tp.get("keys")), _p(tp.get("sorted")),
                             _p(tp.get("refs")), _p(tp.get("parent")), _p(tp.get("left")), _p(tp.get("right")),

@@ -96,8 +96,15 @@ def test_out_of_range_keeps_default():
 
 def test_method_and_layout_support():
     with pytest.raises(HPError) as ei:
-        hp.Env().read_string("Bvh { method hlbvh }").build_params()
+        hp.Env().read_string("Bvh { method sbvh }").build_params()
     assert ei.value.status == 6
+    # HLBVHBuilder: its own Morton bits and the SAH bits in [6,15], at most the Morton bits
+    p = hp.Env().read_string("Bvh { method hlbvh\n hlbvhMortonCodeBits 30\n hlbvhMortonCodeSAHBits 9 }").build_params()
+    assert (p.method, p.morton_bits, p.hlbvh_sah_bits) == (4, 30, 9)
+    assert hp.Env().read_string("Bvh { method hlbvh }").build_params().hlbvh_sah_bits == 15
+    for bad in ("hlbvhMortonCodeSAHBits 16", "hlbvhMortonCodeSAHBits 5",
+                "hlbvhMortonCodeBits 12\n hlbvhMortonCodeSAHBits 15"):
+        assert hp.Env().read_string("Bvh { method hlbvh\n %s }" % bad).build_params().hlbvh_sah_bits == 15
     # HipBVH: "bin", "quad", anything else Oct
     for text, want in (("bin", 2), ("quad", 4), ("oct", 8), ("octree", 8)):
         assert hp.Env().read_string("Bvh { layout %s }" % text).build_params().layout == want
