@@ -9,7 +9,8 @@
 // the clusters are compacted in order. The reference runs ~5 kernels and a
 // host read-back per iteration; here
 //   * one persistent cooperative kernel runs every iteration while more than
-//     TAIL clusters remain: a neighbour phase over shared-memory windows, a
+//     TAIL clusters remain: a neighbour phase over shared-memory windows
+//     (four clusters per thread on long lists), a
 //     grid barrier, a merge/compaction phase whose two prefix sums (merges,
 //     survivors) come from a decoupled look-back over tiles taken in ticket
 //     order, and another barrier. Every wait is bounded; a wait that gives up
@@ -35,7 +36,9 @@ namespace {
 
 constexpr int PB = 1024;            // threads per CTA
 constexpr int MAXR = 512;           // largest radius kept in a shared-memory window
-constexpr int WIN = PB + 2 * MAXR;  // neighbour window
+constexpr int NB4 = 4;              // clusters per thread of the neighbour search on large lists
+constexpr int WIN = NB4 * PB + 2 * MAXR;  // neighbour window
+constexpr int NB4_MIN_N = 2 * 148 * NB4 * PB;  // lists at least this long use 4 clusters per thread
 constexpr int MT_ITEMS = 4;         // clusters per thread in the merge phase
 constexpr int MT = PB * MT_ITEMS;
 constexpr int TAIL = 2048;          // clusters finished by a single CTA
@@ -144,18 +147,25 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
     }
 }
 
-// Nearest neighbour of every cluster of one tile of PB clusters.
-__device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int tile,
-                        float* s) {
+// Nearest neighbour of every cluster of one tile of B*PB clusters: the tile's
+// boxes and r on each side in shared memory (a huge box, never the nearest,
+// outside the cluster list); candidates c-r .. c+r in increasing order, the
+// first strict minimum. With B = 4 a thread searches for 4 consecutive
+// clusters at once and reads each candidate box once for all of them; the
+// candidates are walked in five runs whose valid clusters are known without a
+// test per pair (runs valid for r >= 4).
+template <int B>
+__device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int tile, float* s) {
     float* smnx = s;
     float* smny = s + WIN;
     float* smnz = s + 2 * WIN;
     float* smxx = s + 3 * WIN;
     float* smxy = s + 4 * WIN;
     float* smxz = s + 5 * WIN;
-    const int base = tile * PB;
+    constexpr int TS = B * PB;
+    const int base = tile * TS;
     __syncthreads();
-    for (int k = threadIdx.x; k < PB + 2 * r; k += PB) {
+    for (int k = threadIdx.x; k < TS + 2 * r; k += PB) {
         const int c = base - r + k;
         if (c >= 0 && c < N) {
             const int node = cl[c];
@@ -168,22 +178,69 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
         }
     }
     __syncthreads();
-    const int i = base + threadIdx.x;
-    if (i >= N) return;
-    const int me = r + threadIdx.x;
-    const float ax = smnx[me], ay = smny[me], az = smnz[me], bx = smxx[me], by = smxy[me], bz = smxz[me];
-    float best = HP_MAX_FLOAT;
-    int bi = -1;
-    for (int k = me - r; k < me + r + 1; ++k) {
-        if (k == me) continue;
-        const float d = half_area(fminf(ax, smnx[k]), fminf(ay, smny[k]), fminf(az, smnz[k]),
-                                  fmaxf(bx, smxx[k]), fmaxf(by, smxy[k]), fmaxf(bz, smxz[k]));
-        if (best > d) {
-            best = d;
-            bi = base - r + k;
+    const int l0 = threadIdx.x * B;  // cluster base + l sits at window position l + r
+    if (base + l0 >= N) return;
+    float ax[B], ay[B], az[B], bx[B], by[B], bz[B], best[B];
+    int bi[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+        const int me = l0 + q + r;
+        ax[q] = smnx[me]; ay[q] = smny[me]; az[q] = smnz[me];
+        bx[q] = smxx[me]; by[q] = smxy[me]; bz[q] = smxz[me];
+        best[q] = HP_MAX_FLOAT;
+        bi[q] = -1;
+    }
+    auto upd = [&](int q, int k, float cx, float cy, float cz, float dx, float dy, float dz) {
+        const float d = half_area(fminf(ax[q], cx), fminf(ay[q], cy), fminf(az[q], cz), fmaxf(bx[q], dx),
+                                  fmaxf(by[q], dy), fmaxf(bz[q], dz));
+        if (best[q] > d) {
+            best[q] = d;
+            bi[q] = base - r + k;
+        }
+    };
+#define HP_PLOC_CAND(k) const float cx = smnx[k], cy = smny[k], cz = smnz[k], dx = smxx[k], dy = smxy[k], dz = smxz[k]
+    if (B == 1 || r < 4) {
+        for (int k = l0; k <= l0 + (B - 1) + 2 * r; ++k) {
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+                if (k >= l0 + q && k <= l0 + q + 2 * r && k != l0 + q + r) upd(q, k, cx, cy, cz, dx, dy, dz);
+        }
+    } else {
+        // cluster q: candidates l0+q .. l0+q+2r, itself at l0+q+r
+        for (int k = l0; k < l0 + 3; ++k) {  // q <= k - l0
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+                if (q <= k - l0) upd(q, k, cx, cy, cz, dx, dy, dz);
+        }
+        for (int k = l0 + 3; k < l0 + r; ++k) {  // every cluster, none itself
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q) upd(q, k, cx, cy, cz, dx, dy, dz);
+        }
+        for (int k = l0 + r; k < l0 + r + 4; ++k) {  // every cluster but the one at k
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+                if (q != k - l0 - r) upd(q, k, cx, cy, cz, dx, dy, dz);
+        }
+        for (int k = l0 + r + 4; k <= l0 + 2 * r; ++k) {  // every cluster, none itself
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q) upd(q, k, cx, cy, cz, dx, dy, dz);
+        }
+        for (int k = l0 + 2 * r + 1; k <= l0 + 2 * r + 3; ++k) {  // q >= k - l0 - 2r
+            HP_PLOC_CAND(k);
+#pragma unroll
+            for (int q = 0; q < B; ++q)
+                if (q >= k - l0 - 2 * r) upd(q, k, cx, cy, cz, dx, dy, dz);
         }
     }
-    A.nn[i] = bi;
+#undef HP_PLOC_CAND
+#pragma unroll
+    for (int q = 0; q < B; ++q)
+        if (base + l0 + q < N) A.nn[base + l0 + q] = bi[q];
 }
 
 // Status word of a merge tile: [63:60] iteration tag, [59:58] flag, [57:29] merges, [28:0] survivors.
@@ -238,31 +295,49 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
     }
     int em = m, ek = k;
     const int2 tot = block_scan2(em, ek, s_wa, s_wb);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // Decoupled look-back by one warp over windows of 32 earlier tiles: lane i
+        // reads tile t-i; the window is summed up to the nearest tile whose
+        // inclusive prefix is published, once every tile up to it has published.
+        const int lane = threadIdx.x;
         unsigned long long* st = A.status + tile;
-        st_vol_u64(st, mk_status(tag, tile == 0 ? F_INC : F_AGG, tot.x, tot.y));
+        if (lane == 0) st_vol_u64(st, mk_status(tag, tile == 0 ? F_INC : F_AGG, tot.x, tot.y));
         unsigned pm = 0, pk = 0;
         if (tile > 0) {
             long t = (long)tile - 1;
             unsigned spins = 0;
             while (true) {
-                const unsigned long long s = ld_vol_u64(A.status + t);
-                if ((unsigned)(s >> 60) != tag || (s & F_MASK) == 0) {
-                    if (++spins > SPIN) { hp_report(A.err, HP_DEV_SPIN_LIMIT, (int)tile); break; }
-                    if ((spins & 1023u) == 0 && *((volatile int*)A.err) != 0) break;
+                const long idx = t - lane;
+                const unsigned long long s = idx >= 0 ? ld_vol_u64(A.status + idx) : mk_status(tag, F_INC, 0, 0);
+                const bool ready = (unsigned)(s >> 60) == tag && (s & F_MASK) != 0;
+                const unsigned inc = __ballot_sync(HP_FULL_MASK, ready && (s & F_MASK) == F_INC);
+                const int stop = inc ? __ffs(inc) - 1 : 31;  // the window ends at the nearest inclusive tile
+                const unsigned need = stop == 31 ? HP_FULL_MASK : ((1u << (stop + 1)) - 1u);
+                if (__ballot_sync(HP_FULL_MASK, !ready) & need) {
+                    if (++spins > SPIN) { if (lane == 0) hp_report(A.err, HP_DEV_SPIN_LIMIT, (int)tile); break; }
+                    if ((spins & 1023u) == 0 && __shfl_sync(HP_FULL_MASK, *((volatile int*)A.err), 0) != 0) break;
                     continue;
                 }
-                pm += (unsigned)((s >> 29) & 0x1fffffffu);
-                pk += (unsigned)(s & 0x1fffffffu);
-                if ((s & F_MASK) == F_INC || t == 0) break;
-                --t;
+                unsigned vm = lane <= stop ? (unsigned)((s >> 29) & 0x1fffffffu) : 0u;
+                unsigned vk = lane <= stop ? (unsigned)(s & 0x1fffffffu) : 0u;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    vm += __shfl_xor_sync(HP_FULL_MASK, vm, o);
+                    vk += __shfl_xor_sync(HP_FULL_MASK, vk, o);
+                }
+                pm += vm;
+                pk += vk;
+                if (inc) break;
+                t -= 32;
             }
-            st_vol_u64(st, mk_status(tag, F_INC, pm + tot.x, pk + tot.y));
+            if (lane == 0) st_vol_u64(st, mk_status(tag, F_INC, pm + tot.x, pk + tot.y));
         }
-        s_pref[0] = pm;
-        s_pref[1] = pk;
-        const int tiles = (N + MT - 1) / MT;
-        if ((int)tile == tiles - 1) A.g[0] = N - (int)(pm + tot.x);
+        if (lane == 0) {
+            s_pref[0] = pm;
+            s_pref[1] = pk;
+            const int tiles = (N + MT - 1) / MT;
+            if ((int)tile == tiles - 1) A.g[0] = N - (int)(pm + tot.x);
+        }
     }
     __syncthreads();
     int mr = (int)s_pref[0] + em, kr = (int)s_pref[1] + ek;
@@ -296,7 +371,10 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
         const int r = radius_at(A, it);
         const int* cl_in = (it & 1) ? A.cl1 : A.cl0;
         int* cl_out = (it & 1) ? A.cl0 : A.cl1;
-        for (int tile = blockIdx.x; tile * PB < N; tile += gridDim.x) nn_tile(A, cl_in, N, r, tile, s_win);
+        if (N >= NB4_MIN_N)
+            for (int tile = blockIdx.x; tile * (NB4 * PB) < N; tile += gridDim.x) nn_tile<NB4>(A, cl_in, N, r, tile, s_win);
+        else
+            for (int tile = blockIdx.x; tile * PB < N; tile += gridDim.x) nn_tile<1>(A, cl_in, N, r, tile, s_win);
         if (!grid_barrier(A.bar, A.err)) break;
         while (true) {
             if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);

@@ -99,8 +99,8 @@ __device__ __forceinline__ void scan256x2(uint32_t a, uint32_t b, uint32_t& ea, 
 // Digit-offset look-back for digit `tid` of this tile: the sum of the digit's
 // counts over all earlier tiles, walking back over LB status words per round
 // until a tile whose inclusive prefix is published. Every wait is bounded.
+template <int LB>
 __device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t tile, int tid, int* err) {
-    constexpr int LB = 4;
     uint32_t prefix = 0, spins = 0;
     int64_t t = (int64_t)tile - 1;
     bool done = tile == 0;
@@ -141,7 +141,7 @@ __device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t ti
 //      the counts from round to round;
 //   5. stage the keys in shared memory in digit order and write them out, so
 //      that runs of equal digits leave as contiguous stores.
-template <typename K, int BLOCK, int ITEMS>
+template <typename K, int BLOCK, int ITEMS, int LB = 4>
 __global__ void __launch_bounds__(BLOCK) k_onesweep(
     const K* __restrict__ keys_in, const int32_t* __restrict__ vals_in,
     K* __restrict__ keys_out, int32_t* __restrict__ vals_out, int64_t n, int shift,
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     scan256x2(total, hval, block_start, hist_excl, s_w);
     if (tid < 256) {
         s_block_start[tid] = block_start;
-        const uint32_t prefix = lookback(status, tile, tid, err);
+        const uint32_t prefix = lookback<LB>(status, tile, tid, err);
         if (tile > 0) st_relaxed_u32(&status[(size_t)tile * 256 + tid], ST_FLAG_P | (prefix + total));
         s_global[tid] = hist_excl + prefix - block_start;
     }

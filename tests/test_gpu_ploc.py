@@ -40,6 +40,18 @@ def test_ploc_bit_exact(ctx, n):
     assert bvh.cost() == pytest.approx(oracle.cost(ref["nodes"], ref["box"]), rel=1e-12)
 
 
+@pytest.mark.parametrize("n,radius,adaptive", [(1_500_000, 16, 0), (1_300_000, 2, 0), (1_250_000, 4, 0),
+                                               (1_400_000, 7, 0), (1_300_000, 3, 1)])
+def test_ploc_bit_exact_long_lists(ctx, n, radius, adaptive):
+    """Lists of at least 2 * 148 * 4096 clusters take the neighbour search with
+    four clusters per thread (its run split for r >= 4, the tested path below)."""
+    v, t = hp.gen.clustered_mesh(700 + n, n, clusters=1024)
+    bvh, ref, V, T = _ploc(ctx, v, t, ploc_radius=radius, ploc_max_radius=max(radius, 9), ploc_adaptive=adaptive)
+    nodes, woop, tri = bvh.download()
+    np.testing.assert_array_equal(tri, ref["tri_idx"])
+    np.testing.assert_array_equal(nodes, ref["nodes"])
+
+
 def test_ploc_adaptive_radius_and_fixed_leaves(ctx):
     v, t = hp.gen.uniform_mesh(9, 30000)
     bvh, ref, V, T = _ploc(ctx, v, t, ploc_radius=1, ploc_max_radius=24, ploc_adaptive=1)
