@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
 // choice) is chosen at run time.
 template <typename K> struct sort_cfg;
 template <> struct sort_cfg<uint32_t> { static constexpr int BLOCK = 512, ITEMS = 12; };
-template <> struct sort_cfg<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 8; };
+template <> struct sort_cfg<uint64_t> { static constexpr int BLOCK = 512, ITEMS = 10; };
 
 template <typename K, int BLOCK>
 constexpr size_t onesweep_smem() {
