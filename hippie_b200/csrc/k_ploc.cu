@@ -35,10 +35,19 @@
 namespace {
 
 constexpr int PB = 1024;            // threads per CTA
+static_assert(PB == 1024, "block_scan2 scans 32 warp totals with one warp");
 constexpr int MAXR = 512;           // largest radius kept in a shared-memory window
 constexpr int NB4 = 4;              // clusters per thread of the neighbour search on large lists
 constexpr int WIN = NB4 * PB + 2 * MAXR;  // neighbour window
 constexpr int NB4_MIN_N = 2 * 148 * NB4 * PB;  // lists at least this long use 4 clusters per thread
+// Shorter lists run fused iterations: a tile of PB clusters finds the nearest
+// neighbours of its clusters and of r clusters on each side itself, so each
+// iteration needs one grid barrier instead of two.
+constexpr int NNF = PB + 2 * MAXR;             // neighbour slots of a fused tile
+// Clusters of a fused tile: PB - 2r (one thread per cluster of the tile and its
+// halo), at least PB / 2.
+__host__ __device__ constexpr int fused_tile(int r) { return 2 * r <= PB / 2 ? PB - 2 * r : PB / 2; }
+constexpr size_t LOOP_SMEM = 6 * WIN * sizeof(float) + NNF * sizeof(int);
 constexpr int MT_ITEMS = 4;         // clusters per thread in the merge phase
 constexpr int MT = PB * MT_ITEMS;
 constexpr int TAIL = 2048;          // clusters finished by a single CTA
@@ -75,7 +84,8 @@ struct ploc_args {
     int* cl0;
     int* cl1;
     int* nn;
-    unsigned long long* status;
+    unsigned long long* status;    // look-back words of the two-phase iterations (tiles of MT)
+    unsigned long long* status_f;  // look-back words of the fused iterations (tiles of PB)
     unsigned* tickets;  // [MAX_ITER]
     unsigned* bar;      // [0] arrivals, [1] generation
     int* g;             // [0] cluster count, [1] iterations done
@@ -252,6 +262,7 @@ __device__ __forceinline__ unsigned long long mk_status(unsigned tag, unsigned l
 }
 
 // Block-wide exclusive scan of (a, b) over PB threads. Returns the totals.
+// s_wa and s_wb hold PB / 32 + 1 entries.
 __device__ __forceinline__ int2 block_scan2(int& a, int& b, int* s_wa, int* s_wb) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int ia = a, ib = b;
@@ -263,31 +274,100 @@ __device__ __forceinline__ int2 block_scan2(int& a, int& b, int* s_wa, int* s_wb
     __syncthreads();
     if (lane == 31) { s_wa[warp] = ia; s_wb[warp] = ib; }
     __syncthreads();
-    int oa = 0, ob = 0, ta = 0, tb = 0;
-    for (int w = 0; w < PB / 32; ++w) {
-        if (w < warp) { oa += s_wa[w]; ob += s_wb[w]; }
-        ta += s_wa[w];
-        tb += s_wb[w];
+    if (warp == 0) {  // exclusive scan of the warp totals (PB / 32 == 32 of them); totals at [32]
+        const int va = s_wa[lane], vb = s_wb[lane];
+        int xa = va, xb = vb;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ya = __shfl_up_sync(HP_FULL_MASK, xa, o), yb = __shfl_up_sync(HP_FULL_MASK, xb, o);
+            if (lane >= o) { xa += ya; xb += yb; }
+        }
+        s_wa[lane] = xa - va;
+        s_wb[lane] = xb - vb;
+        if (lane == 31) { s_wa[32] = xa; s_wb[32] = xb; }
     }
-    a = oa + ia - a;
-    b = ob + ib - b;
-    return make_int2(ta, tb);
+    __syncthreads();
+    a = s_wa[warp] + ia - a;
+    b = s_wb[warp] + ib - b;
+    return make_int2(s_wa[32], s_wb[32]);
 }
 
-// One merge tile of MT clusters: flags, prefix sums (tile + look-back), new nodes, compaction.
+// Nearest neighbours of the clusters [tbase - r, tbase + tsz + r) of a fused
+// tile (s_nn[l] for cluster tbase - r + l), from the boxes of clusters
+// [tbase - 2r, tbase + tsz + 2r) in shared memory; candidates in increasing
+// order, the first strict minimum, as in nn_tile.
+__device__ void nn_halo(const ploc_args& A, const int* __restrict__ cl, int N, int r, int tbase, int tsz, float* s,
+                        int* s_nn) {
+    float* smnx = s;
+    float* smny = s + WIN;
+    float* smnz = s + 2 * WIN;
+    float* smxx = s + 3 * WIN;
+    float* smxy = s + 4 * WIN;
+    float* smxz = s + 5 * WIN;
+    const int w0 = tbase - 2 * r;
+    for (int k = threadIdx.x; k < tsz + 4 * r; k += PB) {
+        const int c = w0 + k;
+        if (c >= 0 && c < N) {
+            const int node = cl[c];
+            const float4 mn = __ldcg(A.nbmin + node), mx = __ldcg(A.nbmax + node);
+            smnx[k] = mn.x; smny[k] = mn.y; smnz[k] = mn.z;
+            smxx[k] = mx.x; smxy[k] = mx.y; smxz[k] = mx.z;
+        } else {
+            smnx[k] = smny[k] = smnz[k] = -HP_MAX_FLOAT;
+            smxx[k] = smxy[k] = smxz[k] = HP_MAX_FLOAT;
+        }
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < tsz + 2 * r; l += PB) {
+        const int c = tbase - r + l;
+        int bi = -1;
+        if (c >= 0 && c < N) {
+            const int me = l + r;  // window position of cluster c; its candidates are l .. l + 2r
+            const float ax = smnx[me], ay = smny[me], az = smnz[me], bx = smxx[me], by = smxy[me], bz = smxz[me];
+            float best = HP_MAX_FLOAT;
+            for (int k = l; k <= l + 2 * r; ++k) {
+                if (k == me) continue;
+                const float d = half_area(fminf(ax, smnx[k]), fminf(ay, smny[k]), fminf(az, smnz[k]),
+                                          fmaxf(bx, smxx[k]), fmaxf(by, smxy[k]), fmaxf(bz, smxz[k]));
+                if (best > d) {
+                    best = d;
+                    bi = w0 + k;
+                }
+            }
+        }
+        s_nn[l] = bi;
+    }
+    __syncthreads();
+}
+
+// One merge tile of ITEMS*PB clusters: flags, prefix sums (tile + look-back),
+// new nodes, compaction. FUSED tiles (ITEMS 1) find their neighbours first;
+// the others read the neighbour phase's results.
+template <int ITEMS, bool FUSED>
 __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, int* __restrict__ cl_out,
-                           int N, int it, unsigned tile, int* s_wa, int* s_wb, unsigned* s_pref) {
+                           int N, int r, int it, unsigned tile, int TSZ, unsigned long long* status, float* s_win,
+                           int* s_nn, int* s_wa, int* s_wb, unsigned* s_pref) {
     const unsigned tag = (unsigned)(it % 15) + 1u;
-    const int base = (int)tile * MT + threadIdx.x * MT_ITEMS;
-    int kind[MT_ITEMS];  // 0: dropped (higher partner), 1: kept, 2: merges with nn
+    const int tbase = (int)tile * TSZ;
+    if (FUSED) {
+        __syncthreads();  // the previous tile's shared memory is free
+        nn_halo(A, cl_in, N, r, tbase, TSZ, s_win, s_nn);
+    }
+    const int nlo = tbase - r;  // cluster of s_nn[0]
+    auto nn_of = [&](int c) { return FUSED ? s_nn[c - nlo] : A.nn[c]; };
+    const int base = tbase + threadIdx.x * ITEMS;
+    int kind[ITEMS];  // 0: dropped (higher partner), 1: kept, 2: merges with nn
+    int nbr[ITEMS];
     int m = 0, k = 0;
 #pragma unroll
-    for (int q = 0; q < MT_ITEMS; ++q) {
+    for (int q = 0; q < ITEMS; ++q) {
         const int c = base + q;
         kind[q] = 0;
-        if (c < N) {
-            const int j = A.nn[c];
-            const bool mutual = j >= 0 && j < N && A.nn[j] == c;
+        nbr[q] = -1;
+        if (c < N && (!FUSED || (int)threadIdx.x < TSZ)) {
+            const int j = nn_of(c);
+            nbr[q] = j;
+            const bool mutual = j >= 0 && j < N && (!FUSED || (j >= nlo && j < tbase + TSZ + r)) && nn_of(j) == c;
             kind[q] = (mutual && c < j) ? 2 : ((mutual && j < c) ? 0 : 1);
             m += kind[q] == 2;
             k += kind[q] != 0;
@@ -300,7 +380,7 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
         // reads tile t-i; the window is summed up to the nearest tile whose
         // inclusive prefix is published, once every tile up to it has published.
         const int lane = threadIdx.x;
-        unsigned long long* st = A.status + tile;
+        unsigned long long* st = status + tile;
         if (lane == 0) st_vol_u64(st, mk_status(tag, tile == 0 ? F_INC : F_AGG, tot.x, tot.y));
         unsigned pm = 0, pk = 0;
         if (tile > 0) {
@@ -308,7 +388,7 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
             unsigned spins = 0;
             while (true) {
                 const long idx = t - lane;
-                const unsigned long long s = idx >= 0 ? ld_vol_u64(A.status + idx) : mk_status(tag, F_INC, 0, 0);
+                const unsigned long long s = idx >= 0 ? ld_vol_u64(status + idx) : mk_status(tag, F_INC, 0, 0);
                 const bool ready = (unsigned)(s >> 60) == tag && (s & F_MASK) != 0;
                 const unsigned inc = __ballot_sync(HP_FULL_MASK, ready && (s & F_MASK) == F_INC);
                 const int stop = inc ? __ffs(inc) - 1 : 31;  // the window ends at the nearest inclusive tile
@@ -335,19 +415,19 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
         if (lane == 0) {
             s_pref[0] = pm;
             s_pref[1] = pk;
-            const int tiles = (N + MT - 1) / MT;
+            const int tiles = (N + TSZ - 1) / TSZ;
             if ((int)tile == tiles - 1) A.g[0] = N - (int)(pm + tot.x);
         }
     }
     __syncthreads();
     int mr = (int)s_pref[0] + em, kr = (int)s_pref[1] + ek;
 #pragma unroll
-    for (int q = 0; q < MT_ITEMS; ++q) {
+    for (int q = 0; q < ITEMS; ++q) {
         const int c = base + q;
         if (kind[q] == 0) continue;
         int node = cl_in[c];
         if (kind[q] == 2) {
-            const int nb = cl_in[A.nn[c]];
+            const int nb = cl_in[nbr[q]];
             const int idx = (N - 2) - mr;
             make_parent(A, idx, node, nb);
             node = idx;
@@ -359,7 +439,8 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
 
 __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
     extern __shared__ float s_win[];
-    __shared__ int s_wa[PB / 32], s_wb[PB / 32];
+    int* s_nn = reinterpret_cast<int*>(s_win + 6 * WIN);
+    __shared__ int s_wa[PB / 32 + 1], s_wb[PB / 32 + 1];
     __shared__ unsigned s_pref[2];
     __shared__ unsigned s_ticket;
     __shared__ int s_n;
@@ -371,18 +452,30 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
         const int r = radius_at(A, it);
         const int* cl_in = (it & 1) ? A.cl1 : A.cl0;
         int* cl_out = (it & 1) ? A.cl0 : A.cl1;
-        if (N >= NB4_MIN_N)
+        const bool fused = N < NB4_MIN_N;
+        if (!fused) {
             for (int tile = blockIdx.x; tile * (NB4 * PB) < N; tile += gridDim.x) nn_tile<NB4>(A, cl_in, N, r, tile, s_win);
-        else
-            for (int tile = blockIdx.x; tile * PB < N; tile += gridDim.x) nn_tile<1>(A, cl_in, N, r, tile, s_win);
-        if (!grid_barrier(A.bar, A.err)) break;
-        while (true) {
-            if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);
-            __syncthreads();
-            const unsigned tile = s_ticket;
-            __syncthreads();
-            if ((long)tile * MT >= N) break;
-            merge_tile(A, cl_in, cl_out, N, it, tile, s_wa, s_wb, s_pref);
+            if (!grid_barrier(A.bar, A.err)) break;
+        }
+        if (fused) {
+            // Tiles of PB - 2r clusters, so that a tile and its halo take one
+            // thread per cluster; every CTA takes its tiles in increasing order
+            // (all CTAs are resident), so each look-back waits only on lower
+            // tiles that are in progress.
+            const int tsz = fused_tile(r);
+            for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
+                merge_tile<1, true>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status_f, s_win, s_nn, s_wa, s_wb,
+                                    s_pref);
+        } else {
+            while (true) {
+                if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);
+                __syncthreads();
+                const unsigned tile = s_ticket;
+                __syncthreads();
+                if ((long)tile * MT >= N) break;
+                merge_tile<MT_ITEMS, false>(A, cl_in, cl_out, N, r, it, tile, MT, A.status, s_win, s_nn, s_wa,
+                                            s_wb, s_pref);
+            }
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) A.g[1] = it + 1;
         if (!grid_barrier(A.bar, A.err)) break;
@@ -398,7 +491,7 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
     float(*smx)[TAIL] = reinterpret_cast<float(*)[TAIL]>(s_tail + 3 * TAIL);
     int* snode = reinterpret_cast<int*>(s_tail + 6 * TAIL);
     int* snn = reinterpret_cast<int*>(s_tail + 7 * TAIL);
-    __shared__ int s_wa[PB / 32], s_wb[PB / 32];
+    __shared__ int s_wa[PB / 32 + 1], s_wb[PB / 32 + 1];
     __shared__ int s_n;
     if (*((volatile int*)A.err) != 0) return;
     const int it0 = A.g[1];
@@ -668,6 +761,7 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
     b += hp_carve::pad(nn);            // state
     b += 3 * hp_carve::pad(n * 4);     // cl0, cl1, nn
     b += hp_carve::pad(((n + MT - 1) / MT + 1) * 8);
+    b += hp_carve::pad(((std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1) * 8);
     b += hp_carve::pad(MAX_ITER * 4 + 64);
     b += hp_carve::pad(n * 16) + hp_carve::pad(n * 4);  // records, flags
     return b;
@@ -703,6 +797,8 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     A.nn = cv.take<int>(n);
     const int64_t mtiles = (n + MT - 1) / MT + 1;
     A.status = cv.take<unsigned long long>(mtiles);
+    const int64_t ftiles = (std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1;
+    A.status_f = cv.take<unsigned long long>(ftiles);
     unsigned* ctl = cv.take<unsigned>(MAX_ITER + 16);
     A.tickets = ctl;
     A.bar = ctl + MAX_ITER;
@@ -711,6 +807,7 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     int4* rec = cv.take<int4>(n);
     int* flag = cv.take<int>(n);
     HP_CUDA(cudaMemsetAsync(A.status, 0, mtiles * 8, s));
+    HP_CUDA(cudaMemsetAsync(A.status_f, 0, ftiles * 8, s));
     HP_CUDA(cudaMemsetAsync(ctl, 0, (MAX_ITER + 16) * 4, s));
     HP_CUDA(cudaMemsetAsync(flag, 0, (size_t)n * 4, s));
     k_ploc_leaves<<<hp_div_up(n, 256), 256, 0, s>>>(A, sorted_tri, tbmin, tbmax);
@@ -718,7 +815,7 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     hp_count_launch();
     hp_mark(ctx, s, "ploc_leaves");
     if (n > TAIL) {
-        const size_t smem = 6 * WIN * sizeof(float);
+        const size_t smem = LOOP_SMEM;
         HP_CUDA(cudaFuncSetAttribute(k_ploc_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ploc_loop, PB, smem));
