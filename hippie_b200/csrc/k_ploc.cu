@@ -9,12 +9,18 @@
 // the clusters are compacted in order. The reference runs ~5 kernels and a
 // host read-back per iteration; here
 //   * one persistent cooperative kernel runs every iteration while more than
-//     TAIL clusters remain: a neighbour phase over shared-memory windows
-//     (four clusters per thread on long lists), a
-//     grid barrier, a merge/compaction phase whose two prefix sums (merges,
-//     survivors) come from a decoupled look-back over tiles taken in ticket
-//     order, and another barrier. Every wait is bounded; a wait that gives up
-//     records an error and the kernel stops iterating;
+//     TAIL clusters remain. A tile of clusters loads the boxes of the tile and
+//     2r clusters on each side into shared memory and finds the nearest
+//     neighbours of its clusters and of r clusters on each side (four
+//     clusters per thread on long lists, one on shorter ones; a tile holds
+//     4*PB - 2r or PB - 2r clusters so that it and its halo take every thread
+//     once), so each mutual pair of the tile is decided without another
+//     tile's results; it then flags the merges, takes the two prefix sums
+//     (merges, survivors) by a decoupled look-back over lower tiles, creates
+//     the new nodes and compacts the clusters. Each CTA takes its tiles in
+//     increasing order; one grid barrier ends the iteration. Every wait is
+//     bounded; a wait that gives up records an error and the kernel stops
+//     iterating;
 //   * one CTA finishes the last TAIL clusters in shared memory;
 //   * merge numbering is by cluster order (k = merges at lower positions), so
 //     the tree is deterministic; the reference takes k from warp atomics.
@@ -43,13 +49,12 @@ constexpr int NB4_MIN_N = 2 * 148 * NB4 * PB;  // lists at least this long use 4
 // Shorter lists run fused iterations: a tile of PB clusters finds the nearest
 // neighbours of its clusters and of r clusters on each side itself, so each
 // iteration needs one grid barrier instead of two.
-constexpr int NNF = PB + 2 * MAXR;             // neighbour slots of a fused tile
+constexpr int NNF = NB4 * PB;                  // neighbour slots of a tile and its halo
+constexpr int MIN_TILE4 = NB4 * PB - 2 * MAXR;   // fewest clusters of a tile of the long lists
 // Clusters of a fused tile: PB - 2r (one thread per cluster of the tile and its
 // halo), at least PB / 2.
 __host__ __device__ constexpr int fused_tile(int r) { return 2 * r <= PB / 2 ? PB - 2 * r : PB / 2; }
 constexpr size_t LOOP_SMEM = 6 * WIN * sizeof(float) + NNF * sizeof(int);
-constexpr int MT_ITEMS = 4;         // clusters per thread in the merge phase
-constexpr int MT = PB * MT_ITEMS;
 constexpr int TAIL = 2048;          // clusters finished by a single CTA
 constexpr int TAIL_ITEMS = TAIL / PB;
 constexpr int MAX_ITER = 1 << 16;
@@ -83,9 +88,8 @@ struct ploc_args {
     uint8_t* state;
     int* cl0;
     int* cl1;
-    int* nn;
-    unsigned long long* status;    // look-back words of the two-phase iterations (tiles of MT)
-    unsigned long long* status_f;  // look-back words of the fused iterations (tiles of PB)
+    unsigned long long* status;    // look-back words of the iterations on long lists
+    unsigned long long* status_f;  // look-back words of the iterations on shorter lists
     unsigned* tickets;  // [MAX_ITER]
     unsigned* bar;      // [0] arrivals, [1] generation
     int* g;             // [0] cluster count, [1] iterations done
@@ -165,7 +169,8 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
 // candidates are walked in five runs whose valid clusters are known without a
 // test per pair (runs valid for r >= 4).
 template <int B>
-__device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int tile, float* s) {
+__device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int base, float* s,
+                        int* s_nn) {
     float* smnx = s;
     float* smny = s + WIN;
     float* smnz = s + 2 * WIN;
@@ -173,7 +178,6 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
     float* smxy = s + 4 * WIN;
     float* smxz = s + 5 * WIN;
     constexpr int TS = B * PB;
-    const int base = tile * TS;
     __syncthreads();
     for (int k = threadIdx.x; k < TS + 2 * r; k += PB) {
         const int c = base - r + k;
@@ -189,7 +193,6 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
     }
     __syncthreads();
     const int l0 = threadIdx.x * B;  // cluster base + l sits at window position l + r
-    if (base + l0 >= N) return;
     float ax[B], ay[B], az[B], bx[B], by[B], bz[B], best[B];
     int bi[B];
 #pragma unroll
@@ -249,8 +252,11 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
     }
 #undef HP_PLOC_CAND
 #pragma unroll
-    for (int q = 0; q < B; ++q)
-        if (base + l0 + q < N) A.nn[base + l0 + q] = bi[q];
+    for (int q = 0; q < B; ++q) {
+        const int c = base + l0 + q;
+        s_nn[l0 + q] = (c >= 0 && c < N) ? bi[q] : -1;
+    }
+    __syncthreads();
 }
 
 // Status word of a merge tile: [63:60] iteration tag, [59:58] flag, [57:29] merges, [28:0] survivors.
@@ -343,18 +349,17 @@ __device__ void nn_halo(const ploc_args& A, const int* __restrict__ cl, int N, i
 // One merge tile of ITEMS*PB clusters: flags, prefix sums (tile + look-back),
 // new nodes, compaction. FUSED tiles (ITEMS 1) find their neighbours first;
 // the others read the neighbour phase's results.
-template <int ITEMS, bool FUSED>
+template <int ITEMS>
 __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, int* __restrict__ cl_out,
                            int N, int r, int it, unsigned tile, int TSZ, unsigned long long* status, float* s_win,
                            int* s_nn, int* s_wa, int* s_wb, unsigned* s_pref) {
     const unsigned tag = (unsigned)(it % 15) + 1u;
     const int tbase = (int)tile * TSZ;
-    if (FUSED) {
-        __syncthreads();  // the previous tile's shared memory is free
-        nn_halo(A, cl_in, N, r, tbase, TSZ, s_win, s_nn);
-    }
+    __syncthreads();  // the previous tile's shared memory is free
+    if (ITEMS == 1) nn_halo(A, cl_in, N, r, tbase, TSZ, s_win, s_nn);
+    else nn_tile<ITEMS>(A, cl_in, N, r, tbase - r, s_win, s_nn);  // TSZ + 2r <= ITEMS * PB clusters
     const int nlo = tbase - r;  // cluster of s_nn[0]
-    auto nn_of = [&](int c) { return FUSED ? s_nn[c - nlo] : A.nn[c]; };
+    auto nn_of = [&](int c) { return s_nn[c - nlo]; };
     const int base = tbase + threadIdx.x * ITEMS;
     int kind[ITEMS];  // 0: dropped (higher partner), 1: kept, 2: merges with nn
     int nbr[ITEMS];
@@ -364,10 +369,10 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
         const int c = base + q;
         kind[q] = 0;
         nbr[q] = -1;
-        if (c < N && (!FUSED || (int)threadIdx.x < TSZ)) {
+        if (c < N && c < tbase + TSZ) {
             const int j = nn_of(c);
             nbr[q] = j;
-            const bool mutual = j >= 0 && j < N && (!FUSED || (j >= nlo && j < tbase + TSZ + r)) && nn_of(j) == c;
+            const bool mutual = j >= 0 && j < N && j >= nlo && j < tbase + TSZ + r && nn_of(j) == c;
             kind[q] = (mutual && c < j) ? 2 : ((mutual && j < c) ? 0 : 1);
             m += kind[q] == 2;
             k += kind[q] != 0;
@@ -442,7 +447,6 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
     int* s_nn = reinterpret_cast<int*>(s_win + 6 * WIN);
     __shared__ int s_wa[PB / 32 + 1], s_wb[PB / 32 + 1];
     __shared__ unsigned s_pref[2];
-    __shared__ unsigned s_ticket;
     __shared__ int s_n;
     for (int it = 0; it < MAX_ITER; ++it) {
         if (threadIdx.x == 0) s_n = *((volatile int*)A.g);
@@ -452,30 +456,23 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
         const int r = radius_at(A, it);
         const int* cl_in = (it & 1) ? A.cl1 : A.cl0;
         int* cl_out = (it & 1) ? A.cl0 : A.cl1;
-        const bool fused = N < NB4_MIN_N;
-        if (!fused) {
-            for (int tile = blockIdx.x; tile * (NB4 * PB) < N; tile += gridDim.x) nn_tile<NB4>(A, cl_in, N, r, tile, s_win);
-            if (!grid_barrier(A.bar, A.err)) break;
-        }
-        if (fused) {
-            // Tiles of PB - 2r clusters, so that a tile and its halo take one
-            // thread per cluster; every CTA takes its tiles in increasing order
-            // (all CTAs are resident), so each look-back waits only on lower
-            // tiles that are in progress.
-            const int tsz = fused_tile(r);
+        // Tiles of ITEMS*PB - 2r clusters, so that a tile and its halo take ITEMS
+        // clusters per thread; every CTA takes its tiles in increasing order (all
+        // CTAs are resident), so each look-back waits only on lower tiles that
+        // are in progress.
+        // Tile sizes use the largest radius of the build, so that the tile
+        // count of an iteration never exceeds the previous one's (the look-back
+        // words of lower tiles are then always this iteration's or older ones
+        // with another tag).
+        const int rt = A.adaptive_r ? A.max_radius : A.radius;
+        if (N >= NB4_MIN_N) {
+            const int tsz = NB4 * PB - 2 * rt;
             for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
-                merge_tile<1, true>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status_f, s_win, s_nn, s_wa, s_wb,
-                                    s_pref);
+                merge_tile<NB4>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status, s_win, s_nn, s_wa, s_wb, s_pref);
         } else {
-            while (true) {
-                if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);
-                __syncthreads();
-                const unsigned tile = s_ticket;
-                __syncthreads();
-                if ((long)tile * MT >= N) break;
-                merge_tile<MT_ITEMS, false>(A, cl_in, cl_out, N, r, it, tile, MT, A.status, s_win, s_nn, s_wa,
-                                            s_wb, s_pref);
-            }
+            const int tsz = fused_tile(rt);
+            for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
+                merge_tile<1>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status_f, s_win, s_nn, s_wa, s_wb, s_pref);
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) A.g[1] = it + 1;
         if (!grid_barrier(A.bar, A.err)) break;
@@ -759,8 +756,8 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
     b += 3 * hp_carve::pad(nn * 4);    // left, right, parent
     b += hp_carve::pad(nn * 8);        // counts
     b += hp_carve::pad(nn);            // state
-    b += 3 * hp_carve::pad(n * 4);     // cl0, cl1, nn
-    b += hp_carve::pad(((n + MT - 1) / MT + 1) * 8);
+    b += 2 * hp_carve::pad(n * 4);     // cl0, cl1
+    b += hp_carve::pad(((n + MIN_TILE4 - 1) / MIN_TILE4 + 1) * 8);
     b += hp_carve::pad(((std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1) * 8);
     b += hp_carve::pad(MAX_ITER * 4 + 64);
     b += hp_carve::pad(n * 16) + hp_carve::pad(n * 4);  // records, flags
@@ -794,8 +791,7 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     A.state = cv.take<uint8_t>(nn);
     A.cl0 = cv.take<int>(n);
     A.cl1 = cv.take<int>(n);
-    A.nn = cv.take<int>(n);
-    const int64_t mtiles = (n + MT - 1) / MT + 1;
+    const int64_t mtiles = (n + MIN_TILE4 - 1) / MIN_TILE4 + 1;
     A.status = cv.take<unsigned long long>(mtiles);
     const int64_t ftiles = (std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1;
     A.status_f = cv.take<unsigned long long>(ftiles);
