@@ -168,6 +168,42 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
 // clusters at once and reads each candidate box once for all of them; the
 // candidates are walked in five runs whose valid clusters are known without a
 // test per pair (runs valid for r >= 4).
+// Boxes of clusters [w0, w0 + wn) into the shared-memory window (a huge box,
+// never the nearest, outside the cluster list). The cluster indices of a batch
+// of elements are read first and their boxes after, so that a thread has a
+// batch of loads in flight instead of one dependent pair at a time.
+__device__ __forceinline__ void load_window(const ploc_args& A, const int* __restrict__ cl, int N, int w0, int wn,
+                                            float* s) {
+    constexpr int BATCH = 3;
+    for (int k0 = threadIdx.x; k0 < wn; k0 += BATCH * PB) {
+        int node[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const int k = k0 + u * PB, c = w0 + k;
+            node[u] = (k < wn && c >= 0 && c < N) ? __ldcg(cl + c) : -1;
+        }
+        float4 mn[BATCH], mx[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            if (node[u] >= 0) {
+                mn[u] = __ldcg(A.nbmin + node[u]);
+                mx[u] = __ldcg(A.nbmax + node[u]);
+            } else {
+                mn[u] = make_float4(-HP_MAX_FLOAT, -HP_MAX_FLOAT, -HP_MAX_FLOAT, 0.0f);
+                mx[u] = make_float4(HP_MAX_FLOAT, HP_MAX_FLOAT, HP_MAX_FLOAT, 0.0f);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const int k = k0 + u * PB;
+            if (k < wn) {
+                s[k] = mn[u].x; s[WIN + k] = mn[u].y; s[2 * WIN + k] = mn[u].z;
+                s[3 * WIN + k] = mx[u].x; s[4 * WIN + k] = mx[u].y; s[5 * WIN + k] = mx[u].z;
+            }
+        }
+    }
+}
+
 template <int B>
 __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, int r, int base, float* s,
                         int* s_nn) {
@@ -179,18 +215,7 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
     float* smxz = s + 5 * WIN;
     constexpr int TS = B * PB;
     __syncthreads();
-    for (int k = threadIdx.x; k < TS + 2 * r; k += PB) {
-        const int c = base - r + k;
-        if (c >= 0 && c < N) {
-            const int node = cl[c];
-            const float4 mn = __ldcg(A.nbmin + node), mx = __ldcg(A.nbmax + node);
-            smnx[k] = mn.x; smny[k] = mn.y; smnz[k] = mn.z;
-            smxx[k] = mx.x; smxy[k] = mx.y; smxz[k] = mx.z;
-        } else {  // outside the cluster list: a huge box that is never the nearest
-            smnx[k] = smny[k] = smnz[k] = -HP_MAX_FLOAT;
-            smxx[k] = smxy[k] = smxz[k] = HP_MAX_FLOAT;
-        }
-    }
+    load_window(A, cl, N, base - r, TS + 2 * r, s);
     __syncthreads();
     const int l0 = threadIdx.x * B;  // cluster base + l sits at window position l + r
     float ax[B], ay[B], az[B], bx[B], by[B], bz[B], best[B];
@@ -311,18 +336,7 @@ __device__ void nn_halo(const ploc_args& A, const int* __restrict__ cl, int N, i
     float* smxy = s + 4 * WIN;
     float* smxz = s + 5 * WIN;
     const int w0 = tbase - 2 * r;
-    for (int k = threadIdx.x; k < tsz + 4 * r; k += PB) {
-        const int c = w0 + k;
-        if (c >= 0 && c < N) {
-            const int node = cl[c];
-            const float4 mn = __ldcg(A.nbmin + node), mx = __ldcg(A.nbmax + node);
-            smnx[k] = mn.x; smny[k] = mn.y; smnz[k] = mn.z;
-            smxx[k] = mx.x; smxy[k] = mx.y; smxz[k] = mx.z;
-        } else {
-            smnx[k] = smny[k] = smnz[k] = -HP_MAX_FLOAT;
-            smxx[k] = smxy[k] = smxz[k] = HP_MAX_FLOAT;
-        }
-    }
+    load_window(A, cl, N, w0, tsz + 4 * r, s);
     __syncthreads();
     for (int l = threadIdx.x; l < tsz + 2 * r; l += PB) {
         const int c = tbase - r + l;
