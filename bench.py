@@ -15,8 +15,9 @@ value      build throughput, Mtris/s, inputs resident in HBM (CUDA events);
            with the default choices.
 e2e        the same metrics through the C ABI with pinned host buffers: the
            H2D copy of the mesh plus the build (and a read-back of the node
-           counts), then the H2D copy of the rays, the trace and the D2H copy
-           of all hit records.
+           counts), then hp_trace_host over the host ray and result buffers
+           (every ray uploaded and every hit record downloaded, in chunks whose
+           copies overlap the traces of their neighbours).
 roofline   the radix-sort pass (the build's HBM-bound kernel): algorithmic
            bytes n * 2 * (K + 4) per pass over its average CUDA-event duration.
 Multi-GPU: one process per GPU (torchrun), every rank builds and traces its
@@ -716,9 +717,7 @@ def main(argv=None):
         ctx.build(V, T, params, bvh=bvh)
         bvh.sync()
         b = time.perf_counter()
-        R.copy_(Rh, non_blocking=True)
-        ctx.trace(bvh, R, results=RES)
-        RESh.copy_(RES, non_blocking=True)
+        ctx.trace_host(bvh, Rh, results=RESh)  # hp_trace_host: chunked uploads / traces / downloads overlap
         torch.cuda.synchronize()
         c = time.perf_counter()
         e2e_b.append(b - a)

@@ -212,6 +212,22 @@ class Context:
                               _stream_ptr(stream)))
         return results
 
+    def trace_host(self, bvh: BVH, rays, results=None, stats=None, any_hit=False, chunk=0, stream=None):
+        """hp_trace_host: rays, results and stats in HOST memory (CPU tensors, pinned for
+        overlap); chunked uploads, traces and downloads overlap. Every result record is
+        written in full (a miss reads {-1, tmax, 0, 0}). Synchronises `stream` before
+        returning, so the results are complete."""
+        import torch
+        n = rays.shape[0]
+        assert not rays.is_cuda, "trace_host takes host tensors"
+        if results is None:
+            results = torch.empty((n, 4), dtype=torch.int32, pin_memory=rays.is_pinned())
+        flags = (HP_TRACE_ANY_HIT if any_hit else 0) | (HP_TRACE_STATS if stats is not None else 0)
+        check(load().hp_trace_host(self.h, C.byref(bvh.c), _ptr(rays), n, _ptr(results), _ptr(stats), flags,
+                                   chunk, _stream_ptr(stream)))
+        (torch.cuda.current_stream() if stream is None else stream).synchronize()
+        return results
+
     def trace_sorted(self, bvh: BVH, rays, results=None, stats=None, any_hit=False, bits=30, order=None,
                      stream=None):
         """HipTracer::traceSort: trace in ray Morton order; results at each ray's own index."""

@@ -103,6 +103,7 @@ _SIGS = {
     "hp_batch_build_trace": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "hp_batch_bvh": (C.c_int, [_P, C.c_int32, C.POINTER(hp_bvh)]),
     "hp_trace_sorted": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, C.c_int32, _P, _P]),
+    "hp_trace_host": (C.c_int, [_P, C.POINTER(hp_bvh), _P, C.c_int64, _P, _P, C.c_uint32, C.c_int64, _P]),
     "hp_pixel_table": (C.c_int, [C.c_int32, C.c_int32, _P]),
     "hp_scene_read_bin": (C.c_int, [C.c_char_p, C.POINTER(hp_host_scene)]),
     "hp_scene_write_bin": (C.c_int, [C.c_char_p, C.POINTER(hp_host_scene)]),

@@ -230,6 +230,14 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
     cudaFreeHost(ctx->h_status);
     for (int i = 0; i < ctx->cap_marks; ++i) cudaEventDestroy(ctx->marks[i].ev);
     delete[] ctx->marks;
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(ctx->io_slot[i]);
+        if (ctx->io_up[i]) cudaEventDestroy(ctx->io_up[i]);
+        if (ctx->io_traced[i]) cudaEventDestroy(ctx->io_traced[i]);
+        if (ctx->io_free[i]) cudaEventDestroy(ctx->io_free[i]);
+    }
+    if (ctx->io_h2d) cudaStreamDestroy(ctx->io_h2d);
+    if (ctx->io_d2h) cudaStreamDestroy(ctx->io_d2h);
     delete ctx;
     return HP_OK;
 }
@@ -402,6 +410,67 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
         return hp_trace_sorted(ctx, bvh, rays, num_rays, results, stats, flags, 30, nullptr, stream);
     return hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays,
                            num_rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, int64_t num_rays,
+                        int32_t* results_host, int32_t* stats_host, uint32_t flags, int64_t chunk_rays,
+                        void* stream) {
+    if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_trace_host: null argument");
+    if (num_rays < 0 || chunk_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_host: negative count");
+    if (num_rays == 0) return HP_OK;
+    if (!rays_host || !results_host) return hp_fail(HP_ERR_ARG, "hp_trace_host: null ray or result buffer");
+    const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 22), num_rays);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // slot layout: rays (32 B per ray), results (16 B), stats (8 B)
+    const size_t ray_b = hp_carve::pad((size_t)C * 32), res_b = hp_carve::pad((size_t)C * 16);
+    const size_t need = ray_b + res_b + hp_carve::pad((size_t)C * 8);
+    if (!ctx->io_h2d) {
+        HP_CUDA(cudaStreamCreateWithFlags(&ctx->io_h2d, cudaStreamNonBlocking));
+        HP_CUDA(cudaStreamCreateWithFlags(&ctx->io_d2h, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            HP_CUDA(cudaEventCreateWithFlags(&ctx->io_up[i], cudaEventDisableTiming));
+            HP_CUDA(cudaEventCreateWithFlags(&ctx->io_traced[i], cudaEventDisableTiming));
+            HP_CUDA(cudaEventCreateWithFlags(&ctx->io_free[i], cudaEventDisableTiming));
+        }
+    }
+    if (ctx->io_slot_bytes < need) {
+        // earlier calls may still use the slots
+        HP_CUDA(cudaStreamSynchronize(ctx->io_d2h));
+        for (int i = 0; i < 2; ++i) {
+            HP_CUDA(cudaFree(ctx->io_slot[i]));
+            ctx->io_slot[i] = nullptr;
+        }
+        ctx->io_slot_bytes = 0;
+        for (int i = 0; i < 2; ++i) HP_CUDA(cudaMalloc(&ctx->io_slot[i], need));
+        ctx->io_slot_bytes = need;
+    }
+    const int64_t chunks = (num_rays + C - 1) / C;
+    for (int64_t i = 0; i < chunks; ++i) {
+        const int k = (int)(i & 1);
+        const int64_t off = i * C, m = std::min(C, num_rays - off);
+        float* d_rays = reinterpret_cast<float*>(ctx->io_slot[k]);
+        int32_t* d_res = reinterpret_cast<int32_t*>(ctx->io_slot[k] + ray_b);
+        int32_t* d_stats = stats_host ? reinterpret_cast<int32_t*>(ctx->io_slot[k] + ray_b + res_b) : nullptr;
+        // up: once the slot's previous results are home
+        HP_CUDA(cudaStreamWaitEvent(ctx->io_h2d, ctx->io_free[k], 0));
+        HP_CUDA(cudaMemcpyAsync(d_rays, rays_host + 8 * off, (size_t)m * 32, cudaMemcpyHostToDevice, ctx->io_h2d));
+        HP_CUDA(cudaEventRecord(ctx->io_up[k], ctx->io_h2d));
+        // trace on the caller's stream
+        HP_CUDA(cudaStreamWaitEvent(s, ctx->io_up[k], 0));
+        HP_CUDA(cudaMemsetAsync(d_res, 0, (size_t)m * 16, s));
+        HP_TRY(hp_trace(ctx, bvh, d_rays, m, d_res, d_stats, flags, stream));
+        HP_CUDA(cudaEventRecord(ctx->io_traced[k], s));
+        // down
+        HP_CUDA(cudaStreamWaitEvent(ctx->io_d2h, ctx->io_traced[k], 0));
+        HP_CUDA(cudaMemcpyAsync(results_host + 4 * off, d_res, (size_t)m * 16, cudaMemcpyDeviceToHost, ctx->io_d2h));
+        if (stats_host)
+            HP_CUDA(cudaMemcpyAsync(stats_host + 2 * off, d_stats, (size_t)m * 8, cudaMemcpyDeviceToHost,
+                                    ctx->io_d2h));
+        HP_CUDA(cudaEventRecord(ctx->io_free[k], ctx->io_d2h));
+    }
+    // the caller's stream completes once every result is home
+    for (int k = 0; k < 2; ++k) HP_CUDA(cudaStreamWaitEvent(s, ctx->io_free[k], 0));
+    return HP_OK;
 }
 
 hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays, const int32_t* results,

@@ -265,6 +265,20 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream);
 hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays,
                    int32_t* results, int32_t* stats, uint32_t flags, void* stream);
 
+/* hp_trace over HOST buffers (HipTracer::trace on a RayBuffer whose rays live
+ * in host memory, which the reference's Buffer migrates to the device on use,
+ * utils/Buffer.cpp:437-498): rays_host, results_host and stats_host (or NULL)
+ * are host memory, pinned for overlap. The rays go up in chunks of
+ * chunk_rays (0: 4,194,304) on a copy stream while the previous chunk is
+ * traced on `stream` and the one before comes back on another copy stream,
+ * through two device staging slots the context keeps. Results are identical
+ * to hp_trace's, except that every result record is written in full (a miss
+ * reads {-1, tmax bits, 0, 0}). The call is asynchronous on `stream`: the
+ * host buffers may be read / are complete once `stream` has synchronised. */
+hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, int64_t num_rays,
+                        int32_t* results_host, int32_t* stats_host, uint32_t flags, int64_t chunk_rays,
+                        void* stream);
+
 /* Trace in ray Morton order (HipTracer::traceSort, rt/tracer/HipTracer.cpp:109-125;
  * RayBuffer::mortonSort, rt/ray/RayBuffer.cpp:112-131): keys as hp_ray_keys
  * with the reference's [0,1]^3 ray box and `bits` key bits (the reference's

@@ -33,6 +33,7 @@ def test_bad_arguments_are_rejected():
     assert lib.hp_build(None, None, None, None, None, None) == 2
     assert lib.hp_trace(None, None, None, 0, None, None, 0, None) == 2
     assert lib.hp_radix_sort(None, None, None, None, None, 10, 4, 32, None) == 2
+    assert lib.hp_trace_host(None, None, None, 10, None, None, 0, 0, None) == 2
     assert b"null" in lib.hp_last_error()
 
 
