@@ -267,7 +267,7 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
 
 /* hp_trace over HOST buffers (HipTracer::trace on a RayBuffer whose rays live
  * in host memory, which the reference's Buffer migrates to the device on use,
- * utils/Buffer.cpp:437-498): rays_host, results_host and stats_host (or NULL)
+ * gpu/Buffer.cpp:437-498): rays_host, results_host and stats_host (or NULL)
  * are host memory, pinned for overlap. The rays go up in chunks of
  * chunk_rays (0: 4,194,304) on a copy stream while the previous chunk is
  * traced on `stream` and the one before comes back on another copy stream,
