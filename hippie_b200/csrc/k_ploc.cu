@@ -65,6 +65,16 @@ __device__ __forceinline__ unsigned ld_vol_u32(const unsigned* p) {
     asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Acquire load / release store at GPU scope: a record written before the
+// release store is visible to a thread whose acquire load sees the flag.
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ unsigned long long ld_vol_u64(const unsigned long long* p) {
     unsigned long long v;
     asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
@@ -650,38 +660,39 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
             hp_report(T.err, HP_DEV_BAD_INDEX, v);
             return;
         }
+        // what does not depend on the parent's record is read before waiting for it
+        const bool is_left = T.left[p] == v;
+        const int sib = is_left ? T.right[p] : T.left[p];
+        const int2 cs = T.counts[sib];
+        const int ssize = __float_as_int(T.nbmax[sib].w);
+        const bool leaf = v >= n - 1 || T.state[v] == 0;
         unsigned spins = 0;
-        while (ld_vol_u32(reinterpret_cast<const unsigned*>(T.flag + p)) != (unsigned)T.epoch) {
+        while (ld_acquire_u32(reinterpret_cast<const unsigned*>(T.flag + p)) != (unsigned)T.epoch) {
             if (++spins > SPIN) {
                 hp_report(T.err, HP_DEV_SPIN_LIMIT, v);
                 break;
             }
             if ((spins & 1023u) == 0 && *((volatile int*)T.err) != 0) return;
         }
-        __threadfence();
         const int4 pr = __ldcg(T.rec + p);
-        const bool is_left = T.left[p] == v;
-        const int sib = is_left ? T.right[p] : T.left[p];
         par = pr.x;
         if (pr.w == ST_INTERIOR) {
-            status = (v >= n - 1 || T.state[v] == 0) ? ST_LEAF : ST_INTERIOR;
+            status = leaf ? ST_LEAF : ST_INTERIOR;
             if (is_left) {
                 iidx = pr.x + 1; lidx = pr.y; toff = pr.z;
             } else {
-                const int2 cs = T.counts[sib];
                 iidx = pr.x + 1 + cs.x;
                 lidx = pr.y + cs.y;
-                toff = pr.z + __float_as_int(T.nbmax[sib].w);
+                toff = pr.z + ssize;
             }
         } else {
             status = ST_DEAD;
-            toff = is_left ? pr.z : pr.z + __float_as_int(T.nbmax[sib].w);
+            toff = is_left ? pr.z : pr.z + ssize;
         }
     }
     if (v < n - 1) {
         __stcg(T.rec + v, make_int4(iidx, lidx, toff, status));
-        __threadfence();
-        *((volatile int*)(T.flag + v)) = T.epoch;
+        st_release_u32(reinterpret_cast<unsigned*>(T.flag + v), (unsigned)T.epoch);  // orders the record before
     }
     const float4 mn = T.nbmin[v], mx = T.nbmax[v];
     const int size = __float_as_int(mx.w);
