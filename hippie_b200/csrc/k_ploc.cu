@@ -13,7 +13,7 @@
 //     2r clusters on each side into shared memory and finds the nearest
 //     neighbours of its clusters and of r clusters on each side (four
 //     clusters per thread on long lists, one on shorter ones; a tile holds
-//     4*PB - 2r or PB - 2r clusters so that it and its halo take every thread
+//     4*LPB - 2r or LPB - 2r clusters so that it and its halo take every thread
 //     once), so each mutual pair of the tile is decided without another
 //     tile's results; it then flags the merges, takes the two prefix sums
 //     (merges, survivors) by a decoupled look-back over lower tiles, creates
@@ -40,20 +40,22 @@
 
 namespace {
 
-constexpr int PB = 1024;            // threads per CTA
-static_assert(PB == 1024, "block_scan2 scans 32 warp totals with one warp");
+constexpr int PB = 1024;            // threads of the tail CTA
+constexpr int LPB = 512;            // threads per CTA of the iteration kernel (two CTAs per SM)
 constexpr int MAXR = 512;           // largest radius kept in a shared-memory window
 constexpr int NB4 = 4;              // clusters per thread of the neighbour search on large lists
-constexpr int WIN = NB4 * PB + 2 * MAXR;  // neighbour window
-constexpr int NB4_MIN_N = 2 * 148 * NB4 * PB;  // lists at least this long use 4 clusters per thread
-// Shorter lists run fused iterations: a tile of PB clusters finds the nearest
+constexpr int WIN = NB4 * LPB + 2 * MAXR;  // neighbour window
+constexpr int NB4_MIN_N = 2 * 148 * NB4 * 1024;  // lists at least this long use 4 clusters per thread
+// Shorter lists run fused iterations: a tile of LPB clusters finds the nearest
 // neighbours of its clusters and of r clusters on each side itself, so each
 // iteration needs one grid barrier instead of two.
-constexpr int NNF = NB4 * PB;                  // neighbour slots of a tile and its halo
-constexpr int MIN_TILE4 = NB4 * PB - 2 * MAXR;   // fewest clusters of a tile of the long lists
-// Clusters of a fused tile: PB - 2r (one thread per cluster of the tile and its
-// halo), at least PB / 2.
-__host__ __device__ constexpr int fused_tile(int r) { return 2 * r <= PB / 2 ? PB - 2 * r : PB / 2; }
+constexpr int NNF = NB4 * LPB + 2 * MAXR;       // neighbour slots of a tile and its halo
+constexpr int MIN_TILE4 = NB4 * LPB - 2 * MAXR;  // fewest clusters of a tile of the long lists
+// Clusters of a fused tile: LPB - 2r (one thread per cluster of the tile and its
+// halo), at least LPB / 2.
+__host__ __device__ constexpr int fused_tile(int r) { return 2 * r <= LPB / 2 ? LPB - 2 * r : LPB / 2; }
+// Clusters of a tile of the long lists: 4*LPB - 2r, at least 2*LPB.
+__host__ __device__ constexpr int long_tile(int r) { return 2 * r <= 2 * LPB ? NB4 * LPB - 2 * r : 2 * LPB; }
 constexpr size_t LOOP_SMEM = 6 * WIN * sizeof(float) + NNF * sizeof(int);
 constexpr int TAIL = 2048;          // clusters finished by a single CTA
 constexpr int TAIL_ITEMS = TAIL / PB;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
     }
 }
 
-// Nearest neighbour of every cluster of one tile of B*PB clusters: the tile's
+// Nearest neighbour of every cluster of one tile of B*LPB clusters: the tile's
 // boxes and r on each side in shared memory (a huge box, never the nearest,
 // outside the cluster list); candidates c-r .. c+r in increasing order, the
 // first strict minimum. With B = 4 a thread searches for 4 consecutive
@@ -185,11 +187,11 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
 __device__ __forceinline__ void load_window(const ploc_args& A, const int* __restrict__ cl, int N, int w0, int wn,
                                             float* s) {
     constexpr int BATCH = 3;
-    for (int k0 = threadIdx.x; k0 < wn; k0 += BATCH * PB) {
+    for (int k0 = threadIdx.x; k0 < wn; k0 += BATCH * LPB) {
         int node[BATCH];
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
-            const int k = k0 + u * PB, c = w0 + k;
+            const int k = k0 + u * LPB, c = w0 + k;
             node[u] = (k < wn && c >= 0 && c < N) ? __ldcg(cl + c) : -1;
         }
         float4 mn[BATCH], mx[BATCH];
@@ -205,7 +207,7 @@ __device__ __forceinline__ void load_window(const ploc_args& A, const int* __res
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
-            const int k = k0 + u * PB;
+            const int k = k0 + u * LPB;
             if (k < wn) {
                 s[k] = mn[u].x; s[WIN + k] = mn[u].y; s[2 * WIN + k] = mn[u].z;
                 s[3 * WIN + k] = mx[u].x; s[4 * WIN + k] = mx[u].y; s[5 * WIN + k] = mx[u].z;
@@ -223,7 +225,7 @@ __device__ void nn_tile(const ploc_args& A, const int* __restrict__ cl, int N, i
     float* smxx = s + 3 * WIN;
     float* smxy = s + 4 * WIN;
     float* smxz = s + 5 * WIN;
-    constexpr int TS = B * PB;
+    constexpr int TS = B * LPB;
     __syncthreads();
     load_window(A, cl, N, base - r, TS + 2 * r, s);
     __syncthreads();
@@ -302,9 +304,11 @@ __device__ __forceinline__ unsigned long long mk_status(unsigned tag, unsigned l
            (unsigned long long)(k & 0x1fffffffu);
 }
 
-// Block-wide exclusive scan of (a, b) over PB threads. Returns the totals.
-// s_wa and s_wb hold PB / 32 + 1 entries.
+// Block-wide exclusive scan of (a, b) over NT threads (NT <= 1024). Returns
+// the totals. s_wa and s_wb hold NT / 32 + 1 entries.
+template <int NT>
 __device__ __forceinline__ int2 block_scan2(int& a, int& b, int* s_wa, int* s_wb) {
+    constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int ia = a, ib = b;
 #pragma unroll
@@ -315,22 +319,21 @@ __device__ __forceinline__ int2 block_scan2(int& a, int& b, int* s_wa, int* s_wb
     __syncthreads();
     if (lane == 31) { s_wa[warp] = ia; s_wb[warp] = ib; }
     __syncthreads();
-    if (warp == 0) {  // exclusive scan of the warp totals (PB / 32 == 32 of them); totals at [32]
-        const int va = s_wa[lane], vb = s_wb[lane];
+    if (warp == 0) {  // exclusive scan of the NW warp totals by one warp; totals at [NW]
+        const int va = lane < NW ? s_wa[lane] : 0, vb = lane < NW ? s_wb[lane] : 0;
         int xa = va, xb = vb;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int ya = __shfl_up_sync(HP_FULL_MASK, xa, o), yb = __shfl_up_sync(HP_FULL_MASK, xb, o);
             if (lane >= o) { xa += ya; xb += yb; }
         }
-        s_wa[lane] = xa - va;
-        s_wb[lane] = xb - vb;
-        if (lane == 31) { s_wa[32] = xa; s_wb[32] = xb; }
+        if (lane < NW) { s_wa[lane] = xa - va; s_wb[lane] = xb - vb; }
+        if (lane == NW - 1) { s_wa[NW] = xa; s_wb[NW] = xb; }
     }
     __syncthreads();
     a = s_wa[warp] + ia - a;
     b = s_wb[warp] + ib - b;
-    return make_int2(s_wa[32], s_wb[32]);
+    return make_int2(s_wa[NW], s_wb[NW]);
 }
 
 // Nearest neighbours of the clusters [tbase - r, tbase + tsz + r) of a fused
@@ -348,7 +351,7 @@ __device__ void nn_halo(const ploc_args& A, const int* __restrict__ cl, int N, i
     const int w0 = tbase - 2 * r;
     load_window(A, cl, N, w0, tsz + 4 * r, s);
     __syncthreads();
-    for (int l = threadIdx.x; l < tsz + 2 * r; l += PB) {
+    for (int l = threadIdx.x; l < tsz + 2 * r; l += LPB) {
         const int c = tbase - r + l;
         int bi = -1;
         if (c >= 0 && c < N) {
@@ -370,7 +373,7 @@ __device__ void nn_halo(const ploc_args& A, const int* __restrict__ cl, int N, i
     __syncthreads();
 }
 
-// One merge tile of ITEMS*PB clusters: flags, prefix sums (tile + look-back),
+// One merge tile of at most ITEMS*LPB clusters: flags, prefix sums (tile + look-back),
 // new nodes, compaction. FUSED tiles (ITEMS 1) find their neighbours first;
 // the others read the neighbour phase's results.
 template <int ITEMS>
@@ -381,7 +384,7 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
     const int tbase = (int)tile * TSZ;
     __syncthreads();  // the previous tile's shared memory is free
     if (ITEMS == 1) nn_halo(A, cl_in, N, r, tbase, TSZ, s_win, s_nn);
-    else nn_tile<ITEMS>(A, cl_in, N, r, tbase - r, s_win, s_nn);  // TSZ + 2r <= ITEMS * PB clusters
+    else nn_tile<ITEMS>(A, cl_in, N, r, tbase - r, s_win, s_nn);  // TSZ + 2r <= ITEMS * LPB clusters
     const int nlo = tbase - r;  // cluster of s_nn[0]
     auto nn_of = [&](int c) { return s_nn[c - nlo]; };
     const int base = tbase + threadIdx.x * ITEMS;
@@ -403,7 +406,7 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
         }
     }
     int em = m, ek = k;
-    const int2 tot = block_scan2(em, ek, s_wa, s_wb);
+    const int2 tot = block_scan2<LPB>(em, ek, s_wa, s_wb);
     if (threadIdx.x < 32) {
         // Decoupled look-back by one warp over windows of 32 earlier tiles: lane i
         // reads tile t-i; the window is summed up to the nearest tile whose
@@ -466,10 +469,10 @@ __device__ void merge_tile(const ploc_args& A, const int* __restrict__ cl_in, in
     }
 }
 
-__global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
+__global__ void __launch_bounds__(LPB, 2) k_ploc_loop(ploc_args A) {
     extern __shared__ float s_win[];
     int* s_nn = reinterpret_cast<int*>(s_win + 6 * WIN);
-    __shared__ int s_wa[PB / 32 + 1], s_wb[PB / 32 + 1];
+    __shared__ int s_wa[LPB / 32 + 1], s_wb[LPB / 32 + 1];
     __shared__ unsigned s_pref[2];
     __shared__ int s_n;
     for (int it = 0; it < MAX_ITER; ++it) {
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
         const int r = radius_at(A, it);
         const int* cl_in = (it & 1) ? A.cl1 : A.cl0;
         int* cl_out = (it & 1) ? A.cl0 : A.cl1;
-        // Tiles of ITEMS*PB - 2r clusters, so that a tile and its halo take ITEMS
+        // Tiles of ITEMS*LPB - 2r clusters, so that a tile and its halo take ITEMS
         // clusters per thread; every CTA takes its tiles in increasing order (all
         // CTAs are resident), so each look-back waits only on lower tiles that
         // are in progress.
@@ -490,7 +493,7 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_loop(ploc_args A) {
         // with another tag).
         const int rt = A.adaptive_r ? A.max_radius : A.radius;
         if (N >= NB4_MIN_N) {
-            const int tsz = NB4 * PB - 2 * rt;
+            const int tsz = long_tile(rt);
             for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
                 merge_tile<NB4>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status, s_win, s_nn, s_wa, s_wb, s_pref);
         } else {
@@ -559,7 +562,7 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
             }
         }
         int em = m, ek = k;
-        const int2 tot = block_scan2(em, ek, s_wa, s_wb);
+        const int2 tot = block_scan2<PB>(em, ek, s_wa, s_wb);
         // new entries in registers, then compaction
         int nnode[TAIL_ITEMS];
         float nmn[TAIL_ITEMS][3], nmx[TAIL_ITEMS][3];
@@ -783,7 +786,7 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
     b += hp_carve::pad(nn);            // state
     b += 2 * hp_carve::pad(n * 4);     // cl0, cl1
     b += hp_carve::pad(((n + MIN_TILE4 - 1) / MIN_TILE4 + 1) * 8);
-    b += hp_carve::pad(((std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1) * 8);
+    b += hp_carve::pad(((std::min<int64_t>(n, NB4_MIN_N) + LPB / 2 - 1) / (LPB / 2) + 1) * 8);
     b += hp_carve::pad(MAX_ITER * 4 + 64);
     b += hp_carve::pad(n * 16) + hp_carve::pad(n * 4);  // records, flags
     return b;
@@ -818,7 +821,7 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     A.cl1 = cv.take<int>(n);
     const int64_t mtiles = (n + MIN_TILE4 - 1) / MIN_TILE4 + 1;
     A.status = cv.take<unsigned long long>(mtiles);
-    const int64_t ftiles = (std::min<int64_t>(n, NB4_MIN_N) + PB / 2 - 1) / (PB / 2) + 1;
+    const int64_t ftiles = (std::min<int64_t>(n, NB4_MIN_N) + LPB / 2 - 1) / (LPB / 2) + 1;
     A.status_f = cv.take<unsigned long long>(ftiles);
     unsigned* ctl = cv.take<unsigned>(MAX_ITER + 16);
     A.tickets = ctl;
@@ -839,11 +842,11 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
         const size_t smem = LOOP_SMEM;
         HP_CUDA(cudaFuncSetAttribute(k_ploc_loop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ploc_loop, PB, smem));
+        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ploc_loop, LPB, smem));
         if (per_sm < 1) return hp_fail(HP_ERR_UNSUPPORTED, "PLOC loop kernel does not fit on an SM");
         int grid = ctx->sm_count * per_sm;
         void* args[] = {&A};
-        HP_CUDA(cudaLaunchCooperativeKernel((void*)k_ploc_loop, grid, PB, args, smem, s));
+        HP_CUDA(cudaLaunchCooperativeKernel((void*)k_ploc_loop, grid, LPB, args, smem, s));
         hp_count_launch();
         hp_mark(ctx, s, "ploc_loop");
     }
