@@ -240,6 +240,21 @@ class Context:
                                      bits, _ptr(order), _stream_ptr(stream)))
         return results
 
+    RAY_KEY_METHODS = {"two_point": 0, "aila": 1, "paraboloid": 2, "octahedron": 3, "origin": 4, "costa": 5,
+                       "reis": 6}
+
+    def set_ray_keys(self, method="aila", ray_length=0.25):
+        """RayBuffer::setMortonCodeMethod / setRayLength for this context's ray keys and
+        sorted traces: a name of RAY_KEY_METHODS, a renderer env value (hp_ray_keys_method)
+        or a method number."""
+        if isinstance(method, str):
+            m = self.RAY_KEY_METHODS.get(method)
+            if m is None:
+                m = load().hp_ray_keys_method(method.encode())
+        else:
+            m = int(method)
+        check(load().hp_ctx_set_ray_keys(self.h, m, float(ray_length)))
+
     def ray_keys(self, rays, bits=30, box=None, stream=None):
         import torch
         keys = torch.empty(rays.shape[0], dtype=torch.int64, device=rays.device)

@@ -114,6 +114,8 @@ _SIGS = {
     "hp_camera_screen_to_world": (C.c_int, [_P, _P, C.c_float, C.c_int32, C.c_int32, C.c_float, C.c_float, _P]),
     "hp_gen_primary_rays": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_float, C.c_int32, _P, _P, _P]),
     "hp_ray_keys": (C.c_int, [_P, _P, C.c_int64, _P, C.c_int32, _P, _P]),
+    "hp_ctx_set_ray_keys": (C.c_int, [_P, C.c_int32, C.c_float]),
+    "hp_ray_keys_method": (C.c_int32, [C.c_char_p]),
     "hp_tune_default": (None, [C.POINTER(hp_tune)]),
     "hp_ctx_set_tune": (C.c_int, [_P, C.POINTER(hp_tune)]),
     "hp_ctx_get_tune": (C.c_int, [_P, C.POINTER(hp_tune)]),

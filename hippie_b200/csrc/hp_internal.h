@@ -63,6 +63,8 @@ struct hp_ctx {
     int num_marks = 0;
     int cap_marks = 0;
     hp_tune tune{512, 0, 16, 0, 0, 0, 0, 0.0f, 0.0f, {0}};  // launch choices (hp_ctx_set_tune)
+    int ray_key_method = HP_RAY_KEYS_AILA;  // hp_ctx_set_ray_keys
+    float ray_length = 0.25f;
     // hp_trace_host: copy streams, events and two device staging slots
     cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
     cudaEvent_t io_up[2] = {nullptr, nullptr}, io_traced[2] = {nullptr, nullptr}, io_free[2] = {nullptr, nullptr};

@@ -63,31 +63,178 @@ __global__ void __launch_bounds__(256) k_primary_rays(cam_args c, const int32_t*
 }
 
 struct key_args {
-    float mn[3], inv[3];  // ray box min and 1 / extent
+    float mn[3], mx[3], inv[3];  // ray box min, max and 1 / extent
+    float ray_length;            // RayBuffer::rayLength (two-point keys)
     int bits;
 };
 
-__device__ __forceinline__ int quant13(float a) { return __float2int_rz(__fmul_rn(a, 8191.0f)); }
+// Float to int by truncation, saturating as the GPU conversion does (NaN: 0).
+__device__ __forceinline__ int qz(float a, float scale) { return __float2int_rz(__fmul_rn(a, scale)); }
 
-__global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ rays, int64_t n, key_args k,
-                                                  uint64_t* __restrict__ keys) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 o = __ldg(rays + 2 * i), d = __ldg(rays + 2 * i + 1);
-    const int ax = quant13(__fmul_rn(__fsub_rn(o.x, k.mn[0]), k.inv[0]));
-    const int ay = quant13(__fmul_rn(__fsub_rn(o.y, k.mn[1]), k.inv[1]));
-    const int az = quant13(__fmul_rn(__fsub_rn(o.z, k.mn[2]), k.inv[2]));
-    const float len = __fsqrt_rn(__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x))));
-    const int bx = quant13(__fmul_rn(__fadd_rn(__fdiv_rn(d.x, len), 1.0f), 0.5f));
-    const int by = quant13(__fmul_rn(__fadd_rn(__fdiv_rn(d.y, len), 1.0f), 0.5f));
-    const int bz = quant13(__fmul_rn(__fadd_rn(__fdiv_rn(d.z, len), 1.0f), 0.5f));
+// Own atan2 and acos for the Costa and Reis keys (the reference calls the CUDA
+// math library under fast math): octant reduction and atan(t) ~ t * P(t^2) on
+// [0, 1], P of degree 8 fitted by iteratively reweighted least squares at
+// Chebyshev nodes (max error 1e-7 rad in float); every step IEEE-rounded.
+__device__ __forceinline__ float rk_atan01(float t) {
+    const float s = __fmul_rn(t, t);
+    float p = 0.0024567153304815292f;
+    p = __fmaf_rn(p, s, -0.014401324093341827f);
+    p = __fmaf_rn(p, s, 0.039781175553798676f);
+    p = __fmaf_rn(p, s, -0.07234854251146317f);
+    p = __fmaf_rn(p, s, 0.10498945415019989f);
+    p = __fmaf_rn(p, s, -0.14161229133605957f);
+    p = __fmaf_rn(p, s, 0.19985906779766083f);
+    p = __fmaf_rn(p, s, -0.33332598209381104f);
+    p = __fmaf_rn(p, s, 0.9999998807907104f);
+    return __fmul_rn(t, p);
+}
+__device__ __forceinline__ float rk_atan2(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float hi = fmaxf(ax, ay), lo = fminf(ax, ay);
+    if (!(hi > 0.0f)) return 0.0f;
+    float r = rk_atan01(__fdiv_rn(lo, hi));
+    if (ay > ax) r = __fsub_rn(1.5707963705062866f, r);
+    if (x < 0.0f) r = __fsub_rn(3.1415927410125732f, r);
+    return y < 0.0f ? -r : r;
+}
+__device__ __forceinline__ float rk_acos(float z) {
+    return rk_atan2(__fsqrt_rn(fmaxf(__fmaf_rn(-z, z, 1.0f), 0.0f)), z);
+}
+
+// Ray-box entry distance of the two-point keys (intersect, RayBufferKernels.cu:11-56).
+__device__ __forceinline__ float rk_intersect(float4 o, float4 d, const key_args& k) {
+    const float dd[3] = {d.x, d.y, d.z}, oo[3] = {o.x, o.y, o.z};
+    float t0[3], t1[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float lo = dd[a] >= 0.0f ? k.mn[a] : k.mx[a], hi = dd[a] >= 0.0f ? k.mx[a] : k.mn[a];
+        t0[a] = __fdiv_rn(__fsub_rn(lo, oo[a]), dd[a]);
+        t1[a] = __fdiv_rn(__fsub_rn(hi, oo[a]), dd[a]);
+    }
+    const float tmin = fmaxf(t0[2], fmaxf(t0[0], t0[1]));
+    const float tmax = fminf(t1[2], fminf(t1[0], t1[1]));
+    if (tmin > tmax) return -1.0f;
+    return __fmul_rn(1.0f - 1.0e-3f, tmin >= 0.0f ? tmin : tmax);
+}
+
+template <int M>
+__device__ __forceinline__ uint64_t ray_code(float4 o, float4 d, const key_args& k) {
+    const float a0 = __fmul_rn(__fsub_rn(o.x, k.mn[0]), k.inv[0]);
+    const float a1 = __fmul_rn(__fsub_rn(o.y, k.mn[1]), k.inv[1]);
+    const float a2 = __fmul_rn(__fsub_rn(o.z, k.mn[2]), k.inv[2]);
     uint64_t c = 0;
+    if (M == HP_RAY_KEYS_TWO_POINT) {  // computeMortonCodesTwoPoint64 (RayBufferKernels.cu:492-554)
+        float len = fminf(k.ray_length, fmaxf(d.w, 0.0f));
+        len = fminf(len, rk_intersect(o, d, k));
+        const float e0 = __fmaf_rn(len, d.x, o.x), e1 = __fmaf_rn(len, d.y, o.y), e2 = __fmaf_rn(len, d.z, o.z);
+        const int ia[3] = {qz(a0, 8191.0f), qz(a1, 8191.0f), qz(a2, 8191.0f)};
+        const int ib[3] = {qz(__fmul_rn(__fsub_rn(e0, k.mn[0]), k.inv[0]), 8191.0f),
+                           qz(__fmul_rn(__fsub_rn(e1, k.mn[1]), k.inv[1]), 8191.0f),
+                           qz(__fmul_rn(__fsub_rn(e2, k.mn[2]), k.inv[2]), 8191.0f)};
+#pragma unroll
+        for (int i = 12; i >= 2; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (6 * i - 9 - a);
+#pragma unroll
+        for (int i = 12; i >= 3; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ib[a] >> i) & 1) << (6 * i - 12 - a);
+        c |= (uint64_t)(ib[0] & 1);
+        return c;
+    }
+    if (M == HP_RAY_KEYS_ORIGIN) {  // computeMortonCodesOrigin64 (RayBufferKernels.cu:775-814)
+        const int ia[3] = {qz(a0, 8388607.0f), qz(a1, 8388607.0f), qz(a2, 8388607.0f)};
+#pragma unroll
+        for (int i = 22; i >= 2; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i - 3 - a);
+        c |= (uint64_t)(ia[0] & 1);
+        return c;
+    }
+    const float len = __fsqrt_rn(__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, __fmul_rn(d.x, d.x))));
+    const float nx = __fdiv_rn(d.x, len), ny = __fdiv_rn(d.y, len), nz = __fdiv_rn(d.z, len);
+    if (M == HP_RAY_KEYS_PARABOLOID || M == HP_RAY_KEYS_OCTAHEDRON) {
+        // computeMortonCodesParaboloid64 / Octahedron64 (RayBufferKernels.cu:616-773)
+        float bx, by;
+        if (M == HP_RAY_KEYS_PARABOLOID) {
+            if (nz < 0.0f) {
+                const float dd = __fadd_rn(-nz, 1.0f);
+                bx = __fadd_rn(__fdiv_rn(__fmul_rn(0.25f, nx), dd), 0.25f);
+                by = __fadd_rn(__fdiv_rn(__fmul_rn(0.5f, ny), dd), 0.5f);
+            } else {
+                const float dd = __fadd_rn(nz, 1.0f);
+                bx = __fadd_rn(__fdiv_rn(__fmul_rn(0.25f, nx), dd), 0.75f);
+                by = __fadd_rn(__fdiv_rn(__fmul_rn(0.5f, ny), dd), 0.5f);
+            }
+        } else {
+            const float ax = fabsf(nx), ay = fabsf(ny), az = fabsf(nz);
+            const float fact = __fdiv_rn(1.0f, __fadd_rn(__fadd_rn(ax, ay), az));
+            if (nz >= 0.0f) {
+                bx = __fmul_rn(nx, fact);
+                by = __fmul_rn(ny, fact);
+            } else {
+                bx = __fmul_rn(__fsub_rn(1.0f, __fmul_rn(ay, fact)), nx <= 0.0f ? -1.0f : 1.0f);
+                by = __fmul_rn(__fsub_rn(1.0f, __fmul_rn(ax, fact)), ny <= 0.0f ? -1.0f : 1.0f);
+            }
+            bx = __fmul_rn(__fadd_rn(bx, 1.0f), 0.5f);
+            by = __fmul_rn(__fadd_rn(by, 1.0f), 0.5f);
+        }
+        const int ia[3] = {qz(a0, 32767.0f), qz(a1, 32767.0f), qz(a2, 32767.0f)};
+        const int ib[2] = {qz(bx, 32767.0f), qz(by, 32767.0f)};
+#pragma unroll
+        for (int i = 14; i >= 11; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (63 - 3 * (14 - i) - a);
+#pragma unroll
+        for (int i = 10; i >= 0; --i) {
+            c |= (uint64_t)((ia[0] >> i) & 1) << (5 * i + 1);
+            c |= (uint64_t)((ia[1] >> i) & 1) << (5 * i);
+            if (i > 0) c |= (uint64_t)((ia[2] >> i) & 1) << (5 * i - 1);
+        }
+#pragma unroll
+        for (int i = 14; i >= 5; --i) {
+            c |= (uint64_t)((ib[0] >> i) & 1) << (5 * i - 22);
+            c |= (uint64_t)((ib[1] >> i) & 1) << (5 * i - 23);
+        }
+        return c;
+    }
+    if (M == HP_RAY_KEYS_COSTA || M == HP_RAY_KEYS_REIS) {
+        // computeMortonCodesCosta64 / Reis64 (RayBufferKernels.cu:816-921)
+        const float bx = __fadd_rn(__fdiv_rn(rk_atan2(ny, nx), 6.2831854820251465f), 0.5f);
+        const float by = __fdiv_rn(rk_acos(nz), 3.1415927410125732f);
+        if (M == HP_RAY_KEYS_COSTA) {
+            const int ia[3] = {qz(a0, 32767.0f), qz(a1, 32767.0f), qz(a2, 32767.0f)};
+            const int ib[2] = {qz(bx, 32767.0f), qz(by, 32767.0f)};
+#pragma unroll
+            for (int i = 14; i >= 11; --i) {
+                c |= (uint64_t)((ib[0] >> i) & 1) << (2 * i + 35);
+                c |= (uint64_t)((ib[1] >> i) & 1) << (2 * i + 34);
+            }
+#pragma unroll
+            for (int i = 14; i >= 0; --i)
+                for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i + 13 - a);
+        } else {
+            const int ia[3] = {qz(a0, 2097151.0f), qz(a1, 2097151.0f), qz(a2, 2097151.0f)};
+            const int ib[2] = {qz(bx, 2097151.0f), qz(by, 2097151.0f)};
+#pragma unroll
+            for (int i = 20; i >= 14; --i)
+                for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i + 3 - a);
+            c |= (uint64_t)((ia[0] >> 13) & 1) << 42;
+#pragma unroll
+            for (int i = 20; i >= 0; --i) {
+                c |= (uint64_t)((ib[0] >> i) & 1) << (2 * i + 1);
+                c |= (uint64_t)((ib[1] >> i) & 1) << (2 * i);
+            }
+        }
+        return c;
+    }
+    // computeMortonCodesAila64 (RayBufferKernels.cu:556-615)
+    const int ax = qz(a0, 8191.0f), ay = qz(a1, 8191.0f), az = qz(a2, 8191.0f);
+    const int bx = qz(__fmul_rn(__fadd_rn(nx, 1.0f), 0.5f), 8191.0f);
+    const int by = qz(__fmul_rn(__fadd_rn(ny, 1.0f), 0.5f), 8191.0f);
+    const int bz = qz(__fmul_rn(__fadd_rn(nz, 1.0f), 0.5f), 8191.0f);
 #pragma unroll
     for (int b = 12; b >= 10; --b) {
-        const int s = 63 - 3 * (12 - b);
-        c |= (uint64_t)((ax >> b) & 1) << s;
-        c |= (uint64_t)((ay >> b) & 1) << (s - 1);
-        c |= (uint64_t)((az >> b) & 1) << (s - 2);
+        const int sh = 63 - 3 * (12 - b);
+        c |= (uint64_t)((ax >> b) & 1) << sh;
+        c |= (uint64_t)((ay >> b) & 1) << (sh - 1);
+        c |= (uint64_t)((az >> b) & 1) << (sh - 2);
     }
 #pragma unroll
     for (int b = 9; b >= 1; --b) {
@@ -101,7 +248,16 @@ __global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ ray
         c |= (uint64_t)((by >> b) & 1) << (6 * b - 22);
         c |= (uint64_t)((bz >> b) & 1) << (6 * b - 23);
     }
-    keys[i] = c >> (64 - k.bits);
+    return c;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ rays, int64_t n, key_args k,
+                                                  uint64_t* __restrict__ keys) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t c = ray_code<M>(__ldg(rays + 2 * i), __ldg(rays + 2 * i + 1), k);
+    keys[i] = k.bits == 64 ? c : c >> (64 - k.bits);
 }
 
 // halton (RayGenKernels.cu:20-30): radical inverse of i in the given base.
@@ -262,16 +418,52 @@ extern "C" hp_status hp_ray_keys(hp_ctx* ctx, const float* rays, int64_t num_ray
     const float* b = ray_box6 ? ray_box6 : def;
     for (int a = 0; a < 3; ++a) {
         k.mn[a] = b[a];
+        k.mx[a] = b[3 + a];
         const float ext = b[3 + a] - b[a];
         k.inv[a] = ext > 0.0f ? 1.0f / ext : 0.0f;
     }
     k.bits = bits;
+    k.ray_length = ctx->ray_length;
     if (num_rays == 0) return HP_OK;
-    k_ray_keys<<<hp_div_up(num_rays, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<const float4*>(rays), num_rays, k, keys);
+    const unsigned grid = (unsigned)hp_div_up(num_rays, 256);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const float4* r4 = reinterpret_cast<const float4*>(rays);
+    switch (ctx->ray_key_method) {
+        case HP_RAY_KEYS_TWO_POINT: k_ray_keys<HP_RAY_KEYS_TWO_POINT><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        case HP_RAY_KEYS_PARABOLOID: k_ray_keys<HP_RAY_KEYS_PARABOLOID><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        case HP_RAY_KEYS_OCTAHEDRON: k_ray_keys<HP_RAY_KEYS_OCTAHEDRON><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        case HP_RAY_KEYS_ORIGIN: k_ray_keys<HP_RAY_KEYS_ORIGIN><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        case HP_RAY_KEYS_COSTA: k_ray_keys<HP_RAY_KEYS_COSTA><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        case HP_RAY_KEYS_REIS: k_ray_keys<HP_RAY_KEYS_REIS><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+        default: k_ray_keys<HP_RAY_KEYS_AILA><<<grid, 256, 0, s>>>(r4, num_rays, k, keys); break;
+    }
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     return HP_OK;
+}
+
+// RayBuffer::setMortonCodeMethod / setRayLength (rt/ray/RayBuffer.cpp:167-195).
+extern "C" hp_status hp_ctx_set_ray_keys(hp_ctx* ctx, int32_t method, float ray_length) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_set_ray_keys: null context");
+    if (method < HP_RAY_KEYS_TWO_POINT || method > HP_RAY_KEYS_REIS)
+        return hp_fail(HP_ERR_ARG, "hp_ctx_set_ray_keys: unknown method");
+    if (!(ray_length >= 0.0f)) return hp_fail(HP_ERR_ARG, "hp_ctx_set_ray_keys: ray length must be >= 0");
+    ctx->ray_key_method = method;
+    ctx->ray_length = ray_length;
+    return HP_OK;
+}
+
+// Renderer::stringToMortonCodeMethod (rt/renderer/Renderer.cpp:37-52): the
+// Reis method is spelled "reise"; any other string selects the two-point method.
+extern "C" int32_t hp_ray_keys_method(const char* name) {
+    if (!name) return HP_RAY_KEYS_TWO_POINT;
+    if (!std::strcmp(name, "aila")) return HP_RAY_KEYS_AILA;
+    if (!std::strcmp(name, "paraboloid")) return HP_RAY_KEYS_PARABOLOID;
+    if (!std::strcmp(name, "octahedron")) return HP_RAY_KEYS_OCTAHEDRON;
+    if (!std::strcmp(name, "origin")) return HP_RAY_KEYS_ORIGIN;
+    if (!std::strcmp(name, "costa")) return HP_RAY_KEYS_COSTA;
+    if (!std::strcmp(name, "reise")) return HP_RAY_KEYS_REIS;
+    return HP_RAY_KEYS_TWO_POINT;
 }
 
 extern "C" hp_status hp_trace_sorted(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays,

@@ -308,10 +308,30 @@ hp_status hp_camera_screen_to_world(const float* position, const float* directio
 hp_status hp_gen_primary_rays(hp_ctx* ctx, const float* position, const float* screen_to_world16,
                               int32_t width, int32_t height, float max_dist, int32_t sample_index,
                               const int32_t* index_to_pixel, float* rays, void* stream);
-/* Ray Morton keys (computeMortonCodesAila64, rt/ray/RayBufferKernels.cu:556-615):
- * origin normalised to ray_box6 (host {min xyz, max xyz}; NULL = [0,1]^3 as
- * the reference), direction mapped to [0,1]^3, 13 bits per axis, interleaved;
- * the top `bits` of the 64-bit code. keys: device, num_rays uint64. */
+/* Ray Morton key methods (RayBuffer::MortonCodeMethod, rt/ray/RayBuffer.h:20-28;
+ * the 64-bit kernels computeMortonCodes*64, rt/ray/RayBufferKernels.cu:492-921,
+ * which RayBuffer::computeMortonCodes always uses, RayBuffer.cpp:31-80). */
+typedef enum hp_ray_keys_method_e {
+    HP_RAY_KEYS_TWO_POINT = 0,   /* origin and a point rayLength along the ray, 13 bits per axis */
+    HP_RAY_KEYS_AILA = 1,        /* origin and direction, 13 bits per axis (the default) */
+    HP_RAY_KEYS_PARABOLOID = 2,  /* origin 15 bits, direction by dual-paraboloid map */
+    HP_RAY_KEYS_OCTAHEDRON = 3,  /* origin 15 bits, direction by octahedral map */
+    HP_RAY_KEYS_ORIGIN = 4,      /* origin only, 23 bits per axis */
+    HP_RAY_KEYS_COSTA = 5,       /* spherical direction (atan2, acos) first, then origin */
+    HP_RAY_KEYS_REIS = 6         /* origin 21 bits, then spherical direction */
+} hp_ray_keys_method_e;
+/* The context's key method and two-point ray length (RayBuffer::
+ * setMortonCodeMethod / setRayLength; defaults Aila and 0.25), used by
+ * hp_ray_keys, hp_trace_sorted and a context tuned for sorted tracing. */
+hp_status hp_ctx_set_ray_keys(hp_ctx* ctx, int32_t method, float ray_length);
+/* Renderer::stringToMortonCodeMethod (rt/renderer/Renderer.cpp:37-52): "aila",
+ * "paraboloid", "octahedron", "origin", "costa", "reise"; anything else is the
+ * two-point method. */
+int32_t hp_ray_keys_method(const char* name);
+/* Ray Morton keys by the context's method: the origin normalised to ray_box6
+ * (host {min xyz, max xyz}; NULL = [0,1]^3 as the reference), the direction
+ * mapped by the method, quantised and interleaved as the reference's 64-bit
+ * kernel; the top `bits` of the 64-bit code. keys: device, num_rays uint64. */
 hp_status hp_ray_keys(hp_ctx* ctx, const float* rays, int64_t num_rays, const float* ray_box6,
                       int32_t bits, uint64_t* keys, void* stream);
 

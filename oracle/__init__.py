@@ -37,6 +37,7 @@ _SIGS = {
     "or_pixel_table": (C.c_int32, [C.c_int32, C.c_int32, _P]),
     "or_primary_rays": (None, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P, _P]),
     "or_ray_keys": (None, [_P, C.c_int64, _P, C.c_int32, _P]),
+    "or_ray_keys_method": (None, [_P, C.c_int64, _P, C.c_int32, C.c_int32, C.c_float, _P]),
     "or_build_hlbvh": (C.c_int64, [_P, _P, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int, _P,
                                    _P, _P, _P, _P, _P, _P]),
     "or_tr": (C.c_int, [C.c_int, C.c_int, C.c_float, C.c_float, _P, _P, _P, _P, _P]),
@@ -250,10 +251,16 @@ def primary_rays(origin, m, width, height, sample_index=0, max_dist=np.inf, inde
     return rays
 
 
-def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1)):
+RAY_KEY_METHODS = {"two_point": 0, "aila": 1, "paraboloid": 2, "octahedron": 3, "origin": 4, "costa": 5, "reis": 6}
+
+
+def ray_keys(rays, bits=30, box=(0, 0, 0, 1, 1, 1), method="aila", ray_length=0.25):
+    """Ray Morton keys of RayBuffer::computeMortonCodes (the 64-bit kernels) by method."""
     keys = np.empty(rays.shape[0], np.uint64)
     b = np.ascontiguousarray(box, np.float32)
-    load().or_ray_keys(_p(np.ascontiguousarray(rays)), rays.shape[0], _p(b), bits, _p(keys))
+    m = RAY_KEY_METHODS[method] if isinstance(method, str) else int(method)
+    load().or_ray_keys_method(_p(np.ascontiguousarray(rays, np.float32)), rays.shape[0], _p(b), bits, m,
+                              float(ray_length), _p(keys))
     return keys
 
 

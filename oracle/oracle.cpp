@@ -1810,46 +1810,182 @@ void or_primary_rays(const float* origin, const float* m, int32_t width, int32_t
     }
 }
 
-// computeMortonCodesAila64 (rt/ray/RayBufferKernels.cu:556-615), IEEE-rounded.
-void or_ray_keys(const float* rays, int64_t n, const float* box6, int32_t bits, uint64_t* keys) {
-    float mn[3], inv[3];
+// ---- ray Morton keys: the 64-bit kernels computeMortonCodes*64 of
+// rt/ray/RayBufferKernels.cu:492-921 (method order of RayBuffer::
+// MortonCodeMethod, rt/ray/RayBuffer.h:20-28), every step IEEE-rounded; the
+// origin is normalised by the box's inverse extent; Costa and Reis use the
+// library's own atan2 / acos (an odd polynomial of degree 17 for atan on
+// [0, 1], coefficients fitted by reweighted least squares at Chebyshev nodes).
+namespace {
+
+inline int sat_trunc(float v) {  // float -> int by truncation, saturating, NaN -> 0 (as cvt.rzi on the GPU)
+    if (!(v == v)) return 0;
+    if (v >= 2147483648.0f) return 2147483647;
+    if (v <= -2147483648.0f) return (int)0x80000000u;
+    return (int)std::trunc(v);
+}
+inline int qz(float a, float scale) { return sat_trunc(a * scale); }
+
+inline float rk_atan01(float t) {
+    const float s = t * t;
+    float p = 0.0024567153304815292f;
+    p = std::fmaf(p, s, -0.014401324093341827f);
+    p = std::fmaf(p, s, 0.039781175553798676f);
+    p = std::fmaf(p, s, -0.07234854251146317f);
+    p = std::fmaf(p, s, 0.10498945415019989f);
+    p = std::fmaf(p, s, -0.14161229133605957f);
+    p = std::fmaf(p, s, 0.19985906779766083f);
+    p = std::fmaf(p, s, -0.33332598209381104f);
+    p = std::fmaf(p, s, 0.9999998807907104f);
+    return t * p;
+}
+inline float rk_atan2(float y, float x) {
+    const float ax = std::fabs(x), ay = std::fabs(y);
+    const float hi = std::fmax(ax, ay), lo = std::fmin(ax, ay);
+    if (!(hi > 0.0f)) return 0.0f;
+    float r = rk_atan01(lo / hi);
+    if (ay > ax) r = 1.5707963705062866f - r;
+    if (x < 0.0f) r = 3.1415927410125732f - r;
+    return y < 0.0f ? -r : r;
+}
+inline float rk_acos(float z) { return rk_atan2(std::sqrt(std::fmax(std::fmaf(-z, z, 1.0f), 0.0f)), z); }
+
+uint64_t ray_code(const float* r, int method, const float* mn, const float* mx, const float* inv, float ray_length) {
+    const float a0 = (r[0] - mn[0]) * inv[0], a1 = (r[1] - mn[1]) * inv[1], a2 = (r[2] - mn[2]) * inv[2];
+    uint64_t c = 0;
+    if (method == 0) {  // two point (RayBufferKernels.cu:492-554; intersect :11-56)
+        float t0[3], t1[3];
+        for (int a = 0; a < 3; ++a) {
+            const float lo = r[4 + a] >= 0.0f ? mn[a] : mx[a], hi = r[4 + a] >= 0.0f ? mx[a] : mn[a];
+            t0[a] = (lo - r[a]) / r[4 + a];
+            t1[a] = (hi - r[a]) / r[4 + a];
+        }
+        const float tmin = std::fmax(t0[2], std::fmax(t0[0], t0[1]));
+        const float tmax = std::fmin(t1[2], std::fmin(t1[0], t1[1]));
+        const float hit = tmin > tmax ? -1.0f : (1.0f - 1.0e-3f) * (tmin >= 0.0f ? tmin : tmax);
+        float len = std::fmin(ray_length, std::fmax(r[7], 0.0f));
+        len = std::fmin(len, hit);
+        int ia[3], ib[3];
+        const float aa[3] = {a0, a1, a2};
+        for (int a = 0; a < 3; ++a) {
+            ia[a] = qz(aa[a], 8191.0f);
+            ib[a] = qz((std::fmaf(len, r[4 + a], r[a]) - mn[a]) * inv[a], 8191.0f);
+        }
+        for (int i = 12; i >= 2; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (6 * i - 9 - a);
+        for (int i = 12; i >= 3; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ib[a] >> i) & 1) << (6 * i - 12 - a);
+        c |= (uint64_t)(ib[0] & 1);
+        return c;
+    }
+    if (method == 4) {  // origin (RayBufferKernels.cu:775-814)
+        const int ia[3] = {qz(a0, 8388607.0f), qz(a1, 8388607.0f), qz(a2, 8388607.0f)};
+        for (int i = 22; i >= 2; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i - 3 - a);
+        c |= (uint64_t)(ia[0] & 1);
+        return c;
+    }
+    const float len = std::sqrt(std::fmaf(r[6], r[6], std::fmaf(r[5], r[5], r[4] * r[4])));
+    const float nx = r[4] / len, ny = r[5] / len, nz = r[6] / len;
+    if (method == 2 || method == 3) {  // paraboloid / octahedron (RayBufferKernels.cu:616-773)
+        float bx, by;
+        if (method == 2) {
+            if (nz < 0.0f) {
+                const float dd = -nz + 1.0f;
+                bx = (0.25f * nx) / dd + 0.25f;
+                by = (0.5f * ny) / dd + 0.5f;
+            } else {
+                const float dd = nz + 1.0f;
+                bx = (0.25f * nx) / dd + 0.75f;
+                by = (0.5f * ny) / dd + 0.5f;
+            }
+        } else {
+            const float ax = std::fabs(nx), ay = std::fabs(ny), az = std::fabs(nz);
+            const float fact = 1.0f / ((ax + ay) + az);
+            if (nz >= 0.0f) {
+                bx = nx * fact;
+                by = ny * fact;
+            } else {
+                bx = (1.0f - ay * fact) * (nx <= 0.0f ? -1.0f : 1.0f);
+                by = (1.0f - ax * fact) * (ny <= 0.0f ? -1.0f : 1.0f);
+            }
+            bx = (bx + 1.0f) * 0.5f;
+            by = (by + 1.0f) * 0.5f;
+        }
+        const int ia[3] = {qz(a0, 32767.0f), qz(a1, 32767.0f), qz(a2, 32767.0f)};
+        const int ib[2] = {qz(bx, 32767.0f), qz(by, 32767.0f)};
+        for (int i = 14; i >= 11; --i)
+            for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (63 - 3 * (14 - i) - a);
+        for (int i = 10; i >= 0; --i) {
+            c |= (uint64_t)((ia[0] >> i) & 1) << (5 * i + 1);
+            c |= (uint64_t)((ia[1] >> i) & 1) << (5 * i);
+            if (i > 0) c |= (uint64_t)((ia[2] >> i) & 1) << (5 * i - 1);
+        }
+        for (int i = 14; i >= 5; --i) {
+            c |= (uint64_t)((ib[0] >> i) & 1) << (5 * i - 22);
+            c |= (uint64_t)((ib[1] >> i) & 1) << (5 * i - 23);
+        }
+        return c;
+    }
+    if (method == 5 || method == 6) {  // Costa / Reis (RayBufferKernels.cu:816-921)
+        const float bx = rk_atan2(ny, nx) / 6.2831854820251465f + 0.5f;
+        const float by = rk_acos(nz) / 3.1415927410125732f;
+        if (method == 5) {
+            const int ia[3] = {qz(a0, 32767.0f), qz(a1, 32767.0f), qz(a2, 32767.0f)};
+            const int ib[2] = {qz(bx, 32767.0f), qz(by, 32767.0f)};
+            for (int i = 14; i >= 11; --i) {
+                c |= (uint64_t)((ib[0] >> i) & 1) << (2 * i + 35);
+                c |= (uint64_t)((ib[1] >> i) & 1) << (2 * i + 34);
+            }
+            for (int i = 14; i >= 0; --i)
+                for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i + 13 - a);
+        } else {
+            const int ia[3] = {qz(a0, 2097151.0f), qz(a1, 2097151.0f), qz(a2, 2097151.0f)};
+            const int ib[2] = {qz(bx, 2097151.0f), qz(by, 2097151.0f)};
+            for (int i = 20; i >= 14; --i)
+                for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> i) & 1) << (3 * i + 3 - a);
+            c |= (uint64_t)((ia[0] >> 13) & 1) << 42;
+            for (int i = 20; i >= 0; --i) {
+                c |= (uint64_t)((ib[0] >> i) & 1) << (2 * i + 1);
+                c |= (uint64_t)((ib[1] >> i) & 1) << (2 * i);
+            }
+        }
+        return c;
+    }
+    // Aila (RayBufferKernels.cu:556-615)
+    const int ia[3] = {qz(a0, 8191.0f), qz(a1, 8191.0f), qz(a2, 8191.0f)};
+    const int ib[3] = {qz((nx + 1.0f) * 0.5f, 8191.0f), qz((ny + 1.0f) * 0.5f, 8191.0f),
+                       qz((nz + 1.0f) * 0.5f, 8191.0f)};
+    for (int b = 12; b >= 10; --b)
+        for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> b) & 1) << (63 - 3 * (12 - b) - a);
+    for (int b = 9; b >= 1; --b)
+        for (int a = 0; a < 3; ++a) c |= (uint64_t)((ia[a] >> b) & 1) << (6 * b - a);
+    for (int b = 12; b >= 4; --b)
+        for (int a = 0; a < 3; ++a) c |= (uint64_t)((ib[a] >> b) & 1) << (6 * b - 21 - a);
+    return c;
+}
+
+}  // namespace
+
+void or_ray_keys_method(const float* rays, int64_t n, const float* box6, int32_t bits, int32_t method,
+                        float ray_length, uint64_t* keys) {
+    float mn[3], mx[3], inv[3];
     for (int a = 0; a < 3; ++a) {
         mn[a] = box6[a];
+        mx[a] = box6[3 + a];
         const float ext = box6[3 + a] - box6[a];
         inv[a] = ext > 0.0f ? 1.0f / ext : 0.0f;
     }
-    auto q = [](float a) { return (int)std::trunc(a * 8191.0f); };
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
-        const float* r = rays + 8 * i;
-        int ia[3], ib[3];
-        const float len = std::sqrt(std::fmaf(r[6], r[6], std::fmaf(r[5], r[5], r[4] * r[4])));
-        for (int a = 0; a < 3; ++a) {
-            ia[a] = q((r[a] - mn[a]) * inv[a]);
-            ib[a] = q((r[4 + a] / len + 1.0f) * 0.5f);
-        }
-        uint64_t c = 0;
-        c |= (uint64_t)((ia[0] >> 12) & 1) << 63;
-        c |= (uint64_t)((ia[1] >> 12) & 1) << 62;
-        c |= (uint64_t)((ia[2] >> 12) & 1) << 61;
-        c |= (uint64_t)((ia[0] >> 11) & 1) << 60;
-        c |= (uint64_t)((ia[1] >> 11) & 1) << 59;
-        c |= (uint64_t)((ia[2] >> 11) & 1) << 58;
-        c |= (uint64_t)((ia[0] >> 10) & 1) << 57;
-        c |= (uint64_t)((ia[1] >> 10) & 1) << 56;
-        c |= (uint64_t)((ia[2] >> 10) & 1) << 55;
-        for (int b = 9; b >= 1; --b) {
-            c |= (uint64_t)((ia[0] >> b) & 1) << (6 * b + 0);
-            c |= (uint64_t)((ia[1] >> b) & 1) << (6 * b - 1);
-            c |= (uint64_t)((ia[2] >> b) & 1) << (6 * b - 2);
-        }
-        for (int b = 12; b >= 4; --b) {
-            c |= (uint64_t)((ib[0] >> b) & 1) << (6 * b - 21);
-            c |= (uint64_t)((ib[1] >> b) & 1) << (6 * b - 22);
-            c |= (uint64_t)((ib[2] >> b) & 1) << (6 * b - 23);
-        }
-        keys[i] = c >> (64 - bits);
+        const uint64_t c = ray_code(rays + 8 * i, method, mn, mx, inv, ray_length);
+        keys[i] = bits == 64 ? c : c >> (64 - bits);
     }
+}
+
+// The default method (Aila).
+void or_ray_keys(const float* rays, int64_t n, const float* box6, int32_t bits, uint64_t* keys) {
+    or_ray_keys_method(rays, n, box6, bits, 1, 0.25f, keys);
 }
 
 // ---- A12: HipBVH::getCost (rt/bvh/HipBVH.cpp:346-370, HipBVHKernels.cu:184-238) ----------
