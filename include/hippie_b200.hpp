@@ -208,6 +208,24 @@ public:
     float traceSort(const float* rays, int64_t n, int32_t* results, void* stream = nullptr) {
         return run(rays, n, results, nullptr, 0u, true, stream);
     }
+    /* A RayBuffer in host memory: rays and results on the host (pinned for
+     * overlap), uploaded, traced and downloaded in overlapping chunks. */
+    float traceHost(const float* rays_host, int64_t n, int32_t* results_host, bool anyHit = false,
+                    void* stream = nullptr) {
+        if (!bvh_) throw Error(HP_ERR_ARG, "Tracer: no BVH set");
+        return ctx_.timed(
+            [&] {
+                check(hp_trace_host(ctx_.get(), bvh_->get(), rays_host, n, results_host, nullptr,
+                                    anyHit ? HP_TRACE_ANY_HIT : 0u, 0, stream),
+                      "hp_trace_host");
+            },
+            stream);
+    }
+    /* RayBuffer::setMortonCodeMethod / setRayLength for traceSort, by the
+     * renderer's method names ("aila", "paraboloid", ..., "reise"). */
+    void setMortonCodeMethod(const char* name, float rayLength = 0.25f) {
+        check(hp_ctx_set_ray_keys(ctx_.get(), hp_ray_keys_method(name), rayLength), "hp_ctx_set_ray_keys");
+    }
 
 private:
     float run(const float* rays, int64_t n, int32_t* results, int32_t* stats, uint32_t flags, bool sorted,

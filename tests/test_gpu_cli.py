@@ -41,7 +41,7 @@ Renderer {{
 """
 
 
-@pytest.mark.parametrize("method", ["lbvh", "ploc"])
+@pytest.mark.parametrize("method", ["lbvh", "ploc", "atr", "tr", "hlbvh"])
 def test_cli_matches_python(ctx, tmp_path, method):
     v, t = hp.gen.uniform_mesh(5, 3000)
     obj = tmp_path / "m.obj"
