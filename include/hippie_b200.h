@@ -49,7 +49,7 @@ typedef enum hp_status {
     HP_ERR_OOM = 3,           /* device or host allocation failed */
     HP_ERR_TIMEOUT = 4,       /* a host-side wait exceeded its limit */
     HP_ERR_DEVICE_STATUS = 5, /* a kernel reported an error word (bounded spin gave up, bad index) */
-    HP_ERR_UNSUPPORTED = 6,   /* option not supported by this build */
+    HP_ERR_UNSUPPORTED = 6,   /* option not supported by the library */
     HP_ERR_PARSE = 7          /* environment file could not be parsed */
 } hp_status;
 

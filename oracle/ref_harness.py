@@ -1,7 +1,7 @@
 """ctypes access to oracle/_ref/libhipref.so: the reference's own CUDA kernels
 driven by a restatement of its host sequences (test infrastructure only).
 
-Built from /root/reference by oracle/ref/Makefile where the reference is
+Built from the reference sources by oracle/ref/Makefile where they are
 present; the library then travels with the repository. Tests skip when it is
 absent.
 """

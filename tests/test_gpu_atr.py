@@ -93,7 +93,7 @@ def test_atr_from_env(ctx):
     np.testing.assert_array_equal(bvh.download()[0], ref["nodes"])
 
 
-@pytest.mark.skipif(not R.available(), reason="reference harness not built (needs /root/reference)")
+@pytest.mark.skipif(not R.available(), reason="reference harness not built (needs the reference sources)")
 @pytest.mark.parametrize("kind,n,bits,treelet", [("uniform", 65536, 30, 9), ("clustered", 131072, 60, 9),
                                                  ("mixed", 100000, 60, 20)])
 def test_atr_matches_reference_kernels(ctx, kind, n, bits, treelet):

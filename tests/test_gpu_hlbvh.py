@@ -133,7 +133,7 @@ def test_hlbvh_wide_layouts(ctx, layout):
     assert bvh.validate(dev(v), dev(t))
 
 
-@pytest.mark.skipif(not R.available(), reason="reference harness not built (needs /root/reference)")
+@pytest.mark.skipif(not R.available(), reason="reference harness not built (needs the reference sources)")
 @pytest.mark.parametrize("kind,n,bits,sah", [("uniform", 65536, 60, 15), ("clustered", 131072, 60, 15),
                                              ("mixed", 100000, 60, 9), ("uniform", 30000, 30, 12),
                                              ("clustered", 5000, 60, 6), ("singleton", 401, 60, 15)])

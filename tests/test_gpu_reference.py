@@ -17,7 +17,7 @@ import oracle
 from oracle import ref_harness as R
 
 pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not R.available(), reason="reference harness not built (needs /root/reference)")]
+              pytest.mark.skipif(not R.available(), reason="reference harness not built (needs the reference sources)")]
 
 
 def dev(a):
