@@ -474,6 +474,7 @@ __global__ void __launch_bounds__(LPB, 2) k_ploc_loop(ploc_args A) {
     int* s_nn = reinterpret_cast<int*>(s_win + 6 * WIN);
     __shared__ int s_wa[LPB / 32 + 1], s_wb[LPB / 32 + 1];
     __shared__ unsigned s_pref[2];
+    __shared__ unsigned s_ticket;
     __shared__ int s_n;
     for (int it = 0; it < MAX_ITER; ++it) {
         if (threadIdx.x == 0) s_n = *((volatile int*)A.g);
@@ -485,17 +486,24 @@ __global__ void __launch_bounds__(LPB, 2) k_ploc_loop(ploc_args A) {
         int* cl_out = (it & 1) ? A.cl0 : A.cl1;
         // Tiles of ITEMS*LPB - 2r clusters, so that a tile and its halo take ITEMS
         // clusters per thread; every CTA takes its tiles in increasing order (all
-        // CTAs are resident), so each look-back waits only on lower tiles that
-        // are in progress.
+        // CTAs are resident; tickets are handed out in order), so each look-back
+        // waits only on lower tiles that are in progress.
         // Tile sizes use the largest radius of the build, so that the tile
         // count of an iteration never exceeds the previous one's (the look-back
         // words of lower tiles are then always this iteration's or older ones
         // with another tag).
         const int rt = A.adaptive_r ? A.max_radius : A.radius;
         if (N >= NB4_MIN_N) {
+            // long tiles (~25 us each) go to whichever CTA is free, in ticket order
             const int tsz = long_tile(rt);
-            for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
+            while (true) {
+                if (threadIdx.x == 0) s_ticket = atomicAdd(A.tickets + it, 1u);
+                __syncthreads();
+                const unsigned tile = s_ticket;
+                __syncthreads();
+                if ((long)tile * tsz >= N) break;
                 merge_tile<NB4>(A, cl_in, cl_out, N, r, it, tile, tsz, A.status, s_win, s_nn, s_wa, s_wb, s_pref);
+            }
         } else {
             const int tsz = fused_tile(rt);
             for (unsigned tile = blockIdx.x; (long)tile * tsz < N; tile += gridDim.x)
