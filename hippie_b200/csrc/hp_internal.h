@@ -169,9 +169,10 @@ hp_status hp_lbvh_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
                         hp_bvh_impl* out, const hp_build_taps* taps, cudaStream_t stream);
 // PLOC clustering and depth-first collapse after the references are sorted.
 size_t hp_ploc_scratch_bytes(int64_t n);
+// woop_src (or null): Woop rows per scene triangle, gathered by the collapse.
 hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax,
-                        void* scratch, void* wide_scratch, cudaStream_t stream);
+                        void* scratch, void* wide_scratch, cudaStream_t stream, const float4* woop_src = nullptr);
 // Depth-first collapse of a binary tree (interior nodes 0..n-2, leaves n-1..2n-2,
 // sorted reference p at leaf n-1+p) into 64-byte nodes, the triangle order and
 // Woop triangles. nbmax.w holds each node's size; counts the surviving interior

@@ -40,10 +40,13 @@ constexpr int TB = 256;
 
 // Per-triangle boxes (setupBoxes) and the scene box as their union
 // (SceneLoader.cpp:144-153 computes it over triangle boxes at load time).
+// woop (or null): the Woop rows of every triangle, in scene order, computed
+// here from the vertices the boxes read anyway (the collapse then gathers one
+// 48-byte record per reference instead of the triangle and its vertices).
 __global__ void __launch_bounds__(TB) k_tri_boxes(const float* __restrict__ verts, int64_t nv,
                                                   const int32_t* __restrict__ tris, int64_t n,
                                                   float4* __restrict__ bmin, float4* __restrict__ bmax,
-                                                  uint32_t* box_ord, int* err) {
+                                                  uint32_t* box_ord, int* err, float4* __restrict__ woop = nullptr) {
     float mn[3] = {HP_MAX_FLOAT, HP_MAX_FLOAT, HP_MAX_FLOAT};
     float mx[3] = {-HP_MAX_FLOAT, -HP_MAX_FLOAT, -HP_MAX_FLOAT};
     for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TB) {
@@ -54,6 +57,13 @@ __global__ void __launch_bounds__(TB) k_tri_boxes(const float* __restrict__ vert
               bz = fmaxf(fmaxf(t.z0, t.z1), t.z2);
         bmin[i] = make_float4(ax, ay, az, 0.0f);
         bmax[i] = make_float4(bx, by, bz, 0.0f);
+        if (woop) {
+            float4 w0, w1, w2;
+            hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
+            woop[3 * i] = w0;
+            woop[3 * i + 1] = w1;
+            woop[3 * i + 2] = w2;
+        }
         mn[0] = fminf(mn[0], ax); mn[1] = fminf(mn[1], ay); mn[2] = fminf(mn[2], az);
         mx[0] = fmaxf(mx[0], bx); mx[1] = fmaxf(mx[1], by); mx[2] = fmaxf(mx[2], bz);
     }
@@ -407,6 +417,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     need += hp_carve::pad(hp_sort_hist_bytes(plan.passes));
     if (ploc) {
         need += hp_carve::pad(n * 4) + hp_ploc_scratch_bytes(n);  // sorted references, clustering
+        if (!wide) need += hp_carve::pad(n * 48);                 // Woop rows in scene order
     } else if (atr) {
         need += hp_carve::pad(n * 4);                                                     // sorted references
         need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
@@ -434,9 +445,10 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     if (ploc) {
         int32_t* sorted_refs = cv.take<int32_t>(n);
         void* ploc_scratch = cv.take<char>(hp_ploc_scratch_bytes(n));
+        float4* woop_src = wide ? nullptr : cv.take<float4>(3 * n);
         k_init_build<<<hp_div_up(plan.passes * 256, TB), TB, 0, s>>>(info, hist, plan.passes * 256);
         k_tri_boxes<<<grid_red, TB, 0, s>>>(m->vertices, m->num_vertices, m->triangles, n, tbmin, tbmax,
-                                            info->box_ord, err);
+                                            info->box_ord, err, woop_src);
         hp_count_launch(2);
         hp_mark(ctx, s, "boxes");
         k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
@@ -445,7 +457,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
         hp_mark(ctx, s, "morton");
         hp_sort_args sa{keys, nullptr, skeys, sorted_refs, sort_scratch, hist, true, err, ctx};
         HP_TRY(hp_sort_run(plan, sa, s));
-        HP_TRY(hp_ploc_stage(ctx, m, p, out, sorted_refs, tbmin, tbmax, ploc_scratch, wide_scratch, s));
+        HP_TRY(hp_ploc_stage(ctx, m, p, out, sorted_refs, tbmin, tbmax, ploc_scratch, wide_scratch, s, woop_src));
         if (taps) {
             if (taps->morton_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(keys, taps->morton_keys, n);
             if (taps->sorted_keys) k_tap_keys<K><<<grid_n, TB, 0, s>>>(skeys, taps->sorted_keys, n);

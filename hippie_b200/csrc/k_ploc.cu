@@ -628,6 +628,7 @@ struct td_args {
     int epoch;
     unsigned* ticket;
     const int32_t* sorted_tri;
+    const float4* woop_src;  // Woop rows per scene triangle, or null: computed from the vertices
     const float* verts;
     int64_t nv;
     const int32_t* tris;
@@ -725,6 +726,16 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
         }
         const int tri = T.sorted_tri[v - (n - 1)];
         T.tri_idx[toff] = tri;
+        if (T.woop_src) {
+            if ((unsigned)tri >= (unsigned)n) {
+                hp_report(T.err, HP_DEV_BAD_INDEX, tri);
+                return;
+            }
+            T.woop[3 * (int64_t)toff] = __ldg(T.woop_src + 3 * (int64_t)tri);
+            T.woop[3 * (int64_t)toff + 1] = __ldg(T.woop_src + 3 * (int64_t)tri + 1);
+            T.woop[3 * (int64_t)toff + 2] = __ldg(T.woop_src + 3 * (int64_t)tri + 2);
+            return;
+        }
         float p[9];
         for (int k = 0; k < 3; ++k) {
             int vi = T.tris[3 * (int64_t)tri + k];
@@ -802,7 +813,7 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
 
 hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh_impl* out,
                         const int32_t* sorted_tri, const float4* tbmin, const float4* tbmax, void* scratch,
-                        void* wide_scratch, cudaStream_t s) {
+                        void* wide_scratch, cudaStream_t s, const float4* woop_src) {
     const int n = (int)m->num_triangles;
     const int64_t nn = 2 * (int64_t)n - 1;
     const int r_max = p->ploc_adaptive ? p->ploc_max_radius : p->ploc_radius;
@@ -896,6 +907,7 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     T.epoch = 1;
     T.ticket = ctl + MAX_ITER + 8;
     T.sorted_tri = sorted_tri;
+    T.woop_src = woop_src;
     T.verts = m->vertices;
     T.nv = m->num_vertices;
     T.tris = m->triangles;
