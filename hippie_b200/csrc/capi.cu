@@ -238,6 +238,9 @@ hp_status hp_ctx_destroy(hp_ctx* ctx) {
     }
     if (ctx->io_h2d) cudaStreamDestroy(ctx->io_h2d);
     if (ctx->io_d2h) cudaStreamDestroy(ctx->io_d2h);
+    for (int i = 0; i < 2; ++i)
+        if (ctx->io_trace[i]) cudaStreamDestroy(ctx->io_trace[i]);
+    if (ctx->io_start) cudaEventDestroy(ctx->io_start);
     delete ctx;
     return HP_OK;
 }
@@ -419,22 +422,35 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     if (num_rays < 0 || chunk_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_host: negative count");
     if (num_rays == 0) return HP_OK;
     if (!rays_host || !results_host) return hp_fail(HP_ERR_ARG, "hp_trace_host: null ray or result buffer");
-    const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 22), num_rays);
+    const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 21), num_rays);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    // slot layout: rays (32 B per ray), results (16 B), stats (8 B)
+    // A context tuned for sorted tracing sorts each chunk by 30-bit ray keys, as
+    // hp_trace does for a batch of that size.
+    const int sort_bits = 30;
+    const bool sorted = ctx->tune.trace_sorted && C >= 65536 && C < (int64_t(1) << 30);
+    const hp_sort_plan plan = hp_sort_make_plan(std::max<int64_t>(C, 1), 8, sort_bits, ctx->tune.sort_block);
+    // slot layout: rays (32 B per ray), results (16 B), stats (8 B), then, when
+    // sorting, keys, sorted keys, order and the sort's scratch and histograms
     const size_t ray_b = hp_carve::pad((size_t)C * 32), res_b = hp_carve::pad((size_t)C * 16);
-    const size_t need = ray_b + res_b + hp_carve::pad((size_t)C * 8);
+    const size_t st_b = hp_carve::pad((size_t)C * 8);
+    const size_t sort_b = sorted ? 2 * hp_carve::pad((size_t)C * 8) + hp_carve::pad((size_t)C * 4) +
+                                       hp_carve::pad(plan.scratch_bytes) +
+                                       hp_carve::pad(hp_sort_hist_bytes(plan.passes))
+                                 : 0;
+    const size_t need = ray_b + res_b + st_b + sort_b;
     if (!ctx->io_h2d) {
         HP_CUDA(cudaStreamCreateWithFlags(&ctx->io_h2d, cudaStreamNonBlocking));
         HP_CUDA(cudaStreamCreateWithFlags(&ctx->io_d2h, cudaStreamNonBlocking));
+        HP_CUDA(cudaEventCreateWithFlags(&ctx->io_start, cudaEventDisableTiming));
         for (int i = 0; i < 2; ++i) {
+            HP_CUDA(cudaStreamCreateWithFlags(&ctx->io_trace[i], cudaStreamNonBlocking));
             HP_CUDA(cudaEventCreateWithFlags(&ctx->io_up[i], cudaEventDisableTiming));
             HP_CUDA(cudaEventCreateWithFlags(&ctx->io_traced[i], cudaEventDisableTiming));
             HP_CUDA(cudaEventCreateWithFlags(&ctx->io_free[i], cudaEventDisableTiming));
         }
     }
     if (ctx->io_slot_bytes < need) {
-        // earlier calls may still use the slots
+        // earlier calls may still use the slots (their traces end before their downloads)
         HP_CUDA(cudaStreamSynchronize(ctx->io_d2h));
         for (int i = 0; i < 2; ++i) {
             HP_CUDA(cudaFree(ctx->io_slot[i]));
@@ -444,22 +460,46 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
         for (int i = 0; i < 2; ++i) HP_CUDA(cudaMalloc(&ctx->io_slot[i], need));
         ctx->io_slot_bytes = need;
     }
+    // Work queued on the caller's stream (the build of this BVH) comes first.
+    HP_CUDA(cudaEventRecord(ctx->io_start, s));
+    for (int k = 0; k < 2; ++k) HP_CUDA(cudaStreamWaitEvent(ctx->io_trace[k], ctx->io_start, 0));
+    const hp_bvh_impl* bi = reinterpret_cast<const hp_bvh_impl*>(bvh->impl);
     const int64_t chunks = (num_rays + C - 1) / C;
     for (int64_t i = 0; i < chunks; ++i) {
+        // Chunks alternate between two slots, each traced on a stream of its own,
+        // so that a chunk's trace starts on the SMs that the previous chunk's
+        // trace leaves idle as it drains.
         const int k = (int)(i & 1);
         const int64_t off = i * C, m = std::min(C, num_rays - off);
-        float* d_rays = reinterpret_cast<float*>(ctx->io_slot[k]);
-        int32_t* d_res = reinterpret_cast<int32_t*>(ctx->io_slot[k] + ray_b);
-        int32_t* d_stats = stats_host ? reinterpret_cast<int32_t*>(ctx->io_slot[k] + ray_b + res_b) : nullptr;
+        cudaStream_t t = ctx->io_trace[k];
+        hp_carve cv(ctx->io_slot[k]);
+        float* d_rays = cv.take<float>((size_t)C * 8);
+        int32_t* d_res = cv.take<int32_t>((size_t)C * 4);
+        int32_t* d_stats = cv.take<int32_t>((size_t)C * 2);
+        if (!stats_host) d_stats = nullptr;
+        unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 20 + 2 * k);
         // up: once the slot's previous results are home
         HP_CUDA(cudaStreamWaitEvent(ctx->io_h2d, ctx->io_free[k], 0));
         HP_CUDA(cudaMemcpyAsync(d_rays, rays_host + 8 * off, (size_t)m * 32, cudaMemcpyHostToDevice, ctx->io_h2d));
         HP_CUDA(cudaEventRecord(ctx->io_up[k], ctx->io_h2d));
-        // trace on the caller's stream
-        HP_CUDA(cudaStreamWaitEvent(s, ctx->io_up[k], 0));
-        HP_CUDA(cudaMemsetAsync(d_res, 0, (size_t)m * 16, s));
-        HP_TRY(hp_trace(ctx, bvh, d_rays, m, d_res, d_stats, flags, stream));
-        HP_CUDA(cudaEventRecord(ctx->io_traced[k], s));
+        // trace
+        HP_CUDA(cudaStreamWaitEvent(t, ctx->io_up[k], 0));
+        HP_CUDA(cudaMemsetAsync(d_res, 0, (size_t)m * 16, t));
+        const int32_t* order = nullptr;
+        if (sorted && m >= 65536) {
+            uint64_t* keys = cv.take<uint64_t>((size_t)C);
+            uint64_t* skeys = cv.take<uint64_t>((size_t)C);
+            int32_t* ord = cv.take<int32_t>((size_t)C);
+            void* scratch = cv.take<char>(plan.scratch_bytes);
+            uint32_t* hist = cv.take<uint32_t>((size_t)plan.passes * 256);
+            const hp_sort_plan pm = hp_sort_make_plan(m, 8, sort_bits, ctx->tune.sort_block);
+            HP_TRY(hp_ray_keys(ctx, d_rays, m, nullptr, sort_bits, keys, t));
+            hp_sort_args sa{keys, nullptr, skeys, ord, scratch, hist, false, ctx->d_status, nullptr};
+            HP_TRY(hp_sort_run(pm, sa, t));
+            order = ord;
+        }
+        HP_TRY(hp_trace_launch(ctx, bi, bvh->num_refs, d_rays, m, d_res, d_stats, flags, t, order, counter));
+        HP_CUDA(cudaEventRecord(ctx->io_traced[k], t));
         // down
         HP_CUDA(cudaStreamWaitEvent(ctx->io_d2h, ctx->io_traced[k], 0));
         HP_CUDA(cudaMemcpyAsync(results_host + 4 * off, d_res, (size_t)m * 16, cudaMemcpyDeviceToHost, ctx->io_d2h));

@@ -65,8 +65,10 @@ struct hp_ctx {
     hp_tune tune{512, 0, 16, 0, 0, 0, 0, 0.0f, 0.0f, {0}};  // launch choices (hp_ctx_set_tune)
     int ray_key_method = HP_RAY_KEYS_AILA;  // hp_ctx_set_ray_keys
     float ray_length = 0.25f;
-    // hp_trace_host: copy streams, events and two device staging slots
-    cudaStream_t io_h2d = nullptr, io_d2h = nullptr;
+    // hp_trace_host: copy streams, one trace stream per staging slot, events
+    // and two device staging slots
+    cudaStream_t io_h2d = nullptr, io_d2h = nullptr, io_trace[2] = {nullptr, nullptr};
+    cudaEvent_t io_start = nullptr;
     cudaEvent_t io_up[2] = {nullptr, nullptr}, io_traced[2] = {nullptr, nullptr}, io_free[2] = {nullptr, nullptr};
     char* io_slot[2] = {nullptr, nullptr};
     size_t io_slot_bytes = 0;
@@ -239,10 +241,13 @@ struct hp_batch_trace_args {
 hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint32_t flags, cudaStream_t stream);
 
 // ---- trace / adjoint ---------------------------------------------------------------
-// order (or null): slot k of the launch traces ray order[k].
+// order (or null): slot k of the launch traces ray order[k]. counter (or null
+// for the context's own): the launch's 8-byte work counter; launches that may
+// run at the same time need counters of their own.
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                           int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
-                          cudaStream_t stream, const int32_t* order = nullptr);
+                          cudaStream_t stream, const int32_t* order = nullptr,
+                          unsigned long long* counter = nullptr);
 hp_status hp_adjoint_launch(hp_ctx* ctx, const hp_mesh* m, const float* rays,
                             const int32_t* results, const float* dl_dtuv, int64_t num_rays,
                             float* dl_dvertices, cudaStream_t stream);

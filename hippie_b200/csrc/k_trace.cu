@@ -355,7 +355,7 @@ hp_status hp_trace_batch_launch(hp_ctx* ctx, const hp_batch_trace_args& t, uint3
 
 hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
                           int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
-                          cudaStream_t s, const int32_t* order) {
+                          cudaStream_t s, const int32_t* order, unsigned long long* counter) {
     if (num_rays <= 0) return HP_OK;
     if (n_refs <= 0) {
         k_trace_empty<<<hp_div_up(num_rays, 256), 256, 0, s>>>(
@@ -365,7 +365,7 @@ hp_status hp_trace_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, con
         hp_count_launch();
         return HP_OK;
     }
-    unsigned long long* counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
+    if (!counter) counter = reinterpret_cast<unsigned long long*>(ctx->d_status + 16);
     HP_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     hp_mark(ctx, s, "trace_begin");
     if (b->layout != 2)

@@ -76,3 +76,27 @@ def test_zero_rays_and_bad_arguments(ctx, scene):
     import ctypes as C
     st = load().hp_trace_host(ctx.h, C.byref(bvh.c), None, 5, None, None, 0, 0, None)
     assert st == 2
+
+
+@pytest.mark.parametrize("layout", [4, 8])
+def test_wide_layouts_and_sorted_stats(ctx, scene, layout):
+    """Chunks traced on two streams at once keep their own work counters and,
+    when sorting, their own key and sort scratch, for every layout."""
+    _, rays = scene
+    v, t = hp.gen.clustered_mesh(21, 60000, clusters=64)
+    bvh = ctx.build(torch.from_numpy(v).cuda(), torch.from_numpy(t).cuda(),
+                    hp.BuildParams(method="ploc", morton_bits=60, ploc_radius=16, ploc_max_radius=16, layout=layout))
+    bvh.sync()
+    want, _ = device_trace(ctx, bvh, rays)
+    Rh = torch.from_numpy(rays).pin_memory()
+    np.testing.assert_array_equal(ctx.trace_host(bvh, Rh, chunk=65536).numpy(), want)
+    st = torch.zeros((rays.shape[0], 2), dtype=torch.int32).pin_memory()
+    ctx.set_tune(trace_sorted=1)
+    try:
+        got = ctx.trace_host(bvh, Rh, stats=st, chunk=100000).numpy()
+    finally:
+        ctx.reset_tune()
+    np.testing.assert_array_equal(got, want)
+    hit = want[:, 0] >= 0
+    assert (st.numpy()[~hit] == 0).all() and (st.numpy()[hit] > 0).all()
+    ctx.check()
