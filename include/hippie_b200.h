@@ -269,9 +269,13 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
  * in host memory, which the reference's Buffer migrates to the device on use,
  * gpu/Buffer.cpp:437-498): rays_host, results_host and stats_host (or NULL)
  * are host memory, pinned for overlap. The rays go up in chunks of
- * chunk_rays (0: 4,194,304) on a copy stream while the previous chunk is
- * traced on `stream` and the one before comes back on another copy stream,
- * through two device staging slots the context keeps. Results are identical
+ * chunk_rays (0: 2,097,152) on a copy stream while the previous chunk is
+ * traced and the one before comes back on another copy stream, through two
+ * device staging slots the context keeps; each slot's chunks trace on a
+ * stream of their own (after the work already queued on `stream`), so that
+ * one chunk's trace fills the SMs that its predecessor's leaves as it drains.
+ * A context tuned for sorted tracing sorts each chunk of at least 65,536 rays
+ * by 30-bit ray keys, in scratch of its slot. Results are identical
  * to hp_trace's, except that every result record is written in full (a miss
  * reads {-1, tmax bits, 0, 0}). The call is asynchronous on `stream`: the
  * host buffers may be read / are complete once `stream` has synchronised. */
