@@ -422,7 +422,7 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     if (num_rays < 0 || chunk_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_host: negative count");
     if (num_rays == 0) return HP_OK;
     if (!rays_host || !results_host) return hp_fail(HP_ERR_ARG, "hp_trace_host: null ray or result buffer");
-    const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 21), num_rays);
+    const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 22), num_rays);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     // A context tuned for sorted tracing sorts each chunk by 30-bit ray keys, as
     // hp_trace does for a batch of that size.
@@ -464,13 +464,32 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     HP_CUDA(cudaEventRecord(ctx->io_start, s));
     for (int k = 0; k < 2; ++k) HP_CUDA(cudaStreamWaitEvent(ctx->io_trace[k], ctx->io_start, 0));
     const hp_bvh_impl* bi = reinterpret_cast<const hp_bvh_impl*>(bvh->impl);
-    const int64_t chunks = (num_rays + C - 1) / C;
-    for (int64_t i = 0; i < chunks; ++i) {
+    // Chunk sizes: chunk_rays each, or by default doubling from 262,144 rays up
+    // to 4,194,304 and halving again at the end, so that the first upload and
+    // the last download, which nothing overlaps, stay short.
+    std::vector<int64_t> sizes;
+    if (chunk_rays > 0) {
+        for (int64_t off = 0; off < num_rays; off += C) sizes.push_back(std::min(C, num_rays - off));
+    } else {
+        const int64_t lo = std::min<int64_t>(C, 262144);
+        int64_t left = num_rays;
+        std::vector<int64_t> tail;
+        for (int64_t a = lo; a < C && left > 4 * a; a *= 2) {
+            sizes.push_back(a);
+            tail.push_back(a);
+            left -= 2 * a;
+        }
+        const int64_t mid = (left + C - 1) / C;
+        for (int64_t j = 0; j < mid; ++j) sizes.push_back(left / mid + (j < left % mid ? 1 : 0));
+        sizes.insert(sizes.end(), tail.rbegin(), tail.rend());
+    }
+    int64_t off = 0;
+    for (size_t i = 0; i < sizes.size(); off += sizes[i], ++i) {
         // Chunks alternate between two slots, each traced on a stream of its own,
         // so that a chunk's trace starts on the SMs that the previous chunk's
         // trace leaves idle as it drains.
         const int k = (int)(i & 1);
-        const int64_t off = i * C, m = std::min(C, num_rays - off);
+        const int64_t m = sizes[i];
         cudaStream_t t = ctx->io_trace[k];
         hp_carve cv(ctx->io_slot[k]);
         float* d_rays = cv.take<float>((size_t)C * 8);

@@ -269,7 +269,9 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
  * in host memory, which the reference's Buffer migrates to the device on use,
  * gpu/Buffer.cpp:437-498): rays_host, results_host and stats_host (or NULL)
  * are host memory, pinned for overlap. The rays go up in chunks of
- * chunk_rays (0: 2,097,152) on a copy stream while the previous chunk is
+ * chunk_rays (0: sizes doubling from 262,144 rays to at most 4,194,304 and
+ * halving again at the end, so that the first upload and the last download,
+ * which nothing overlaps, stay short) on a copy stream while the previous chunk is
  * traced and the one before comes back on another copy stream, through two
  * device staging slots the context keeps; each slot's chunks trace on a
  * stream of their own (after the work already queued on `stream`), so that

@@ -100,3 +100,20 @@ def test_wide_layouts_and_sorted_stats(ctx, scene, layout):
     hit = want[:, 0] >= 0
     assert (st.numpy()[~hit] == 0).all() and (st.numpy()[hit] > 0).all()
     ctx.check()
+
+
+def test_default_chunk_schedule(ctx, scene):
+    """With no chunk size given, chunks double from 262,144 rays and halve
+    again at the end (here 262,144 + 1,048,576 + 262,144 rays)."""
+    bvh, _ = scene
+    v, _t = hp.gen.clustered_mesh(21, 60000, clusters=64)
+    rays = hp.gen.rays_sphere(29, 1572864, np.concatenate([v.min(0), v.max(0)]))
+    want, _ = device_trace(ctx, bvh, rays)
+    Rh = torch.from_numpy(rays).pin_memory()
+    np.testing.assert_array_equal(ctx.trace_host(bvh, Rh).numpy(), want)
+    ctx.set_tune(trace_sorted=1)
+    try:
+        np.testing.assert_array_equal(ctx.trace_host(bvh, Rh).numpy(), want)
+    finally:
+        ctx.reset_tune()
+    ctx.check()
