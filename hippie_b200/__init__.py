@@ -314,6 +314,15 @@ class Context:
                                       rays.shape[0], _ptr(dl_dverts), _stream_ptr(stream)))
         return dl_dverts
 
+    def set_arithmetic(self, mode: str = "ieee"):
+        """"ieee" (default) or "reference": the reciprocals of the reference's
+        fast-math build in Woop rows and in the binary tracer (hp_ctx_set_arithmetic)."""
+        check(load().hp_ctx_set_arithmetic(self.h, {"ieee": 0, "reference": 1}[mode]))
+
+    def set_sort_spin_limit(self, spins: int = 0):
+        """Spins of one radix-sort look-back wait before it gives up (0: the default)."""
+        check(load().hp_ctx_set_sort_spin_limit(self.h, int(spins)))
+
     def radix_sort(self, keys, vals=None, bits=None, stream=None):
         import torch
         kb = keys.element_size()

@@ -3,7 +3,8 @@
 Every CUDA source is compiled with
     nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -fmad=false
 (-fmad=false: the kernels spell out each fused multiply-add they want, so
-that a CPU restatement can reproduce their results bit for bit) and the host
+that a CPU restatement can reproduce their results bit for bit; k_refarith.cu
+is compiled with -use_fast_math, see FILE_FLAGS) and the host
 sources with g++ -ffp-contract=off. Objects go to hippie_b200/_build/, the
 shared library to hippie_b200/libhippie_b200.so. Rebuilds are incremental
 (by modification time of sources and headers).
@@ -33,6 +34,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-fopenmp",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE)] + ARCH
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-I", str(INCLUDE)]
+# k_refarith.cu holds the reference-arithmetic kernels, compiled with the
+# reference's own -use_fast_math (approximate quotient, denormals flushed,
+# compiler contraction; the flag comes after -fmad=false and overrides it).
+FILE_FLAGS = {"k_refarith.cu": ["-use_fast_math", "-fmad=true"]}
 
 
 def _nvcc() -> str:
@@ -62,7 +67,7 @@ def _compile(src: Path, force: bool, hdr_mtime: float) -> Path:
         if obj.stat().st_mtime >= max(src.stat().st_mtime, hdr_mtime):
             return obj
     if src.suffix == ".cu":
-        cmd = [_nvcc()] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)]
+        cmd = [_nvcc()] + NVCC_FLAGS + FILE_FLAGS.get(src.name, []) + ["-c", str(src), "-o", str(obj)]
     else:
         cmd = ["g++"] + CXX_FLAGS + ["-I", _cuda_include(), "-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)

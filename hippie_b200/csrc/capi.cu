@@ -308,7 +308,9 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
         return HP_OK;
     }
     hp_mark(ctx, s, "begin");
-    return hp_lbvh_build(ctx, m, p, b, taps, s);
+    HP_TRY(hp_lbvh_build(ctx, m, p, b, taps, s));
+    if (ctx->arith == HP_ARITH_REFERENCE) HP_TRY(hp_woop_ref_launch(ctx, b, n, m, s));
+    return HP_OK;
 }
 
 hp_status hp_bvh_sync(hp_ctx* ctx, hp_bvh* bvh, void* stream) {
@@ -399,8 +401,11 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
         return hp_fail(HP_ERR_UNSUPPORTED, "hp_refit: a BVH of a batch is rebuilt with hp_batch_build");
     if (reinterpret_cast<hp_bvh_impl*>(bvh->impl)->layout != HP_LAYOUT_BIN)
         return hp_fail(HP_ERR_UNSUPPORTED, "hp_refit: only the binary layout is refitted in place (rebuild wide BVHs)");
-    return hp_refit_launch(ctx, reinterpret_cast<hp_bvh_impl*>(bvh->impl), bvh->num_refs, m,
-                           reinterpret_cast<cudaStream_t>(stream));
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(bvh->impl);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_TRY(hp_refit_launch(ctx, b, bvh->num_refs, m, s));
+    if (ctx->arith == HP_ARITH_REFERENCE) HP_TRY(hp_woop_ref_launch(ctx, b, bvh->num_refs, m, s));
+    return HP_OK;
 }
 
 hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t num_rays, int32_t* results,
@@ -560,6 +565,20 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
     uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
     hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false, ctx->d_status, ctx};
     return hp_sort_run(plan, a, s);
+}
+
+hp_status hp_ctx_set_arithmetic(hp_ctx* ctx, int32_t mode) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_set_arithmetic: null context");
+    if (mode != HP_ARITH_IEEE && mode != HP_ARITH_REFERENCE)
+        return hp_fail(HP_ERR_ARG, "hp_ctx_set_arithmetic: mode must be HP_ARITH_IEEE or HP_ARITH_REFERENCE");
+    ctx->arith = mode;
+    return HP_OK;
+}
+
+hp_status hp_ctx_set_sort_spin_limit(hp_ctx* ctx, uint32_t spins) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_set_sort_spin_limit: null context");
+    ctx->sort_spin_limit = spins ? spins : HP_SORT_SPIN_LIMIT_DEFAULT;
+    return HP_OK;
 }
 
 }  // extern "C"

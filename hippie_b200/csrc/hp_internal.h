@@ -65,6 +65,10 @@ struct hp_ctx {
     hp_tune tune{512, 0, 16, 0, 0, 0, 0, 0.0f, 0.0f, {0}};  // launch choices (hp_ctx_set_tune)
     int ray_key_method = HP_RAY_KEYS_AILA;  // hp_ctx_set_ray_keys
     float ray_length = 0.25f;
+    // Spins of one look-back wait of the radix sort before it gives up and
+    // reports HP_DEV_SPIN_LIMIT (hp_ctx_set_sort_spin_limit).
+    uint32_t sort_spin_limit = HP_SORT_SPIN_LIMIT_DEFAULT;
+    int arith = HP_ARITH_IEEE;  // hp_ctx_set_arithmetic
     // hp_trace_host: copy streams, one trace stream per staging slot, events
     // and two device staging slots
     cudaStream_t io_h2d = nullptr, io_d2h = nullptr, io_trace[2] = {nullptr, nullptr};
@@ -80,6 +84,14 @@ void hp_mark(hp_ctx* ctx, cudaStream_t s, const char* name);
 void hp_count_launch(int k = 1);
 
 hp_status hp_ctx_reserve(hp_ctx* ctx, size_t bytes, cudaStream_t stream);
+
+// Reference arithmetic (k_refarith.cu): Woop rows of every reference of a
+// built BVH rewritten with the fast-math reciprocal, and the binary tracer
+// with the fast-math reciprocals (same arguments as hp_trace_launch).
+hp_status hp_woop_ref_launch(hp_ctx* ctx, hp_bvh_impl* b, int64_t n_refs, const hp_mesh* m, cudaStream_t s);
+hp_status hp_trace_ref_launch(hp_ctx* ctx, const hp_bvh_impl* b, int64_t n_refs, const float* rays,
+                              int64_t num_rays, int32_t* results, int32_t* stats, uint32_t flags,
+                              unsigned long long* counter, const int32_t* order, cudaStream_t s);
 
 // Bump allocator over the context arena (256-byte aligned pieces).
 struct hp_carve {

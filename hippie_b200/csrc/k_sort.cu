@@ -27,7 +27,7 @@ namespace {
 constexpr uint32_t ST_FLAG_A = 1u << 30;   // tile aggregate available
 constexpr uint32_t ST_FLAG_P = 2u << 30;   // inclusive prefix available
 constexpr uint32_t ST_MASK = (1u << 30) - 1u;
-constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 22;
+constexpr uint32_t LOOKBACK_SPIN_LIMIT = HP_SORT_SPIN_LIMIT_DEFAULT;
 
 __device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
     uint32_t v;
@@ -100,7 +100,8 @@ __device__ __forceinline__ void scan256x2(uint32_t a, uint32_t b, uint32_t& ea, 
 // counts over all earlier tiles, walking back over LB status words per round
 // until a tile whose inclusive prefix is published. Every wait is bounded.
 template <int LB>
-__device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t tile, int tid, int* err) {
+__device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t tile, int tid, int* err,
+                                             uint32_t spin_limit) {
     uint32_t prefix = 0, spins = 0;
     int64_t t = (int64_t)tile - 1;
     bool done = tile == 0;
@@ -115,7 +116,7 @@ __device__ __forceinline__ uint32_t lookback(const uint32_t* status, uint32_t ti
             if (t - k < 0) { done = true; break; }
             uint32_t s = sw[k];
             while ((s & ~ST_MASK) == 0u) {
-                if (++spins > LOOKBACK_SPIN_LIMIT) {
+                if (++spins > spin_limit) {
                     hp_report(err, HP_DEV_SPIN_LIMIT, (int)tile);
                     s = ST_FLAG_P;
                     break;
@@ -146,7 +147,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     const K* __restrict__ keys_in, const int32_t* __restrict__ vals_in,
     K* __restrict__ keys_out, int32_t* __restrict__ vals_out, int64_t n, int shift,
     uint32_t dmask, const uint32_t* __restrict__ hist, uint32_t* status,
-    uint32_t* tile_counter, int* err) {
+    uint32_t* tile_counter, int* err, uint32_t spin_limit) {
     constexpr int NW = BLOCK / 32;
     constexpr int TILE = BLOCK * ITEMS;
     static_assert(BLOCK >= 256, "one thread per digit");
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
     scan256x2(total, hval, block_start, hist_excl, s_w);
     if (tid < 256) {
         s_block_start[tid] = block_start;
-        const uint32_t prefix = lookback<LB>(status, tile, tid, err);
+        const uint32_t prefix = lookback<LB>(status, tile, tid, err, spin_limit);
         if (tile > 0) st_relaxed_u32(&status[(size_t)tile * 256 + tid], ST_FLAG_P | (prefix + total));
         s_global[tid] = hist_excl + prefix - block_start;
     }
@@ -248,12 +249,20 @@ __global__ void __launch_bounds__(BLOCK) k_onesweep(
         }
     }
     __syncthreads();
+    // Output positions are in range whenever every look-back completed. After
+    // a wait gave up (reported above), this pass's prefixes are too small and
+    // the next pass reads keys whose digit counts no longer match the
+    // histograms, so positions are checked before every store.
     const int count = (int)min((int64_t)TILE, n - base);
     for (int j = tid; j < count; j += BLOCK) {
         K k = skeys[j];
         uint32_t g = s_global[digit_of(k, shift, dmask)] + (uint32_t)j;
-        keys_out[g] = k;
-        vals_out[g] = svals[j];
+        if ((int64_t)g < n) {
+            keys_out[g] = k;
+            vals_out[g] = svals[j];
+        } else {
+            hp_report(err, HP_DEV_BAD_INDEX, (int)tile);
+        }
     }
 }
 
@@ -314,7 +323,8 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
         int w = std::min(8, plan.bits - shift);
         k_onesweep<K, BLOCK, ITEMS><<<(unsigned)plan.tiles, BLOCK, smem, stream>>>(
             kin, vin, kout, vout, n, shift, (1u << w) - 1u, a.hist + 256 * p,
-            status + (size_t)p * plan.tiles * 256, counters + p, a.status);
+            status + (size_t)p * plan.tiles * 256, counters + p, a.status,
+            a.ctx ? a.ctx->sort_spin_limit : LOOKBACK_SPIN_LIMIT);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(a.ctx, stream, "sort_pass");
@@ -533,6 +543,10 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_base[NOALLOC_MAX_DEVICES] = {};
 
+// The sort's kernels report into a (code, info) pair inside the fixed array;
+// the caller's status is one int32 and receives only the code.
+__global__ void k_noalloc_status_out(const int* own, int32_t* out) { *out = own[0]; }
+
 }  // namespace
 
 extern "C" hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* vals_in, void* keys_out,
@@ -546,7 +560,11 @@ extern "C" hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* v
         return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: n = " + std::to_string(n) +
                                        " exceeds the fixed scratch capacity of " +
                                        std::to_string(HP_NOALLOC_SORT_MAX_KEYS) + " keys");
-    if (n == 0) return HP_OK;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        if (device_status) HP_CUDA(cudaMemsetAsync(device_status, 0, sizeof(int32_t), s));
+        return HP_OK;
+    }
     if (!keys_in || !keys_out || !vals_out) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: null buffer");
     int dev = 0;
     HP_CUDA(cudaGetDevice(&dev));
@@ -568,7 +586,15 @@ extern "C" hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* v
     uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
     int* own_status = cv.take<int>(64);
     if (cv.off > NOALLOC_BYTES) return hp_fail(HP_ERR_ARG, "hp_radix_sort_noalloc: scratch plan exceeds the fixed array");
-    hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false,
-                   device_status ? reinterpret_cast<int*>(device_status) : own_status, nullptr};
-    return hp_sort_run(plan, a, reinterpret_cast<cudaStream_t>(stream));
+    // The array keeps the previous call's contents: the status pair starts at
+    // zero every call (the sort clears its own look-back words and histograms).
+    HP_CUDA(cudaMemsetAsync(own_status, 0, 2 * sizeof(int), s));
+    hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false, own_status, nullptr};
+    HP_TRY(hp_sort_run(plan, a, s));
+    if (device_status) {
+        k_noalloc_status_out<<<1, 1, 0, s>>>(own_status, device_status);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+    }
+    return HP_OK;
 }

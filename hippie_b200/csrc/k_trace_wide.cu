@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(TB) k_trace_wide(const float4* __restrict__ ra
                             if (STATS) ++n_tris;
                             const float4 v0 = __ldg(woop + 3 * (int64_t)tri);
                             const float ozz = __fmaf_rn(-oz, v0.z, __fmaf_rn(-oy, v0.y, __fmaf_rn(-ox, v0.x, v0.w)));
-                            const float den = __fmaf_rn(dz, v0.z, __fmaf_rn(dy, v0.y, __fmul_rn(dx, v0.x)));
+                            const float den = __fmaf_rn(dz, v0.z, __fmaf_rn(dx, v0.x, __fmul_rn(dy, v0.y)));
                             const float t = __fmul_rn(ozz, __frcp_rn(den));
                             if (!(t > tmin) || t > bt) continue;
                             int id = INT_MAX;
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(TB) k_trace_wide(const float4* __restrict__ ra
                             if (!(u >= 0.0f)) continue;
                             const float4 v2 = __ldg(woop + 3 * (int64_t)tri + 2);
                             const float oyy = __fmaf_rn(oz, v2.z, __fmaf_rn(oy, v2.y, __fmaf_rn(ox, v2.x, v2.w)));
-                            const float dyy = __fmaf_rn(dz, v2.z, __fmaf_rn(dy, v2.y, __fmul_rn(dx, v2.x)));
+                            const float dyy = __fmaf_rn(dz, v2.z, __fmaf_rn(dx, v2.x, __fmul_rn(dy, v2.y)));
                             const float v = __fmaf_rn(t, dyy, oyy);
                             if (!(v >= 0.0f) || !(__fadd_rn(u, v) <= 1.0f)) continue;
                             bt = t; bu = u; bv = v; bh = tri;

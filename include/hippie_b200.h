@@ -412,6 +412,24 @@ hp_status hp_batch_build_trace(hp_ctx* ctx, hp_batch* b, const float* rays, int3
  * cost / validate / hp_trace); hp_bvh_free on it releases nothing. */
 hp_status hp_batch_bvh(hp_batch* b, int32_t mesh, hp_bvh* out);
 
+/* ---- arithmetic ---------------------------------------------------------- */
+/* The reference compiles its kernels with -use_fast_math
+ * (gpu/HipCompiler.cpp:127-129): its `1.0f / x` in the tracer's ray setup and
+ * triangle test (rt/tracer/HipTracerBinKernels.cu:87-89, 219-220) and in the
+ * Woop inverse (rcp, util/Math.h:20,368; rt/bvh/HipBVHKernels.cu:12-33) is the
+ * approximate quotient, and denormals are flushed to zero. By default this
+ * library computes those reciprocals with IEEE round-to-nearest
+ * (HP_ARITH_IEEE). HP_ARITH_REFERENCE computes them as the reference's build
+ * does, with denormals flushed, so that Woop rows and closest hits match the
+ * reference's bit for bit (ties in t still go to the lower triangle id). It
+ * applies to hp_build and hp_refit (the Woop rows of every layout) and to the
+ * binary-layout tracer (hp_trace, hp_trace_sorted, hp_trace_host); batches
+ * and the Quad / Oct tracer keep IEEE arithmetic. Builds are otherwise
+ * unchanged (the Morton scale always uses the reference's quotient). */
+#define HP_ARITH_IEEE 0
+#define HP_ARITH_REFERENCE 1
+hp_status hp_ctx_set_arithmetic(hp_ctx* ctx, int32_t mode);
+
 /* ---- primitives ------------------------------------------------------------ */
 /* Stable LSD radix sort of (key, value) pairs by key bits [0, bits). key_bytes
  * is 4 or 8. vals_in may be NULL (values are then 0..n-1). Output in keys_out /
@@ -419,6 +437,15 @@ hp_status hp_batch_bvh(hp_batch* b, int32_t mesh, hp_bvh* out);
 hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in,
                         void* keys_out, int32_t* vals_out, int64_t n,
                         int32_t key_bytes, int32_t bits, void* stream);
+
+/* Spins one look-back wait of the context's radix sort passes (hp_radix_sort
+ * and every build) makes before it gives up: the wait then records
+ * HP_ERR_DEVICE_STATUS for the next hp_ctx_check and the sort goes on with the
+ * prefix it has, so its output is not sorted but every write stays inside the
+ * output. 0 restores the default, HP_SORT_SPIN_LIMIT_DEFAULT. The reference
+ * has no such bound (its sort synchronises the host after every kernel). */
+#define HP_SORT_SPIN_LIMIT_DEFAULT 4194304u
+hp_status hp_ctx_set_sort_spin_limit(hp_ctx* ctx, uint32_t spins);
 
 /* The same sort for callers that must not allocate GPU memory: no context, no
  * cudaMalloc / cudaFree / allocating library call. This entry point has no
@@ -430,11 +457,17 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
  * once on every GPU that uses the library and kept until the process exits:
  * at most HP_NOALLOC_SORT_MAX_KEYS keys per call, larger n returns HP_ERR_ARG.
  * The first call on a device looks up that array's device address, so make
- * the first call on each device before any stream capture. All calls share
- * the one array: calls whose GPU work overlaps (different streams, or
- * several host threads) race; serialise them on one stream. Every call clears
- * the scratch state it needs. device_status (optional, device memory, one
- * int32) receives a nonzero code if a bounded wait inside the sort gave up. */
+ * the first call on each device before any stream capture. That address is
+ * cached for the life of the process: it assumes the device's primary
+ * context lives as long (after cudaDeviceReset the cached address is stale
+ * and this entry point must not be called again). All calls share the one
+ * array: calls whose GPU work overlaps (different streams, or several host
+ * threads) race; serialise them on one stream. Every call clears the scratch
+ * state it needs. device_status (optional, device memory, ONE int32, need
+ * not be zeroed) is written by every call, in stream order: 0, or
+ * 1 if a bounded wait inside the sort gave up, in which case
+ * the output is not sorted. The call returns before the GPU work ends, so
+ * without device_status such a give-up goes unreported. */
 #define HP_NOALLOC_SORT_MAX_KEYS 262144
 hp_status hp_radix_sort_noalloc(const void* keys_in, const int32_t* vals_in,
                                 void* keys_out, int32_t* vals_out, int64_t n,

@@ -54,6 +54,7 @@ _SIGS = {
     "or_intersect64": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, _P]),
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     "or_adjoint64": (None, [_P, _P, _P, _P, _P, C.c_int64, _P]),
+    "or_canonical": (C.c_int64, [_P, C.c_int64, _P, C.c_int64, _P, _P]),
 }
 
 
@@ -347,3 +348,18 @@ def intersect64(v0, v1, v2, o, d, tmin=0.0):
     a = [np.ascontiguousarray(x, np.float64) for x in (v0, v1, v2, o, d)]
     hit = load().or_intersect64(*[_p(x) for x in a], tmin, _p(tuv))
     return bool(hit), tuv
+
+
+def canonical(nodes, tri_idx):
+    """Canonical form of a collapsed binary BVH (node numbering and the order of
+    triangles inside a leaf removed): (rows [count, 13] int32 = 12 child-box
+    words + size word per node in depth-first order, leaf triangle ids sorted
+    per leaf in visit order)."""
+    nodes = np.ascontiguousarray(nodes, np.int32)
+    tri_idx = np.ascontiguousarray(tri_idx, np.int32)
+    rows = np.zeros((max(nodes.shape[0], 1), 13), np.int32)
+    tris = np.zeros(max(tri_idx.shape[0], 1), np.int32)
+    c = load().or_canonical(_p(nodes), nodes.shape[0], _p(tri_idx), tri_idx.shape[0], _p(rows), _p(tris))
+    if c < 0:
+        raise ValueError("not a tree over these node and triangle arrays")
+    return rows[:c], tris[:tri_idx.shape[0]]

@@ -65,11 +65,12 @@ inline float area6(float mnx, float mny, float mnz, float mxx, float mxy, float 
     return 2.0f * std::fmaf(dz, dx, std::fmaf(dx, dy, dy * dz));
 }
 
-// detImpl<3> (util/Math.h:326-330), terms in reference order, one fma per term.
+// detImpl<3> (util/Math.h:326-330), terms in reference order with the
+// contraction nvcc applies to that expression under fast math: the first
+// difference fuses the first product over the second, each later term is one fma.
 inline float det3(const float* a) {
 #define A(r, c) a[(r) + 3 * (c)]
-    float acc = (A(0, 0) * A(1, 1)) * A(2, 2);
-    acc = std::fmaf(-(A(0, 0) * A(1, 2)), A(2, 1), acc);
+    float acc = std::fmaf(A(0, 0) * A(1, 1), A(2, 2), -((A(0, 0) * A(1, 2)) * A(2, 1)));
     acc = std::fmaf(A(1, 0) * A(2, 1), A(0, 2), acc);
     acc = std::fmaf(-(A(1, 0) * A(2, 2)), A(0, 1), acc);
     acc = std::fmaf(A(2, 0) * A(0, 1), A(1, 2), acc);
@@ -2064,8 +2065,12 @@ void or_trace(const void* nodes_in, const float* woop4, const int32_t* tri_idx, 
                     const float* v0 = woop4 + 12 * (int64_t)tri;
                     const float* v1 = v0 + 4;
                     const float* v2 = v0 + 8;
+                    // The fast-math roundings of HipTracerBinKernels.cu:216-241 as the
+                    // kernels write them: left-to-right chains for o.w; the
+                    // denominator and the v term fuse x over the rounded y product,
+                    // the u term y over the rounded x product.
                     const float Oz = std::fmaf(-oz, v0[2], std::fmaf(-oy, v0[1], std::fmaf(-ox, v0[0], v0[3])));
-                    const float den = std::fmaf(dz, v0[2], std::fmaf(dy, v0[1], dx * v0[0]));
+                    const float den = std::fmaf(dz, v0[2], std::fmaf(dx, v0[0], dy * v0[1]));
                     const float t = Oz * (1.0f / den);
                     bool closer = t < hit_t;
                     if (!closer && t == hit_t && hit >= 0) closer = tri_idx[tri] < tri_idx[hit];
@@ -2075,7 +2080,7 @@ void or_trace(const void* nodes_in, const float* woop4, const int32_t* tri_idx, 
                         const float u = std::fmaf(t, Dx, Ox);
                         if (u >= 0.0f) {
                             const float Oy = std::fmaf(oz, v2[2], std::fmaf(oy, v2[1], std::fmaf(ox, v2[0], v2[3])));
-                            const float Dy = std::fmaf(dz, v2[2], std::fmaf(dy, v2[1], dx * v2[0]));
+                            const float Dy = std::fmaf(dz, v2[2], std::fmaf(dx, v2[0], dy * v2[1]));
                             const float v = std::fmaf(t, Dy, Oy);
                             if (v >= 0.0f && u + v <= 1.0f) {
                                 hit_t = t; hit = tri; hit_u = u; hit_v = v;
@@ -2198,3 +2203,41 @@ void or_adjoint64(const float* verts, const int32_t* tris, const float* rays, co
 }
 
 }  // extern "C"
+
+// ---- canonical form of a collapsed binary BVH ---------------------------------
+// Builders that number nodes by atomics (the reference's collapser,
+// rt/bvh/BVHCollapserKernels.cu:268-433) leave node order and the order of
+// triangles inside a leaf undefined; the tree itself is defined. Its canonical
+// form: nodes in depth-first order from the root, child 0 before child 1;
+// per node its 12 child-box words and its size word (~size for a leaf), and
+// per leaf its triangle ids in ascending order, appended in visit order.
+// Returns the number of nodes visited, or -1 if an index leaves the arrays or
+// a node is reached twice.
+extern "C" int64_t or_canonical(const int32_t* nodes, int64_t num_nodes, const int32_t* tri_idx, int64_t num_refs,
+                                int32_t* rows /* [num_nodes][13] */, int32_t* tris /* [num_refs] */) {
+    if (num_nodes <= 0) return 0;
+    std::vector<int32_t> stack{0};
+    std::vector<char> seen((size_t)num_nodes, 0);
+    int64_t count = 0, nt = 0;
+    while (!stack.empty()) {
+        const int32_t i = stack.back();
+        stack.pop_back();
+        if (i < 0 || i >= num_nodes || seen[(size_t)i]) return -1;
+        seen[(size_t)i] = 1;
+        const int32_t* nd = nodes + 16 * (int64_t)i;
+        int32_t* row = rows + 13 * count++;
+        for (int k = 0; k < 12; ++k) row[k] = nd[k];
+        row[12] = nd[14];
+        if (nd[14] < 0) {
+            const int32_t b = nd[12], e = nd[13];
+            if (b < 0 || e < b || e > num_refs || nt + (e - b) > num_refs) return -1;
+            std::copy(tri_idx + b, tri_idx + e, tris + nt);
+            std::sort(tris + nt, tris + nt + (e - b));
+            nt += e - b;
+        } else {
+            stack.push_back(nd[13] < 0 ? ~nd[13] : nd[13]);
+            stack.push_back(nd[12] < 0 ? ~nd[12] : nd[12]);
+        }
+    }
+    return count;
+}

@@ -6,9 +6,10 @@
 #   rt/tracer/HipTracerBinKernels.cu: inline PTX uses `vote.ballot.b32` without
 #     `.sync`, which ptxas rejects for sm_70 and later; it becomes
 #     `vote.sync.ballot.b32` over the active lanes.
-# Everything else is compiled from /root/reference where it lies.
+# Everything else is compiled from the reference tree where it lies.
+# REF (the reference's src/hippie directory) is set by the Makefile.
 set -e
-REF=${REF:-/root/reference/src/hippie}
+: "${REF:?REF must name the reference's src/hippie directory}"
 OUT=$1
 mkdir -p "$OUT/util" "$OUT/tracer"
 tr -d '\r' < "$REF/util/Math.h" \

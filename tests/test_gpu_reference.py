@@ -5,8 +5,12 @@ Bit-exact: Morton keys, sorted keys and reference order, Karras topology,
 refitted pre-collapse boxes. After the collapse, whose numbering the reference
 takes from atomics, both trees are compared in a canonical depth-first form
 (structure, child boxes bit for bit, each leaf's set of triangles). The SAH
-cost agrees to 0.1 %; hits of the reference tracer agree by triangle id, and
-in t / u / v to 1e-6 relative (with the floor 1 that unit-scene values take).
+cost agrees to 0.1 %. With the reference's arithmetic selected
+(hp_ctx_set_arithmetic: its fast-math reciprocals), Woop rows are bit-identical
+and every hit record equals the reference tracer's except on rays with two
+hits at exactly the same t, where this library reports the lower triangle id;
+those are counted. With the default IEEE reciprocals, hits agree by triangle
+id on all but a few rays near triangle edges, and t to 1e-6 relative.
 """
 import numpy as np
 import pytest
@@ -111,7 +115,22 @@ def test_ploc_matches_reference_kernels(ctx):
     assert bvh.cost() == pytest.approx(rc, rel=1e-3)
 
 
-def test_trace_matches_reference_tracer(ctx):
+def compare_hits(mine, ref):
+    """Split rays into equal hit records, exact-t ties and other differences.
+
+    A tie: both hit at the same t (bit for bit) on different triangles, and
+    this library reports the lower triangle id (the reference keeps the first
+    one its traversal meets). Returns (equal, ties, indices of the others)."""
+    same = np.all(mine == ref, axis=1)
+    both = (mine[:, 0] >= 0) & (ref[:, 0] >= 0)
+    tie = ~same & both & (mine[:, 1] == ref[:, 1]) & (mine[:, 0] < ref[:, 0])
+    return int(same.sum()), int(tie.sum()), np.nonzero(~same & ~tie)[0]
+
+
+def test_trace_matches_reference_tracer_ieee(ctx):
+    """Default (IEEE reciprocal) arithmetic against the reference tracer on the
+    same nodes and Woop rows: the reciprocals differ in the last bit, so a few
+    rays near a triangle edge may change triangle; t agrees to 1e-6."""
     n = 65536
     v, t = hp.gen.uniform_mesh(0xC0FFEE + 1, n)
     rays = hp.gen.rays_targeted(0xC0FFEE + 11, 1 << 20)
@@ -131,3 +150,91 @@ def test_trace_matches_reference_tracer(ctx):
     err = np.abs(tm - tr) / np.maximum(1.0, np.abs(tr))
     assert np.quantile(err[:, 0], 0.999) <= 1e-6
     assert np.quantile(err[:, 1:], 0.99) <= 1e-4
+
+
+def _ref_ctx():
+    c = hp.Context(0)
+    c.set_arithmetic("reference")
+    return c
+
+
+def _check_reference_hits(rctx, V, T, rays, params, method, **build_kw):
+    """Build and trace in reference arithmetic; compare (1) Woop rows per
+    triangle with the reference's woopify, (2) hits with the reference tracer
+    on this library's BVH, (3) hits with the reference's own build + tracer.
+    Every differing ray must be an exact-t tie won by the lower id."""
+    Rr = dev(rays)
+    bvh = rctx.build(V, T, params)
+    mine = rctx.trace(bvh, Rr, results=torch.zeros((rays.shape[0], 4), dtype=torch.int32, device="cuda"))
+    mine = mine.cpu().numpy()
+    rctx.check()
+    nodes, woop, tri = bvh.download()
+    box = np.array(bvh.c.scene_box, np.float32)
+    ref = R.build(V, T, box, method=method, **build_kw)
+    mw = np.zeros_like(woop)
+    rw = np.zeros_like(woop)
+    mw[tri] = woop
+    rw[ref["tri_idx"]] = ref["woop"]
+    np.testing.assert_array_equal(mw.view(np.int32), rw.view(np.int32))
+    on_mine, _ = R.trace(torch.from_numpy(nodes).cuda(), torch.from_numpy(woop).cuda(), torch.from_numpy(tri).cuda(),
+                         Rr)
+    own, _ = R.trace(torch.from_numpy(ref["nodes"]).cuda(), torch.from_numpy(ref["woop"]).cuda(),
+                     torch.from_numpy(ref["tri_idx"]).cuda(), Rr)
+    out = {}
+    for name, r in (("same_bvh", on_mine), ("reference_build", own)):
+        eq, ties, other = compare_hits(mine, r)
+        assert other.size == 0, (name, other[:10], mine[other[:10]], r[other[:10]])
+        out[name] = (eq, ties)
+    print(f"reference-arithmetic hits: {rays.shape[0]} rays; equal / exact-t ties: {out}")
+    return out
+
+
+def test_trace_reference_arithmetic_bit_identical_uniform64k():
+    """65,536 uniform triangles (30-bit LBVH), 1,048,576 targeted rays."""
+    v, t = hp.gen.uniform_mesh(0xC0FFEE, 65536, 0.01)
+    rays = hp.gen.rays_targeted(0xC0FFEE + 1, 1 << 20, -0.5, 1.5)
+    rctx = _ref_ctx()
+    try:
+        out = _check_reference_hits(rctx, dev(v), dev(t), rays, hp.BuildParams(morton_bits=30), "lbvh", bits=30)
+        assert out["same_bvh"][0] + out["same_bvh"][1] == rays.shape[0]
+    finally:
+        rctx.close()
+
+
+def test_trace_reference_arithmetic_bit_identical_ploc4m():
+    """4,194,304 clustered triangles (PLOC radius 16, 60-bit), all 16,777,216
+    sphere rays: the bench workload."""
+    seed = 0xC0FFEE + 1
+    v, t = hp.gen.clustered_mesh(seed, 4194304, 1024, 0.02, 0.005)
+    box = np.concatenate([v.min(0), v.max(0)]).astype(np.float32)
+    rays = hp.gen.rays_sphere(seed + 1, 16777216, box)
+    rctx = _ref_ctx()
+    try:
+        p = hp.BuildParams(method="ploc", morton_bits=60, ploc_radius=16, ploc_max_radius=256, ploc_adaptive=0)
+        _check_reference_hits(rctx, dev(v), dev(t), rays, p, "ploc", bits=60, radius=16, max_radius=256)
+    finally:
+        rctx.close()
+
+
+def test_reference_arithmetic_refit_woop():
+    """hp_refit in reference arithmetic rewrites the Woop rows as the reference's
+    woopify of the moved vertices (compared through a fresh reference build)."""
+    v, t = hp.gen.heightfield(3, 64, 128)
+    rctx = _ref_ctx()
+    try:
+        V, T = dev(v), dev(t)
+        bvh = rctx.build(V, T, hp.BuildParams(morton_bits=60))
+        v2 = v.copy()
+        v2[:, 2] += np.random.default_rng(1).uniform(-0.01, 0.01, v.shape[0]).astype(np.float32)
+        V2 = dev(v2)
+        rctx.refit(bvh, V2, T)
+        rctx.check()
+        _, woop, tri = bvh.download()
+        ref = R.build(V2, T, np.concatenate([v2.min(0), v2.max(0)]).astype(np.float32), method="lbvh", bits=60)
+        mw = np.zeros_like(woop)
+        rw = np.zeros_like(woop)
+        mw[tri] = woop
+        rw[ref["tri_idx"]] = ref["woop"]
+        np.testing.assert_array_equal(mw.view(np.int32), rw.view(np.int32))
+    finally:
+        rctx.close()

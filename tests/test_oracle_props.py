@@ -184,3 +184,41 @@ def test_ploc_oracle_tree_valid(n):
     if n > 100:
         lb = oracle.build_lbvh(v, t, bits=60)
         assert oracle.cost(r["nodes"], r["box"]) < oracle.cost(lb["nodes"], lb["box"])
+
+
+def test_canonical_form_ignores_numbering():
+    """oracle.canonical: the depth-first form of a collapsed tree does not change
+    when interior nodes are renumbered or a leaf's triangles are reordered, and
+    it matches a direct walk of the tree."""
+    import hippie_b200 as hp
+    v, t = hp.gen.clustered_mesh(21, 5000, clusters=16)
+    r = oracle.build_ploc(v, t, radius=4, max_radius=64)
+    nodes, tri = r["nodes"], r["tri_idx"]
+    rows, tris = oracle.canonical(nodes, tri)
+    assert rows.shape[0] == nodes.shape[0]
+    assert sorted(tris.tolist()) == list(range(t.shape[0]))
+    # renumber interior nodes 1.. in reverse and reverse every leaf's triangles
+    n_int = int(r["counts"][0])
+    perm = np.arange(nodes.shape[0])
+    perm[1:n_int] = perm[1:n_int][::-1]
+    new = np.empty_like(nodes)
+    new[perm] = nodes
+    for i in range(new.shape[0]):
+        for k in (12, 13):
+            c = new[i, k]
+            if new[i, 14] >= 0 and 0 <= c < n_int:
+                new[i, k] = perm[c]
+        if new[i, 15] >= 0:
+            new[i, 15] = perm[new[i, 15]]
+    tri2 = tri.copy()
+    for i in range(new.shape[0]):
+        if new[i, 14] < 0:
+            b, e = new[i, 12], new[i, 13]
+            tri2[b:e] = tri2[b:e][::-1]
+    rows2, tris2 = oracle.canonical(new, tri2)
+    np.testing.assert_array_equal(rows, rows2)
+    np.testing.assert_array_equal(tris, tris2)
+    with pytest.raises(ValueError):
+        bad = nodes.copy()
+        bad[0, 12] = nodes.shape[0] + 5
+        oracle.canonical(bad, tri)

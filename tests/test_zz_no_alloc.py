@@ -39,18 +39,33 @@ def test_noalloc_sort_matches_arena_sort_on_consecutive_calls():
     lib = _lib.load()
     ctx = hp.Context(0)
     stream = torch.cuda.current_stream()
-    status = torch.zeros(1, dtype=torch.int32, device="cuda")
-    for call, (n, kb, bits) in enumerate([(200003, 8, 60), (MAX_KEYS, 4, 30), (4099, 8, 64)]):
+    # One int32 of status, as the header documents; it starts with a stale
+    # nonzero value because every call overwrites it with its own code.
+    status = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    cases = [  # (n, key bytes, bits, caller values, status word)
+        (200003, 8, 60, False, True),
+        (MAX_KEYS, 4, 30, True, True),   # caller-supplied values: a permutation
+        (4099, 8, 64, False, False),     # no status word
+        (70001, 4, 8, True, True),       # one pass, written straight to the output
+        (MAX_KEYS, 8, 60, True, False),
+    ]
+    for call, (n, kb, bits, with_vals, with_status) in enumerate(cases):
         K = _keys(n, kb, bits, seed=call)
-        ref_k, ref_v = ctx.radix_sort(K, bits=bits)
+        V = None
+        if with_vals:
+            V = torch.from_numpy(np.random.default_rng(100 + call).permutation(n).astype(np.int32)).cuda()
+        ref_k, ref_v = ctx.radix_sort(K, vals=V, bits=bits)
+        ctx.check()
         out_k = torch.full_like(K, -1)
         out_v = torch.full((n,), -1, dtype=torch.int32, device="cuda")
-        st = lib.hp_radix_sort_noalloc(C.c_void_p(K.data_ptr()), None, C.c_void_p(out_k.data_ptr()),
-                                       C.c_void_p(out_v.data_ptr()), n, kb, bits,
-                                       C.c_void_p(status.data_ptr()), C.c_void_p(stream.cuda_stream))
+        st = lib.hp_radix_sort_noalloc(C.c_void_p(K.data_ptr()), None if V is None else C.c_void_p(V.data_ptr()),
+                                       C.c_void_p(out_k.data_ptr()), C.c_void_p(out_v.data_ptr()), n, kb, bits,
+                                       C.c_void_p(status.data_ptr()) if with_status else None,
+                                       C.c_void_p(stream.cuda_stream))
         assert st == 0, lib.hp_last_error()
         torch.cuda.synchronize()
-        assert int(status.item()) == 0
+        if with_status:
+            assert int(status.item()) == 0
         assert torch.equal(out_v, ref_v), f"call {call}: values differ"
         assert torch.equal(out_k, ref_k), f"call {call}: keys differ"
     ctx.close()
