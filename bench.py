@@ -19,10 +19,19 @@ e2e        the same metrics through the C ABI with pinned host buffers: the
            (every ray uploaded and every hit record downloaded, in chunks whose
            copies overlap the traces of their neighbours).
 roofline   the radix-sort pass (the build's HBM-bound kernel): algorithmic
-           bytes n * 2 * (K + 4) per pass over its average CUDA-event duration.
-Multi-GPU: one process per GPU (torchrun), every rank builds and traces its
-own scene of the same size (independent units, no collective on the data
-path); the reported time is the max over ranks.
+           bytes n * 2 * (K + 4) per pass over its average CUDA-event duration;
+           roofline.phases gives every HBM-bound build phase with the survey's
+           algorithmic bytes (scene box + boxes + Morton, the sort), and
+           large.roofline_phases_lbvh the same plus the refit climb on the
+           33,554,432-triangle LBVH.
+Multi-GPU: one process per GPU (torchrun). Default (--parallel rays): one
+scene, its rays split contiguously across the ranks; every rank builds the
+BVH from the same input (no collective on the data path), or with
+--bvh-broadcast 1 rank 0 builds it and broadcasts nodes, Woop rows and
+triangle indices over NCCL; value = triangles of the one scene over the max
+build time, trace_mrays_s = all rays over the max trace time (strong scaling).
+--parallel replicas: every rank builds and traces a scene of its own (weak
+scaling). Times are the max over ranks.
 
 --impl reference times the CPU restatement of the same algorithms (the
 reference has no CPU path of its own) on the host cores, rank 0 only.
@@ -55,16 +64,24 @@ CONFIGS = {
 DEFAULT_CONFIG = "ploc4m"
 
 
-def make_inputs(cfg, rank):
-    import hippie_b200 as hp
+def make_inputs(cfg, rank, library_free=False):
+    """The workload's mesh and rays (rank > 0: another scene of the same size,
+    for replicas). library_free: the oracle's copy of the generators, so that
+    the CPU arm never loads the GPU library (same bytes)."""
+    if library_free:
+        import oracle
+        gen = oracle.gen
+    else:
+        import hippie_b200 as hp
+        gen = hp.gen
     seed = SEED + cfg["config_id"] + 1000 * rank
     if cfg["mesh"] == "uniform":
-        v, t = hp.gen.uniform_mesh(seed, cfg["n"], 0.01)
-        rays = hp.gen.rays_targeted(seed + 1, cfg["rays"], -0.5, 1.5)
+        v, t = gen.uniform_mesh(seed, cfg["n"], 0.01)
+        rays = gen.rays_targeted(seed + 1, cfg["rays"], -0.5, 1.5)
     else:
-        v, t = hp.gen.clustered_mesh(seed, cfg["n"], 1024, 0.02, 0.005)
+        v, t = gen.clustered_mesh(seed, cfg["n"], 1024, 0.02, 0.005)
         box = np.concatenate([v.min(0), v.max(0)]).astype(np.float32)
-        rays = hp.gen.rays_sphere(seed + 1, cfg["rays"], box)
+        rays = gen.rays_sphere(seed + 1, cfg["rays"], box)
     return v, t, rays
 
 
@@ -158,6 +175,64 @@ def committed_traffic(name):
         except ValueError:
             return None
     return None
+
+
+def profile_phases(ctx, fn):
+    """Run fn() with the context's phase events on; {phase: [ms per occurrence]}."""
+    import ctypes as C
+    import torch
+    from hippie_b200 import _lib
+    lib = _lib.load()
+    lib.hp_profile_reset(ctx.h)
+    lib.hp_profile_enable(ctx.h, 1)
+    fn()
+    torch.cuda.synchronize()
+    out = {}
+    for i in range(1, lib.hp_profile_count(ctx.h)):
+        nm = C.create_string_buffer(64)
+        ms = C.c_float()
+        lib.hp_profile_get(ctx.h, i, nm, 64, C.byref(ms))
+        out.setdefault(nm.value.decode(), []).append(ms.value)
+    lib.hp_profile_enable(ctx.h, 0)
+    lib.hp_profile_reset(ctx.h)
+    return out
+
+
+def phase_rooflines(n, bits, phases, peak):
+    """HBM fractions of the build phases with the survey's algorithmic bytes
+    (K = key bytes, AABB = 24 B):
+      scene box + boxes + Morton  36 n + n (12 idx + 36 verts + K + 4)
+      radix sort                  n * P * 2 * (K + 4), P = ceil(bits / 8)
+      refit (LBVH climb)          24 (2n-2) + 24 (n-1) + 8 (n-1) + 4 (2n-1) + 8 (n-1)
+    over the phases' CUDA-event times. The refit is the two climb kernels
+    (CTA-local nodes in shared memory, then the nodes that cross CTA ranges);
+    its collapse-cost and state writes are not in the formula."""
+    kb = 4 if bits <= 32 else 8
+    passes = (bits + 7) // 8
+    rows = []
+
+    def add(name, nbytes, ms, extra=None):
+        if ms <= 0:
+            return
+        a = nbytes / (ms * 1e-3) / 1e9
+        r = {"phase": name, "bytes": int(nbytes), "ms": round(ms, 5), "achieved_gbs": round(a, 1),
+             "frac": round(a / peak, 4)}
+        if extra:
+            r.update(extra)
+        rows.append(r)
+
+    if "boxes" in phases and "morton" in phases:
+        add("scene box + boxes + Morton", 36 * n + n * (12 + 36 + kb + 4),
+            sum(phases["boxes"]) + sum(phases["morton"]))
+    if "sort_pass" in phases:
+        add(f"radix sort ({len(phases['sort_pass'])} passes)", n * passes * 2 * (kb + 4), sum(phases["sort_pass"]),
+            {"per_pass_ms": round(float(np.mean(phases["sort_pass"])), 5)})
+    if "climb" in phases:
+        refit = 24 * (2 * n - 2) + 24 * (n - 1) + 8 * (n - 1) + 4 * (2 * n - 1) + 8 * (n - 1)
+        local = sum(phases.get("climb_local", []))
+        add("refit (LBVH climb)", refit, local + sum(phases["climb"]),
+            {"local_ms": round(local, 5), "frontier_ms": round(sum(phases["climb"]), 5)})
+    return rows
 
 
 def oracle_build(cfg, v, t):
@@ -425,8 +500,25 @@ def extra_large(ctx, steps=3, seed=SEED + 4):
 
     t_lbvh, t_atr, t_gen, t_prim, t_sec, t_sort = (med(0, 1), med(1, 2), med(2, 3), med(3, 4), med(4, 5),
                                                    med(5, 6))
+    # Build-phase roofline fractions of the LBVH (boxes + Morton, sort, refit
+    # climb) from per-phase CUDA events of one more build; the ATR stage's
+    # treelet kernels are instruction-bound and reported by time only.
+    peak, peak_kind = peak_hbm()
+    ph = profile_phases(ctx, lambda: ctx.build(V, T, p_lbvh, bvh=lb))
+    ph_atr = profile_phases(ctx, lambda: ctx.build(V, T, p_atr, bvh=at))
+    # Traversal is latency- and L2-bound: its HBM fraction counts only the
+    # ray and result bytes it must move (32 B in, 16 B out per ray).
+    io = 48 * w * h
+    trace_roof = {"bound": "latency / L2 (BVH of 33.5 M triangles, about 1.3 GB, exceeds the 126 MB L2)",
+                  "io_bytes_per_trace": io,
+                  "primary_io_frac": io / (t_prim * 1e-3) / 1e9 / peak,
+                  "secondary_io_frac": io / (t_sec * 1e-3) / 1e9 / peak,
+                  "secondary_sorted_io_frac": io / (t_sort * 1e-3) / 1e9 / peak}
     return {"workload": "33,554,432 tris (uniform + clustered, interleaved), LBVH 60-bit + ATR treelet 9 x 2; "
                         "32Mi pinhole primaries (8192x4096) + 32Mi sphere rays",
+            "roofline_phases_lbvh": phase_rooflines(n, 60, ph, peak), "peak_gbs": peak, "peak_kind": peak_kind,
+            "atr_phases_ms": {k: round(sum(x), 4) for k, x in ph_atr.items()},
+            "trace_roofline": trace_roof,
             "lbvh_build_ms": t_lbvh, "atr_build_ms": t_atr, "atr_mtris_s": n / t_atr / 1e3,
             "lbvh_mtris_s": n / t_lbvh / 1e3, "sah_cost_lbvh": lb.cost(), "sah_cost_atr": at.cost(),
             "primary_gen_ms": t_gen, "primary_trace_mrays_s": w * h / t_prim / 1e3,
@@ -521,17 +613,27 @@ def extra_methods(ctx, cfg, V, T, R, RES, steps=3):
 
 
 def run_reference(args, cfg, rank):
-    """CPU restatement of the path, timed on the host cores (rank 0 only)."""
+    """CPU restatement of the path (the oracle), timed on the host cores, rank 0
+    only. Each step builds and traces the whole workload when the run fits
+    about 150 s of CPU time (calibrated on 131,072 triangles and rays), else
+    the same fraction of the triangles and of the rays."""
     if rank != 0:
         return 0
     import oracle
-    v, t, rays = make_inputs(cfg, 0)
+    v, t, rays = make_inputs(cfg, 0, library_free=True)
     oracle.load()
     steps, warmup = args.steps, args.warmup
-    budget = 150.0 / max(1, steps + warmup)
-    m = cpu_sample(cfg, v, t, 0.6 * budget)
+    c = min(t.shape[0], 131072)
+    t0 = time.perf_counter()
+    r = oracle_build(cfg, v, np.ascontiguousarray(t[:c]))
+    t1 = time.perf_counter()
+    oracle.trace(r["nodes"], r["woop"], r["tri_idx"], rays[:c])
+    t2 = time.perf_counter()
+    full = (t1 - t0) * t.shape[0] / c + (t2 - t1) * rays.shape[0] / c
+    frac = min(1.0, 150.0 / max(1, steps + warmup) / max(full, 1e-6))
+    m = max(c, int(t.shape[0] * frac)) if frac < 1.0 else t.shape[0]
+    k = max(c, int(rays.shape[0] * frac)) if frac < 1.0 else rays.shape[0]
     tm = np.ascontiguousarray(t[:m])
-    k = min(rays.shape[0], 1 << 17)
     bt, tt = [], []
     for i in range(warmup + steps):
         t0 = time.perf_counter()
@@ -546,13 +648,15 @@ def run_reference(args, cfg, rank):
     tr = float(np.mean(tt))
     val = m / b / 1e6
     cores = os.cpu_count() or 1
+    whole = m == t.shape[0] and k == rays.shape[0]
+    sample = ("the whole workload every step" if whole else
+              f"first {m} of {t.shape[0]} triangles built, first {k} of {rays.shape[0]} rays traced per step")
     line = {"metric": METRIC, "value": val, "unit": "Mtris/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * (b + tr), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "method": cfg["method"], "sample_tris": m, "sample_rays": k},
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "method": cfg["method"], "triangles": m, "rays": k},
             "trace_mrays_s": k / tr / 1e6,
-            "cpu_baseline": {"value": val, "unit": "Mtris/s", "cores": cores, "kind": "port",
-                             "sample": f"first {m} triangles built, {k} rays traced per step"},
+            "cpu_baseline": {"value": val, "unit": "Mtris/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "Mtris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -572,6 +676,11 @@ def main(argv=None):
     ap.add_argument("--extras", type=int, default=1,
                     help="also measure the batched (2048 meshes) and differentiable (heightfield) workloads")
     ap.add_argument("--rays", type=int, default=0, help="override the workload's ray count (profiling)")
+    ap.add_argument("--parallel", default="rays", choices=["rays", "replicas"],
+                    help="N > 1: 'rays' splits one scene's rays across the ranks (every rank holds the BVH); "
+                         "'replicas' gives every rank a scene of its own")
+    ap.add_argument("--bvh-broadcast", type=int, default=0,
+                    help="rays mode: rank 0 builds and broadcasts the BVH over NCCL (default: every rank builds)")
     ap.add_argument("--reference-kernels", type=int, default=1,
                     help="also time the reference's own CUDA kernels where they were built (1 GPU)")
     args = ap.parse_args(argv)
@@ -593,18 +702,46 @@ def main(argv=None):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     import hippie_b200 as hp
     from hippie_b200 import _lib
+    from hippie_b200.shard import broadcast_bvh_arrays, ray_ranges
     lib = _lib.load()
     ctx = hp.Context(local)
-    v, t, rays = make_inputs(cfg, rank)
-    n, nr = t.shape[0], rays.shape[0]
+    # rays: one scene, its rays split contiguously across ranks, the BVH on every
+    # rank (built there, or built on rank 0 and broadcast); replicas: every rank
+    # builds and traces a scene of its own.
+    mode = args.parallel if world > 1 else "rays"
+    bcast = mode == "rays" and world > 1 and bool(args.bvh_broadcast)
+    v, t, rays = make_inputs(cfg, rank if mode == "replicas" else 0)
+    n, nr_all = t.shape[0], rays.shape[0]
+    lo, hi = ray_ranges(nr_all, world)[rank] if mode == "rays" else (0, nr_all)
+    nr = hi - lo                                     # this rank's rays
+    job_tris = world * n if mode == "replicas" else n
+    job_rays = world * nr_all if mode == "replicas" else nr_all
     Vh = torch.from_numpy(v).pin_memory()
     Th = torch.from_numpy(t).pin_memory()
-    Rh = torch.from_numpy(rays).pin_memory()
+    Rh = torch.from_numpy(np.ascontiguousarray(rays[lo:hi])).pin_memory()
+    del rays
     V, T, R = Vh.cuda(), Th.cuda(), Rh.cuda()
     RES = torch.empty((nr, 4), dtype=torch.int32, device="cuda")
     RESh = torch.empty((nr, 4), dtype=torch.int32).pin_memory()
     params = build_params(cfg)
-    bvh = ctx.build(V, T, params)
+    bvh = hp.BVH.reserve(ctx, n) if bcast and rank != 0 else hp.BVH(ctx)
+
+    def build_step():
+        """One build of the scene on this rank, or, with the broadcast, on rank 0
+        followed by an NCCL broadcast of its arrays into every rank's BVH."""
+        if not bcast:
+            ctx.build(V, T, params, bvh=bvh)
+            return
+        info = None
+        if rank == 0:
+            ctx.build(V, T, params, bvh=bvh)
+            bvh.sync()
+            info = bvh.info()
+        got = broadcast_bvh_arrays(bvh.arrays(), info)
+        if rank != 0:
+            bvh.set_info(got["num_interior"], got["num_leaf"], got["scene_box"], got["morton_scale"])
+
+    build_step()
     stream = torch.cuda.current_stream()
     if args.once:
         ctx.trace(bvh, R, results=RES)
@@ -614,14 +751,23 @@ def main(argv=None):
                           "leaves": bvh.c.num_leaf}), flush=True)
         del bvh
         ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
         return 0
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(*xs):
+        if world == 1:
+            return list(xs)
+        tt = torch.tensor(list(xs), device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return tt.tolist()
+
     for _ in range(args.warmup):
-        ctx.build(V, T, params, bvh=bvh)
+        build_step()
         ctx.trace(bvh, R, results=RES)
     torch.cuda.synchronize()
     ctx.check()
@@ -634,7 +780,7 @@ def main(argv=None):
         t0 = time.perf_counter()
         choice = ctx.autotune(V, T, R, params, ploc_radius=True)
         tune_s = time.perf_counter() - t0
-        ctx.build(V, T, params, bvh=bvh)
+        build_step()
         ctx.trace(bvh, R, results=RES)
         torch.cuda.synchronize()
         ctx.check()
@@ -650,7 +796,7 @@ def main(argv=None):
     w0 = time.time()
     for k in range(args.steps):
         ev[k][0].record(stream)
-        ctx.build(V, T, params, bvh=bvh)
+        build_step()
         ev[k][1].record(stream)
         ctx.trace(bvh, R, results=RES)
         ev[k][2].record(stream)
@@ -665,10 +811,7 @@ def main(argv=None):
     build_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
     trace_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
     step_ms = float(ev[0][0].elapsed_time(ev[-1][2])) / args.steps
-    if world > 1:
-        tt = torch.tensor([build_ms, trace_ms, step_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        build_ms, trace_ms, step_ms = tt.tolist()
+    build_ms, trace_ms, step_ms = max_over_ranks(build_ms, trace_ms, step_ms)
 
     # ---- the same rays traced in ray Morton order (keys + sort + trace, HipTracer::traceSort) ----
     for _ in range(2):
@@ -680,11 +823,7 @@ def main(argv=None):
         evs[k][1].record(stream)
     torch.cuda.synchronize()
     ctx.check()
-    sorted_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
-    if world > 1:
-        tt = torch.tensor([sorted_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        sorted_ms = tt.item()
+    sorted_ms, = max_over_ranks(float(np.mean([e[0].elapsed_time(e[1]) for e in evs])))
 
     # ---- the same trace with the default launch choices (no tuning, input order) ----
     tuned_set = ctx.get_tune()
@@ -697,11 +836,7 @@ def main(argv=None):
         evp[k][1].record(stream)
     torch.cuda.synchronize()
     ctx.check()
-    plain_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evp]))
-    if world > 1:
-        tt = torch.tensor([plain_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        plain_ms = tt.item()
+    plain_ms, = max_over_ranks(float(np.mean([e[0].elapsed_time(e[1]) for e in evp])))
     ctx.set_tune(**{k: tuned_set[k] for k in ("sort_block", "trace_ctas_per_sm", "trace_stack", "trace_sorted")})
     tuned = None if choice is None else {
         "choice": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in choice.items()},
@@ -711,10 +846,11 @@ def main(argv=None):
     e2e_b, e2e_t = [], []
     for k in range(max(3, args.steps // 2)):
         torch.cuda.synchronize()
+        barrier()
         a = time.perf_counter()
         V.copy_(Vh, non_blocking=True)
         T.copy_(Th, non_blocking=True)
-        ctx.build(V, T, params, bvh=bvh)
+        build_step()
         bvh.sync()
         b = time.perf_counter()
         ctx.trace_host(bvh, Rh, results=RESh)  # hp_trace_host: chunked uploads / traces / downloads overlap
@@ -722,64 +858,48 @@ def main(argv=None):
         c = time.perf_counter()
         e2e_b.append(b - a)
         e2e_t.append(c - b)
-    e2e_b_s, e2e_t_s = float(np.median(e2e_b)), float(np.median(e2e_t))
-    if world > 1:
-        tt = torch.tensor([e2e_b_s, e2e_t_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_b_s, e2e_t_s = tt.tolist()
+    e2e_b_s, e2e_t_s = max_over_ranks(float(np.median(e2e_b)), float(np.median(e2e_t)))
 
-    # ---- roofline of the radix-sort pass (per-pass CUDA events on the build stream) ----
-    lib.hp_profile_reset(ctx.h)
-    lib.hp_profile_enable(ctx.h, 1)
-    ctx.build(V, T, params, bvh=bvh)
-    torch.cuda.synchronize()
-    import ctypes as C
-    phases = {}
-    passes = []
-    for i in range(1, lib.hp_profile_count(ctx.h)):
-        nm = C.create_string_buffer(64)
-        ms = C.c_float()
-        lib.hp_profile_get(ctx.h, i, nm, 64, C.byref(ms))
-        name = nm.value.decode()
-        phases[name] = phases.get(name, 0.0) + ms.value
-        if name == "sort_pass":
-            passes.append(ms.value)
-    lib.hp_profile_enable(ctx.h, 0)
-    lib.hp_profile_reset(ctx.h)
+    # ---- per-phase CUDA events of one more build: sort-pass roofline and the phase fractions ----
+    phases_l = profile_phases(ctx, build_step)
+    phases = {k: sum(x) for k, x in phases_l.items()}
+    passes = phases_l.get("sort_pass", [])
     kb = 4 if cfg["bits"] <= 32 else 8
     pass_bytes = n * 2 * (kb + 4)
     pass_ms = float(np.mean(passes)) if passes else float("nan")
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     peak, peak_kind = peak_hbm()
     traffic = committed_traffic("sort_pass")
+    parallelism = (f"replicas x{world}" if mode == "replicas" else
+                   f"rays x{world}, BVH " + ("broadcast from rank 0 (NCCL)" if bcast else "built on every rank"))
 
     line = {
-        "metric": METRIC, "value": world * n / (build_ms * 1e-3) / 1e6, "unit": "Mtris/s",
+        "metric": METRIC, "value": job_tris / (build_ms * 1e-3) / 1e6, "unit": "Mtris/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": cfg["workload"], "method": cfg["method"], "triangles": n, "rays": nr,
-                   "morton_bits": cfg["bits"], "parallelism": f"replicas x{world}",
+        "higher_is_better": True, "scaling": "weak" if mode == "replicas" else "strong", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "method": cfg["method"], "triangles": n, "rays": nr_all,
+                   "morton_bits": cfg["bits"], "parallelism": parallelism,
                    "l2": "inputs larger than L2 (mesh 200 MB, rays 512 MB)"},
-        "trace_mrays_s": world * nr / (trace_ms * 1e-3) / 1e6,
-        "trace_sorted_mrays_s": world * nr / (sorted_ms * 1e-3) / 1e6,
-        "trace_untuned_mrays_s": world * nr / (plain_ms * 1e-3) / 1e6,
+        "trace_mrays_s": job_rays / (trace_ms * 1e-3) / 1e6,
+        "trace_sorted_mrays_s": job_rays / (sorted_ms * 1e-3) / 1e6,
+        "trace_untuned_mrays_s": job_rays / (plain_ms * 1e-3) / 1e6,
         "autotuned": tuned,
         "build_ms": build_ms, "trace_ms": trace_ms,
         "phases_ms": {k: round(x, 4) for k, x in phases.items()},
-        "e2e": {"value": world * n / e2e_b_s / 1e6, "unit": "Mtris/s",
-                "trace_mrays_s": world * nr / e2e_t_s / 1e6,
-                "h2d_bytes_per_step": int(v.nbytes + t.nbytes + rays.nbytes),
-                "d2h_bytes_per_step": int(nr * 16 + 8)},
+        "e2e": {"value": job_tris / e2e_b_s / 1e6, "unit": "Mtris/s",
+                "trace_mrays_s": job_rays / e2e_t_s / 1e6,
+                "h2d_bytes_per_step": int(world * (v.nbytes + t.nbytes) + job_rays * 32),
+                "d2h_bytes_per_step": int(job_rays * 16 + 8 * world)},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix sort pass)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": pass_bytes,
-                     "launch_ms": pass_ms},
+                     "launch_ms": pass_ms, "phases": phase_rooflines(n, cfg["bits"], phases_l, peak)},
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, v, t, rays)
+        line["cpu_baseline"] = cpu_baseline(cfg, v, t, Rh.numpy())
     if rank == 0 and world == 1 and args.reference_kernels:
         line["reference_kernels_gpu"] = reference_kernels(cfg, V, T, R, v)
     ctx.reset_tune()  # the other workloads run with the default launch choices

@@ -142,6 +142,36 @@ class BVH:
         check(load().hp_bvh_validate(self.ctx.h, C.byref(self.c), C.byref(m), C.byref(ok), _stream_ptr(stream)))
         return bool(ok.value)
 
+    @classmethod
+    def reserve(cls, ctx: "Context", num_refs: int, layout: int = 2) -> "BVH":
+        """Storage for a BVH of num_refs references, to be filled by a copy or
+        broadcast of another BVH's arrays and then set_info (hp_bvh_reserve)."""
+        b = cls(ctx)
+        check(load().hp_bvh_reserve(ctx.h, C.byref(b.c), int(num_refs), int(layout)))
+        return b
+
+    def set_info(self, num_interior, num_leaf, scene_box, morton_scale, stream=None):
+        box = np.ascontiguousarray(scene_box, np.float32)
+        sc = np.ascontiguousarray(morton_scale, np.float32)
+        check(load().hp_bvh_set_info(self.ctx.h, C.byref(self.c), int(num_interior), int(num_leaf),
+                                     box.ctypes.data, sc.ctypes.data, _stream_ptr(stream)))
+
+    def info(self) -> dict:
+        """Node counts, scene box and Morton scale (after sync)."""
+        return {"num_interior": self.c.num_interior, "num_leaf": self.c.num_leaf,
+                "scene_box": list(self.c.scene_box), "morton_scale": list(self.c.morton_scale)}
+
+    def arrays(self):
+        """torch views (no copy) of the device arrays: nodes (capacity rows of
+        8 * layout int32), Woop rows (num_refs x 12 float32), triangle indices."""
+        import torch
+        cap = max(2 * max(self.c.capacity_refs, 2) - 1, 3)
+        n = self.c.num_refs
+        dev = torch.device("cuda", self.ctx.device)
+        return (torch.as_tensor(_DeviceArray(self.c.nodes, (cap, 8 * self.layout), "<i4"), device=dev),
+                torch.as_tensor(_DeviceArray(self.c.woop, (n, 12), "<f4"), device=dev),
+                torch.as_tensor(_DeviceArray(self.c.tri_indices, (n,), "<i4"), device=dev))
+
     def download(self, stream=None):
         """Copy nodes (N x 16 int32), woop (n x 12 float32) and triangle indices to the host."""
         self.sync(stream)
@@ -151,6 +181,15 @@ class BVH:
         check(load().hp_bvh_download(self.ctx.h, C.byref(self.c), nodes.ctypes.data, woop.ctypes.data,
                                      tri.ctypes.data, _stream_ptr(stream)))
         return nodes, woop, tri
+
+
+class _DeviceArray:
+    """A device buffer of the library described by __cuda_array_interface__ (so
+    torch.as_tensor can view it without a copy); the owner must outlive it."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"data": (int(ptr or 0), False), "shape": tuple(shape),
+                                         "typestr": typestr, "version": 3}
 
 
 def _mesh(verts, tris) -> hp_mesh:

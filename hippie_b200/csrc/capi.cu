@@ -162,6 +162,12 @@ float ord2f_host(uint32_t u) {
     return f;
 }
 
+uint32_t f2ord_host(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
 }  // namespace
 
 extern "C" {
@@ -310,6 +316,47 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
     hp_mark(ctx, s, "begin");
     HP_TRY(hp_lbvh_build(ctx, m, p, b, taps, s));
     if (ctx->arith == HP_ARITH_REFERENCE) HP_TRY(hp_woop_ref_launch(ctx, b, n, m, s));
+    return HP_OK;
+}
+
+hp_status hp_bvh_reserve(hp_ctx* ctx, hp_bvh* out, int64_t num_refs, int32_t layout) {
+    if (!ctx || !out) return hp_fail(HP_ERR_ARG, "hp_bvh_reserve: null argument");
+    if (num_refs < 0 || num_refs >= (int64_t(1) << 30)) return hp_fail(HP_ERR_ARG, "hp_bvh_reserve: num_refs out of range");
+    if (layout == 0) layout = HP_LAYOUT_BIN;
+    if (layout != HP_LAYOUT_BIN && layout != HP_LAYOUT_QUAD && layout != HP_LAYOUT_OCT)
+        return hp_fail(HP_ERR_ARG, "hp_bvh_reserve: layout must be 2, 4 or 8");
+    if (out->impl && reinterpret_cast<hp_bvh_impl*>(out->impl)->view)
+        return hp_fail(HP_ERR_ARG, "hp_bvh_reserve: the output is a view into a batch");
+    HP_TRY(bvh_alloc(out, num_refs, layout));
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(out->impl);
+    b->layout = layout;
+    out->layout = layout;
+    out->node_bytes = 32 * layout;
+    out->num_refs = num_refs;
+    out->num_interior = out->num_leaf = -1;
+    return HP_OK;
+}
+
+hp_status hp_bvh_set_info(hp_ctx* ctx, hp_bvh* bvh, int32_t num_interior, int32_t num_leaf,
+                          const float* scene_box6, const float* morton_scale3, void* stream) {
+    if (!ctx || !bvh || !bvh->impl || !scene_box6 || !morton_scale3)
+        return hp_fail(HP_ERR_ARG, "hp_bvh_set_info: null argument");
+    hp_bvh_impl* b = reinterpret_cast<hp_bvh_impl*>(bvh->impl);
+    const int64_t max_nodes = std::max<int64_t>(2 * std::max<int64_t>(bvh->num_refs, 2) - 1, 3);
+    if (num_interior < 0 || num_leaf < 0 || (int64_t)num_interior + num_leaf > max_nodes)
+        return hp_fail(HP_ERR_ARG, "hp_bvh_set_info: node counts do not fit the BVH");
+    hp_bvh_info info{};
+    info.num_interior = num_interior;
+    info.num_leaf = num_leaf;
+    for (int k = 0; k < 6; ++k) info.box_ord[k] = f2ord_host(scene_box6[k]);
+    for (int k = 0; k < 3; ++k) info.scale[k] = morton_scale3[k];
+    // pageable source: the call returns once the 48 bytes are staged
+    HP_CUDA(cudaMemcpyAsync(b->info, &info, sizeof(info), cudaMemcpyHostToDevice,
+                            reinterpret_cast<cudaStream_t>(stream)));
+    bvh->num_interior = num_interior;
+    bvh->num_leaf = num_leaf;
+    for (int k = 0; k < 6; ++k) bvh->scene_box[k] = scene_box6[k];
+    for (int k = 0; k < 3; ++k) bvh->morton_scale[k] = morton_scale3[k];
     return HP_OK;
 }
 

@@ -56,7 +56,7 @@ struct hp_ctx {
     size_t l2_bytes = 0;
     char* arena = nullptr;
     size_t arena_bytes = 0;
-    int* d_status = nullptr;       // [64] device error words and counters
+    int* d_status = nullptr;       // [64] device words: 0-1 error code and info, 16-17 trace ray counter, 20-23 hp_trace_host counters, 32 LBVH climb leaf ticket
     int* h_status = nullptr;       // pinned mirror
     bool profiling = false;
     hp_prof_mark* marks = nullptr; // event pool

@@ -181,23 +181,19 @@ __global__ void __launch_bounds__(TB) k_karras(const K* __restrict__ keys, int n
     range[i] = make_int2(min(i, j), max(i, j));
 }
 
-// One thread per sorted reference p (leaf node n-1+p): woopify its triangle,
-// store the leaf box, then climb. The second thread to reach a node merges
-// the children's boxes, sums sizes and evaluates the collapse rule of
-// computeNodeStatesAdaptive (BVHCollapserKernels.cu:58-136):
-//   leaf cost = ci*A, interior cost = ct*A + c(left) + c(right),
-//   state 0 (collapse into a leaf) iff ci*A*size < interior cost;
-// or, without adaptive leaves, computeNodeStates (:138-184): size <= maxLeafSize.
-// Node boxes keep the cost in min.w and the size (as int bits) in max.w.
-__global__ void __launch_bounds__(TB) k_climb(
+// Leaf records, one thread per sorted reference p (leaf node n-1+p): the Woop
+// rows of its triangle (HipBVH::woopifyTriangles, rt/bvh/HipBVHKernels.cu:35-65),
+// the leaf box (setupLeaves, rt/bvh/LBVHBuilderKernels.cu:162-195), its leaf
+// cost ci*A and size 1. Node boxes keep the cost in min.w and the size (as int
+// bits) in max.w. Coalesced stores; the triangle gather is the only random
+// access.
+__global__ void __launch_bounds__(TB) k_leaves(
     int n, const int32_t* __restrict__ sorted_tri, const float* __restrict__ verts, int64_t nv,
-    const int32_t* __restrict__ tris, const int* __restrict__ parent, const int* __restrict__ left,
-    const int* __restrict__ right, const int2* __restrict__ range, float4* nbmin, float4* nbmax,
-    float4* __restrict__ woop, int* counters, int* max_hi, uint8_t* state, float ct, float ci,
-    int adaptive, int max_leaf, int* err) {
+    const int32_t* __restrict__ tris, float4* __restrict__ nbmin, float4* __restrict__ nbmax,
+    float4* __restrict__ woop, float ci, int adaptive, int* err) {
     const int p = blockIdx.x * TB + threadIdx.x;
     if (p >= n) return;
-    const int tri = sorted_tri[p];
+    const int tri = __ldg(sorted_tri + p);
     tri_verts t = load_tri(verts, nv, tris, tri, err);
     float4 w0, w1, w2;
     hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
@@ -208,50 +204,209 @@ __global__ void __launch_bounds__(TB) k_climb(
           az = fminf(fminf(t.z0, t.z1), t.z2);
     float bx = fmaxf(fmaxf(t.x0, t.x1), t.x2), by = fmaxf(fmaxf(t.y0, t.y1), t.y2),
           bz = fmaxf(fmaxf(t.z0, t.z1), t.z2);
-    float cost = adaptive ? __fmul_rn(ci, hp_area(ax, ay, az, bx, by, bz)) : 0.0f;
-    const int leaf = n - 1 + p;
-    nbmin[leaf] = make_float4(ax, ay, az, cost);
-    nbmax[leaf] = make_float4(bx, by, bz, __int_as_float(1));
-    int node = parent[leaf];
+    const float cost = adaptive ? __fmul_rn(ci, hp_area(ax, ay, az, bx, by, bz)) : 0.0f;
+    nbmin[n - 1 + p] = make_float4(ax, ay, az, cost);
+    nbmax[n - 1 + p] = make_float4(bx, by, bz, __int_as_float(1));
+}
+
+// Bottom-up refit (refit, rt/bvh/LBVHBuilderKernels.cu:254-305). A thread
+// arriving first at a node leaves; the second merges the children's boxes,
+// sums sizes and evaluates the collapse rule of computeNodeStatesAdaptive
+// (BVHCollapserKernels.cu:58-136):
+//   leaf cost = ci*A, interior cost = ct*A + c(left) + c(right),
+//   state 0 (collapse into a leaf) iff ci*A*size < interior cost;
+// or, without adaptive leaves, computeNodeStates (:138-184): size <= maxLeafSize.
+//
+// Two phases, so that almost all memory traffic is coalesced. Every LBVH node
+// covers a contiguous range [lo, hi] of sorted leaves and its index lies in
+// that range; a CTA owning the CB = 512 leaves [base, base + CB) therefore owns every node
+// whose range lies inside its own ("local" nodes: their indices, children and
+// boxes are all in [base, base + CB)). Phase A (k_climb_local) loads the
+// CTA's node indices and leaf boxes with coalesced loads, climbs the local
+// nodes with shared-memory arrival counters and boxes (block-scope ordering),
+// and writes their boxes, states and maxHi words back with coalesced stores;
+// a thread whose next node is not local stops and appends its child to the
+// frontier list. (Computing the local nodes in barrier-separated rounds
+// instead was slower: the CTAs' local subtrees are deep.) Phase B
+// (k_climb_frontier) climbs from the frontier entries through the non-local
+// nodes (those whose ranges cross a CTA boundary: about depth per boundary)
+// with the global counters and one acq_rel atomic per arrival.
+constexpr int CB = 512;
+constexpr size_t CLIMB_SMEM = (size_t)CB * (4 * sizeof(float4) + 6 * sizeof(int) + sizeof(int2));
+
+struct climb_args {
+    int n;
+    const int* parent;
+    const int* left;
+    const int* right;
+    const int2* range;
+    float4* nbmin;
+    float4* nbmax;
+    int* counters;     // arrivals at non-local nodes (zeroed)
+    int* max_hi;       // maxHi words (initialised to -1)
+    uint8_t* state;
+    int* frontier;     // children whose parent is not local to their CTA
+    unsigned* frontier_count;
+    float ct, ci;
+    int adaptive, max_leaf;
+    int* err;
+};
+
+// Box, cost, size and state of a node from its left (l*) and right (r*) children.
+__device__ __forceinline__ int merge_node(const climb_args& A, float4 lmn, float4 lmx, float4 rmn, float4 rmx,
+                                          float4& omn, float4& omx) {
+    const float mnx = fminf(lmn.x, rmn.x), mny = fminf(lmn.y, rmn.y), mnz = fminf(lmn.z, rmn.z);
+    const float mxx = fmaxf(lmx.x, rmx.x), mxy = fmaxf(lmx.y, rmx.y), mxz = fmaxf(lmx.z, rmx.z);
+    const int size = __float_as_int(lmx.w) + __float_as_int(rmx.w);
+    int st;
+    float c;
+    if (A.adaptive) {
+        const float area = hp_area(mnx, mny, mnz, mxx, mxy, mxz);
+        const float c_int = __fadd_rn(__fmaf_rn(A.ct, area, lmn.w), rmn.w);
+        const float c_leaf = __fmul_rn(__fmul_rn(A.ci, area), (float)size);
+        st = (c_leaf < c_int) ? 0 : 1;
+        c = st ? c_int : c_leaf;
+    } else {
+        st = (size <= A.max_leaf) ? 0 : 1;
+        c = 0.0f;
+    }
+    omn = make_float4(mnx, mny, mnz, c);
+    omx = make_float4(mxx, mxy, mxz, __int_as_float(size));
+    return st;
+}
+
+__global__ void __launch_bounds__(CB, 4) k_climb_local(climb_args A) {
+    extern __shared__ __align__(16) unsigned char climb_smem[];
+    float4* s_imn = reinterpret_cast<float4*>(climb_smem);  // local interior node base + k
+    float4* s_imx = s_imn + CB;
+    float4* s_lmn = s_imx + CB;                             // leaf base + k
+    float4* s_lmx = s_lmn + CB;
+    int2* s_rng = reinterpret_cast<int2*>(s_lmx + CB);      // ranges of nodes base + k
+    int* s_cnt = reinterpret_cast<int*>(s_rng + CB);        // arrivals at local nodes
+    int* s_left = s_cnt + CB;
+    int* s_right = s_left + CB;
+    int* s_up = s_right + CB;                               // parents of nodes base + k
+    int* s_mh = s_up + CB;                                  // maxHi of positions base + k
+    int* s_st = s_mh + CB;                                  // state of local nodes
+    const int n = A.n;
+    const int base = blockIdx.x * CB, k = threadIdx.x, p = base + k;
+    const int last = min(base + CB, n) - 1;  // this CTA's last leaf
+    s_cnt[k] = 0;
+    s_mh[k] = -1;
+    if (p < n - 1) {
+        s_left[k] = __ldg(A.left + p);
+        s_right[k] = __ldg(A.right + p);
+        s_up[k] = __ldg(A.parent + p);
+        s_rng[k] = __ldg(A.range + p);
+    } else {
+        s_rng[k] = make_int2(-1, -1);  // not an interior node: never local
+    }
+    float4 cmn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), cmx = cmn;
+    int node = -1;
+    if (p < n) {
+        cmn = A.nbmin[n - 1 + p];
+        cmx = A.nbmax[n - 1 + p];
+        s_lmn[k] = cmn;
+        s_lmx[k] = cmx;
+        node = __ldg(A.parent + n - 1 + p);
+    }
+    __syncthreads();
+    int child = n - 1 + p;
     int guard = 0;
-    while (node >= 0) {
-        if (node >= n - 1 || ++guard > n) {  // a valid tree reaches the root within n steps
-            hp_report(err, HP_DEV_BAD_INDEX, node);
-            return;
+    while (p < n && node >= 0) {
+        const int kn = node - base;
+        const int2 rg = ((unsigned)kn < (unsigned)CB) ? s_rng[kn] : make_int2(-1, -1);
+        if (!(rg.x >= base && rg.y <= last && kn <= rg.y - base && kn >= rg.x - base)) {
+            // the next node's range crosses the CTA's: phase B continues from child
+            const unsigned slot = atomicAdd(A.frontier_count, 1u);
+            A.frontier[slot] = child;
+            break;
         }
-        __threadfence();
-        if (atomicAdd(&counters[node], 1) == 0) return;
-        __threadfence();
-        const int l = left[node], r = right[node];
-        if ((unsigned)l >= (unsigned)(2 * n - 1) || (unsigned)r >= (unsigned)(2 * n - 1)) {
-            hp_report(err, HP_DEV_BAD_INDEX, node);
-            return;
+        if (++guard > CB) {
+            hp_report(A.err, HP_DEV_BAD_INDEX, node);
+            break;
         }
-        const float4 lmn = __ldcg(nbmin + l), lmx = __ldcg(nbmax + l);
-        const float4 rmn = __ldcg(nbmin + r), rmx = __ldcg(nbmax + r);
-        const float mnx = fminf(lmn.x, rmn.x), mny = fminf(lmn.y, rmn.y), mnz = fminf(lmn.z, rmn.z);
-        const float mxx = fmaxf(lmx.x, rmx.x), mxy = fmaxf(lmx.y, rmx.y), mxz = fmaxf(lmx.z, rmx.z);
-        const int size = __float_as_int(lmx.w) + __float_as_int(rmx.w);
-        int st;
-        float c;
-        if (adaptive) {
-            const float area = hp_area(mnx, mny, mnz, mxx, mxy, mxz);
-            const float c_int = __fadd_rn(__fmaf_rn(ct, area, lmn.w), rmn.w);
-            const float c_leaf = __fmul_rn(__fmul_rn(ci, area), (float)size);
-            st = (c_leaf < c_int) ? 0 : 1;
-            c = st ? c_int : c_leaf;
-        } else {
-            st = (size <= max_leaf) ? 0 : 1;
-            c = 0.0f;
+        const int l = s_left[kn], r = s_right[kn];
+        if (l != child && r != child) {
+            hp_report(A.err, HP_DEV_BAD_INDEX, node);
+            break;
         }
-        __stcg(nbmin + node, make_float4(mnx, mny, mnz, c));
-        __stcg(nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
-        state[node] = (uint8_t)st;
-        if (st == 0 && node != 0) {
-            const int2 rg = range[node];
-            atomicMax(&max_hi[rg.x], rg.y);
+        const bool is_left = l == child;
+        const int sib = is_left ? r : l;
+        const int ks = (sib >= n - 1) ? sib - (n - 1) - base : sib - base;
+        if ((unsigned)ks >= (unsigned)CB) {
+            hp_report(A.err, HP_DEV_BAD_INDEX, node);
+            break;
         }
-        node = parent[node];
+        __threadfence_block();
+        if (atomicAdd(&s_cnt[kn], 1) == 0) break;
+        __threadfence_block();
+        const float4 smn = sib >= n - 1 ? s_lmn[ks] : s_imn[ks];
+        const float4 smx = sib >= n - 1 ? s_lmx[ks] : s_imx[ks];
+        float4 omn, omx;
+        const int st = is_left ? merge_node(A, cmn, cmx, smn, smx, omn, omx)
+                               : merge_node(A, smn, smx, cmn, cmx, omn, omx);
+        s_imn[kn] = omn;
+        s_imx[kn] = omx;
+        s_st[kn] = st;
+        if (st == 0 && node != 0) atomicMax(&s_mh[rg.x - base], rg.y);
+        cmn = omn;
+        cmx = omx;
+        child = node;
+        node = s_up[kn];
+    }
+    __syncthreads();
+    // write back the local nodes (index base + k) and the maxHi words of the
+    // CTA's positions; phase B raises maxHi further with global atomics
+    const int2 rg = s_rng[k];
+    if (p < n - 1 && rg.x >= base && rg.y <= last) {
+        __stcg(A.nbmin + p, s_imn[k]);
+        __stcg(A.nbmax + p, s_imx[k]);
+        A.state[p] = (uint8_t)s_st[k];
+    }
+    if (p < n && s_mh[k] >= 0) A.max_hi[p] = s_mh[k];
+}
+
+__global__ void __launch_bounds__(TB) k_climb_frontier(climb_args A) {
+    const unsigned count = *A.frontier_count;
+    const int n = A.n;
+    for (unsigned e = blockIdx.x * TB + threadIdx.x; e < count; e += gridDim.x * TB) {
+        int child = A.frontier[e];
+        if ((unsigned)child >= (unsigned)(2 * n - 1)) {
+            hp_report(A.err, HP_DEV_BAD_INDEX, child);
+            continue;
+        }
+        float4 cmn = __ldcg(A.nbmin + child), cmx = __ldcg(A.nbmax + child);
+        int node = __ldg(A.parent + child);
+        int guard = 0;
+        while (node >= 0) {
+            if (node >= n - 1 || ++guard > n) {
+                hp_report(A.err, HP_DEV_BAD_INDEX, node);
+                break;
+            }
+            const int l = __ldg(A.left + node), r = __ldg(A.right + node), up = __ldg(A.parent + node);
+            const int2 rg = __ldg(A.range + node);
+            if (hp_arrive(&A.counters[node]) == 0) break;
+            if ((unsigned)l >= (unsigned)(2 * n - 1) || (unsigned)r >= (unsigned)(2 * n - 1) ||
+                (l != child && r != child)) {
+                hp_report(A.err, HP_DEV_BAD_INDEX, node);
+                break;
+            }
+            const bool is_left = l == child;
+            const int sib = is_left ? r : l;
+            const float4 smn = __ldcg(A.nbmin + sib), smx = __ldcg(A.nbmax + sib);
+            float4 omn, omx;
+            const int st = is_left ? merge_node(A, cmn, cmx, smn, smx, omn, omx)
+                                   : merge_node(A, smn, smx, cmn, cmx, omn, omx);
+            __stcg(A.nbmin + node, omn);
+            __stcg(A.nbmax + node, omx);
+            A.state[node] = (uint8_t)st;
+            if (st == 0 && node != 0) atomicMax(&A.max_hi[rg.x], rg.y);
+            cmn = omn;
+            cmx = omx;
+            child = node;
+            node = up;
+        }
     }
 }
 
@@ -426,7 +581,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     } else {
         need += hp_carve::pad(nn * 4) + 2 * hp_carve::pad(n * 4) + hp_carve::pad(n * 8);  // parent, l, r, range
         need += 2 * hp_carve::pad(nn * 16);                   // node boxes
-        need += hp_carve::pad(n * 4) * 7 + hp_carve::pad(n);  // counters, maxhi, reach, flags, ranks, state
+        need += hp_carve::pad(n * 4) * 8 + hp_carve::pad(n);  // counters, maxhi, reach, flags, ranks, frontier, state
         need += 2 * hp_scan2_scratch_bytes(n + 1);
     }
     HP_TRY(hp_ctx_reserve(ctx, need, s));
@@ -534,6 +689,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     int* rank_int = cv.take<int>(n);
     int* rank_leaf = cv.take<int>(n);
     uint8_t* state = cv.take<uint8_t>(n);
+    int* frontier = cv.take<int>(n);
     void* scan_a = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
     void* scan_b = cv.take<char>(hp_scan2_scratch_bytes(n + 1));
 
@@ -553,9 +709,25 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     k_karras<K><<<grid_n, TB, 0, s>>>(skeys, (int)n, parent, left, right, range);
     hp_count_launch();
     hp_mark(ctx, s, "karras");
-    k_climb<<<grid_n, TB, 0, s>>>((int)n, out->tri_idx, m->vertices, m->num_vertices, m->triangles,
-                                  parent, left, right, range, nbmin, nbmax, out->woop, counters,
-                                  max_hi, state, p->ct, p->ci, p->adaptive_leaf, p->max_leaf_size, err);
+    k_leaves<<<grid_n, TB, 0, s>>>((int)n, out->tri_idx, m->vertices, m->num_vertices, m->triangles, nbmin,
+                                   nbmax, out->woop, p->ci, p->adaptive_leaf, err);
+    hp_count_launch();
+    hp_mark(ctx, s, "leaves");
+    {
+        climb_args A{(int)n, parent, left, right, range, nbmin, nbmax, counters, max_hi, state, frontier,
+                     reinterpret_cast<unsigned*>(ctx->d_status + 32), p->ct, p->ci, p->adaptive_leaf,
+                     p->max_leaf_size, err};
+        HP_CUDA(cudaMemsetAsync(A.frontier_count, 0, sizeof(unsigned), s));
+        HP_CUDA(cudaFuncSetAttribute(k_climb_local, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)CLIMB_SMEM));
+        k_climb_local<<<(unsigned)hp_div_up(n, CB), CB, CLIMB_SMEM, s>>>(A);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+        hp_mark(ctx, s, "climb_local");
+        k_climb_frontier<<<(unsigned)(ctx->sm_count * 8), TB, 0, s>>>(A);
+        HP_CUDA(cudaGetLastError());
+        hp_count_launch();
+    }
     hp_count_launch();
     hp_mark(ctx, s, "climb");
     if (wide) {  // N-wide layouts: references stay in sorted (= depth-first) order

@@ -222,6 +222,18 @@ hp_status hp_bvh_sync(hp_ctx* ctx, hp_bvh* bvh, void* stream);
 hp_status hp_bvh_download(hp_ctx* ctx, hp_bvh* bvh, void* nodes_host, void* woop_host,
                           int32_t* tri_host, void* stream);
 hp_status hp_bvh_free(hp_ctx* ctx, hp_bvh* bvh);
+/* Replicating a built BVH into another device's memory (one mesh, its rays
+ * split across GPUs): the receiver reserves storage for num_refs references
+ * in a layout, the sender's nodes, woop and tri_indices arrays are copied or
+ * broadcast into it (for example ncclBroadcast of the three device buffers),
+ * and the receiver then records the sender's node counts, scene box and
+ * Morton scale (from the sender's hp_bvh after hp_bvh_sync). The reference
+ * has no counterpart (HipBVH lives on one device, gpu/HipModule.cpp:19-50).
+ * hp_bvh_reserve allocates (or keeps storage of sufficient capacity) and
+ * leaves the contents undefined; hp_bvh_set_info is stream-ordered. */
+hp_status hp_bvh_reserve(hp_ctx* ctx, hp_bvh* out, int64_t num_refs, int32_t layout);
+hp_status hp_bvh_set_info(hp_ctx* ctx, hp_bvh* bvh, int32_t num_interior, int32_t num_leaf,
+                          const float* scene_box6, const float* morton_scale3, void* stream);
 /* SAH cost as HipBVH::getCost (sum over nodes of ct|ci*size times node area
  * over scene area), computed on the device and summed in a fixed order in
  * double precision, so repeated calls agree bit for bit. Synchronous. */

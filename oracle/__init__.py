@@ -55,6 +55,10 @@ _SIGS = {
     "or_brute64": (None, [_P, _P, C.c_int64, _P, C.c_int64, _P]),
     "or_adjoint64": (None, [_P, _P, _P, _P, _P, C.c_int64, _P]),
     "or_canonical": (C.c_int64, [_P, C.c_int64, _P, C.c_int64, _P, _P]),
+    "or_gen_uniform_mesh": (None, [C.c_uint64, C.c_int64, C.c_float, _P, _P]),
+    "or_gen_clustered_mesh": (None, [C.c_uint64, C.c_int64, C.c_int32, C.c_float, C.c_float, _P, _P]),
+    "or_gen_rays_targeted": (None, [C.c_uint64, C.c_int64, C.c_float, C.c_float, _P]),
+    "or_gen_rays_sphere": (None, [C.c_uint64, C.c_int64, _P, _P]),
 }
 
 
@@ -363,3 +367,34 @@ def canonical(nodes, tri_idx):
     if c < 0:
         raise ValueError("not a tree over these node and triangle arrays")
     return rows[:c], tris[:tri_idx.shape[0]]
+
+
+class gen:
+    """The benchmark's synthetic inputs, generated without the GPU library (the
+    same streams as hippie_b200.gen, checked equal byte for byte)."""
+
+    @staticmethod
+    def uniform_mesh(seed, n, half_extent=0.01):
+        v = np.empty((3 * n, 3), np.float32)
+        t = np.empty((n, 3), np.int32)
+        load().or_gen_uniform_mesh(seed, n, half_extent, _p(v), _p(t))
+        return v, t
+
+    @staticmethod
+    def clustered_mesh(seed, n, clusters=1024, sigma=0.02, half_extent=0.005):
+        v = np.empty((3 * n, 3), np.float32)
+        t = np.empty((n, 3), np.int32)
+        load().or_gen_clustered_mesh(seed, n, clusters, sigma, half_extent, _p(v), _p(t))
+        return v, t
+
+    @staticmethod
+    def rays_targeted(seed, n, lo=-0.5, hi=1.5):
+        r = np.empty((n, 8), np.float32)
+        load().or_gen_rays_targeted(seed, n, lo, hi, _p(r))
+        return r
+
+    @staticmethod
+    def rays_sphere(seed, n, box):
+        r = np.empty((n, 8), np.float32)
+        load().or_gen_rays_sphere(seed, n, _p(np.ascontiguousarray(box, np.float32)), _p(r))
+        return r

@@ -2241,3 +2241,92 @@ extern "C" int64_t or_canonical(const int32_t* nodes, int64_t num_nodes, const i
     }
     return count;
 }
+
+// ---- synthetic inputs, without the library ------------------------------------
+// The same streams as the library's generators (hippie_b200/csrc/gen.cpp), so
+// that the CPU arm of the benchmark builds its inputs without loading the GPU
+// library: a SplitMix64 finaliser over (seed, item, slot), uniforms
+// (h >> 40) * 2^-24, Box-Muller normals in double. tests/test_raygen.py checks
+// that both produce the same bytes.
+namespace {
+inline uint64_t gn_mix(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+inline float gn_u(uint64_t seed, uint64_t item, uint32_t slot) {
+    const uint64_t h = gn_mix((seed * 0xD1B54A32D192ED03ull) ^ (item * 64u + slot));
+    return (float)((double)(h >> 40) * (1.0 / 16777216.0));
+}
+inline double gn_normal(uint64_t seed, uint64_t item, uint32_t slot) {
+    const double a = 1.0 - (double)gn_u(seed, item, slot);
+    const double b = (double)gn_u(seed, item, slot + 1);
+    return std::sqrt(-2.0 * std::log(a)) * std::cos(6.283185307179586 * b);
+}
+}  // namespace
+
+extern "C" {
+
+void or_gen_uniform_mesh(uint64_t seed, int64_t n, float h, float* v, int32_t* t) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        float c[3];
+        for (int a = 0; a < 3; ++a) c[a] = gn_u(seed, i, a);
+        for (int k = 0; k < 3; ++k) {
+            for (int a = 0; a < 3; ++a) v[9 * i + 3 * k + a] = c[a] + (2.0f * gn_u(seed, i, 3 + 3 * k + a) - 1.0f) * h;
+            t[3 * i + k] = (int32_t)(3 * i + k);
+        }
+    }
+}
+
+void or_gen_clustered_mesh(uint64_t seed, int64_t n, int32_t clusters, float sigma, float h, float* v,
+                           int32_t* t) {
+    const uint64_t cseed = seed ^ 0xA5A5A5A55A5A5A5Aull;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t cl = i % clusters;
+        float c[3];
+        for (int a = 0; a < 3; ++a) c[a] = gn_u(cseed, cl, a) + (float)((double)sigma * gn_normal(seed, i, 2 * a));
+        for (int k = 0; k < 3; ++k) {
+            for (int a = 0; a < 3; ++a) v[9 * i + 3 * k + a] = c[a] + (2.0f * gn_u(seed, i, 8 + 3 * k + a) - 1.0f) * h;
+            t[3 * i + k] = (int32_t)(3 * i + k);
+        }
+    }
+}
+
+void or_gen_rays_targeted(uint64_t seed, int64_t n, float lo, float hi, float* rays) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        double o[3], d[3], len = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            o[a] = (double)(lo + (hi - lo) * gn_u(seed, i, a));
+            d[a] = (double)gn_u(seed, i, 3 + a) - o[a];
+            len += d[a] * d[a];
+        }
+        len = std::sqrt(len);
+        if (len == 0.0) { d[0] = 0.0; d[1] = 0.0; d[2] = 1.0; len = 1.0; }
+        float* r = rays + 8 * i;
+        r[0] = (float)o[0]; r[1] = (float)o[1]; r[2] = (float)o[2]; r[3] = 0.0f;
+        r[4] = (float)(d[0] / len); r[5] = (float)(d[1] / len); r[6] = (float)(d[2] / len);
+        r[7] = INFINITY;
+    }
+}
+
+void or_gen_rays_sphere(uint64_t seed, int64_t n, const float* box, float* rays) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        float* r = rays + 8 * i;
+        for (int a = 0; a < 3; ++a) r[a] = box[a] + (box[3 + a] - box[a]) * gn_u(seed, i, a);
+        r[3] = 0.0f;
+        const double z = 2.0 * (double)gn_u(seed, i, 3) - 1.0;
+        const double phi = 6.283185307179586 * (double)gn_u(seed, i, 4);
+        const double s = std::sqrt(std::max(0.0, 1.0 - z * z));
+        r[4] = (float)(s * std::cos(phi));
+        r[5] = (float)(s * std::sin(phi));
+        r[6] = (float)z;
+        r[7] = INFINITY;
+    }
+}
+
+}  // extern "C"

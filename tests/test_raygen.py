@@ -67,3 +67,21 @@ def test_halton():
     assert oracle.halton(3, 2) == np.float32(0.75)
     assert oracle.halton(1, 3) == np.float32(1 / 3)
     assert oracle.halton(0, 2) == 0
+
+
+def test_oracle_generators_equal_library_generators():
+    """The CPU arm of bench.py makes its inputs with oracle.gen (no GPU library);
+    they are the same bytes as hippie_b200.gen's."""
+    import oracle
+    for seed in (0xC0FFEE, 0xC0FFEE + 1, 7):
+        a, b = hp.gen.uniform_mesh(seed, 5003, 0.01), oracle.gen.uniform_mesh(seed, 5003, 0.01)
+        np.testing.assert_array_equal(a[0].view(np.int32), b[0].view(np.int32))
+        np.testing.assert_array_equal(a[1], b[1])
+        a, b = hp.gen.clustered_mesh(seed, 7001, 64, 0.02, 0.005), oracle.gen.clustered_mesh(seed, 7001, 64, 0.02, 0.005)
+        np.testing.assert_array_equal(a[0].view(np.int32), b[0].view(np.int32))
+        np.testing.assert_array_equal(a[1], b[1])
+        box = np.concatenate([a[0].min(0), a[0].max(0)]).astype(np.float32)
+        np.testing.assert_array_equal(hp.gen.rays_sphere(seed + 1, 9999, box).view(np.int32),
+                                      oracle.gen.rays_sphere(seed + 1, 9999, box).view(np.int32))
+        np.testing.assert_array_equal(hp.gen.rays_targeted(seed + 1, 9999, -0.5, 1.5).view(np.int32),
+                                      oracle.gen.rays_targeted(seed + 1, 9999, -0.5, 1.5).view(np.int32))
