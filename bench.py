@@ -225,8 +225,11 @@ def phase_rooflines(n, bits, phases, peak):
         add("scene box + boxes + Morton", 36 * n + n * (12 + 36 + kb + 4),
             sum(phases["boxes"]) + sum(phases["morton"]))
     if "sort_pass" in phases:
-        add(f"radix sort ({len(phases['sort_pass'])} passes)", n * passes * 2 * (kb + 4), sum(phases["sort_pass"]),
-            {"per_pass_ms": round(float(np.mean(phases["sort_pass"])), 5)})
+        seg = sum(phases.get("sort_segments", []))
+        name = (f"radix sort ({len(phases['sort_pass'])} passes + segment sort)" if seg > 0 else
+                f"radix sort ({len(phases['sort_pass'])} passes)")
+        add(name, n * passes * 2 * (kb + 4), sum(phases["sort_pass"]) + seg,
+            {"per_pass_ms": round(float(np.mean(phases["sort_pass"])), 5), "segments_ms": round(seg, 5)})
     if "climb" in phases:
         refit = 24 * (2 * n - 2) + 24 * (n - 1) + 8 * (n - 1) + 4 * (2 * n - 1) + 8 * (n - 1)
         local = sum(phases.get("climb_local", []))

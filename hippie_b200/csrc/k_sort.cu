@@ -280,6 +280,398 @@ constexpr size_t onesweep_smem() {
     return a > b ? a : b;
 }
 
+// ---- wide keys: top 24 bits by three LSD passes, then a sort of every segment ----
+// For keys of more than 48 bits, the full LSD sort is ceil(bits/8) passes over
+// global memory (8 for 60-bit Morton codes). Instead: three of those passes
+// order the keys stably by their top 24 sorted bits; the array is then a
+// sequence of segments of equal 24-bit prefix, each in input order, and most
+// segments are short (a 24-bit prefix of a Morton code is a cell of 1/256 of
+// the scene per axis). k_seg_sort gives every CTA the segments that start in
+// its window of SEG_WINDOW positions: one-key segments are copied, segments of
+// up to 32 keys are sorted by one warp each (a bitonic network over
+// (low bits, position), so equal keys keep their order), longer ones by the
+// whole CTA with stable 8-bit passes in shared memory. Every key is read and
+// written once more instead of five more times; the result equals the stable
+// sort by key. Segments larger than SEG_CAP (very uneven key distributions)
+// are listed and sorted by k_seg_big, one CTA per segment, with stable passes
+// through global memory.
+constexpr int SEG_BLOCK = 256, SEG_ITEMS = 8, SEG_CAP = SEG_BLOCK * SEG_ITEMS, SEG_WINDOW = 1536;
+constexpr int SEG_NW = SEG_BLOCK / 32;
+constexpr int SEG_RANK_MAX = 512;  // segments ranked element by element
+constexpr int64_t HYBRID_MIN_N = int64_t(1) << 20;
+
+__host__ __device__ constexpr bool hybrid_sort(int64_t n, int key_bytes, int bits) {
+    return key_bytes == 8 && bits > 48 && n >= HYBRID_MIN_N;
+}
+
+constexpr int SEG_TOP = 3;  // 8-bit digits ordered by global passes
+
+// Histograms of the SEG_TOP 8-bit digits at shifts s0, s0 + 8, ...
+__global__ void k_hist_top(const uint64_t* __restrict__ keys, int64_t n, int s0, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sh[256 * SEG_TOP];
+    for (int i = threadIdx.x; i < 256 * SEG_TOP; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys[i];
+#pragma unroll
+        for (int d = 0; d < SEG_TOP; ++d) atomicAdd(&sh[256 * d + ((uint32_t)(k >> (s0 + 8 * d)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256 * SEG_TOP; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// The prefix of a key: its bits [L, L + 8 * SEG_TOP) (bits above the sorted
+// width are not part of the order).
+__device__ __forceinline__ uint32_t seg_prefix(uint64_t k, int L) {
+    return (uint32_t)(k >> L) & ((1u << (8 * SEG_TOP)) - 1u);
+}
+
+// First position after the segment (run of equal prefix) holding `pos`; keys
+// are sorted by prefix.
+__device__ __forceinline__ int64_t seg_end(const uint64_t* __restrict__ keys, int64_t n, int64_t pos, int L) {
+    const uint32_t pre = seg_prefix(keys[pos], L);
+    int64_t lo = pos + 1, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (seg_prefix(keys[mid], L) > pre) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Stable rank of a block's SEG_CAP-element tile by the 8-bit digit at `shift`:
+// element e = warp * 32 * ITEMS + i * 32 + lane is key[i] of that lane. On
+// return pos[i] is its position in the tile sorted by digit (ties in element
+// order) and tot[d] the tile's count of digit d. cnt [SEG_NW][256] and
+// dstart [256] are shared scratch. Ends with a barrier.
+__device__ __forceinline__ void seg_block_rank(const uint64_t (&key)[SEG_ITEMS], int m, int shift,
+                                               uint16_t* cnt, uint32_t* dstart, uint32_t* tot,
+                                               uint32_t (&pos)[SEG_ITEMS]) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int i = tid; i < SEG_NW * 256; i += SEG_BLOCK) cnt[i] = 0;
+    __syncthreads();
+    uint16_t* wc = cnt + warp * 256;
+    uint32_t dg[SEG_ITEMS], rk[SEG_ITEMS];
+#pragma unroll
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        const int e = warp * 32 * SEG_ITEMS + i * 32 + lane;
+        const bool valid = e < m;
+        const uint32_t d = valid ? ((uint32_t)(key[i] >> shift) & 255u) : 0u;
+        uint32_t peers = __ballot_sync(HP_FULL_MASK, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t bal = __ballot_sync(HP_FULL_MASK, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
+        const uint32_t below = __popc(peers & lt);
+        const uint32_t c = valid ? wc[d] : 0u;
+        __syncwarp();
+        if (valid && below == 0) wc[d] = (uint16_t)(c + __popc(peers));
+        __syncwarp();
+        dg[i] = d;
+        rk[i] = c + below;
+    }
+    __syncthreads();
+    if (tid < 256) {  // per digit: exclusive offsets of the warps, and the digit's total
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < SEG_NW; ++w) {
+            const uint32_t c = cnt[w * 256 + tid];
+            cnt[w * 256 + tid] = (uint16_t)run;
+            run += c;
+        }
+        tot[tid] = run;
+        // exclusive scan of the totals over the 256 digits (8 warps)
+        uint32_t x = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(HP_FULL_MASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) dstart[256 + warp] = x;  // warp totals in dstart[256..263]
+        dstart[tid] = x - run;
+    }
+    __syncthreads();
+    if (tid < 256) {
+        uint32_t add = 0;
+        for (int w = 0; w < warp; ++w) add += dstart[256 + w];
+        dstart[tid] += add;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SEG_ITEMS; ++i) pos[i] = dstart[dg[i]] + cnt[warp * 256 + dg[i]] + rk[i];
+    __syncthreads();
+}
+
+struct seg_smem {
+    uint64_t key[2][SEG_CAP];
+    int32_t val[2][SEG_CAP];
+    uint16_t cnt[SEG_NW * 256];
+    uint32_t dstart[256 + 8];
+    uint32_t tot[256];
+    uint32_t part[SEG_BLOCK];
+    int2 med[SEG_CAP / (SEG_RANK_MAX + 1) + 1];  // segments longer than SEG_RANK_MAX keys
+    int64_t range[4];
+    int nseg, nmed;
+};
+
+// Sorts the low L bits of one segment held in S.key[0][0, m) (positions in
+// S.val[0]) with stable 8-bit passes in shared memory; returns the buffer
+// holding the result.
+__device__ int seg_block_sort(seg_smem& S, int m, int L) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int passes = (L + 7) / 8;
+    int src = 0;
+    for (int p = 0; p < passes; ++p) {
+        uint64_t key[SEG_ITEMS];
+        int32_t val[SEG_ITEMS];
+#pragma unroll
+        for (int i = 0; i < SEG_ITEMS; ++i) {
+            const int e = warp * 32 * SEG_ITEMS + i * 32 + lane;
+            key[i] = e < m ? S.key[src][e] : 0ull;
+            val[i] = e < m ? S.val[src][e] : 0;
+        }
+        uint32_t pos[SEG_ITEMS];
+        seg_block_rank(key, m, 8 * p, S.cnt, S.dstart, S.tot, pos);
+#pragma unroll
+        for (int i = 0; i < SEG_ITEMS; ++i) {
+            const int e = warp * 32 * SEG_ITEMS + i * 32 + lane;
+            if (e < m) {
+                S.key[1 - src][pos[i]] = key[i];
+                S.val[1 - src][pos[i]] = val[i];
+            }
+        }
+        __syncthreads();
+        src = 1 - src;
+    }
+    return src;
+}
+
+// Sorts in[cs, cs + m) (m <= SEG_CAP, whole segments of equal prefix) by the
+// low L bits within each segment and writes the result to out[cs, cs + m).
+// Segments of up to SEG_RANK_MAX keys (almost all of them) need no
+// coordination: every element finds its segment's bounds (its neighbours tell
+// a one-key segment; otherwise a binary search in shared memory), counts the
+// smaller (low bits, position) pairs in its segment and stores itself at
+// start + count. Longer segments are listed and sorted by the CTA with stable
+// 8-bit passes.
+__device__ void seg_sort_chunk(seg_smem& S, const uint64_t* __restrict__ kin, const int32_t* __restrict__ vin,
+                               uint64_t* __restrict__ kout, int32_t* __restrict__ vout, int64_t cs, int m,
+                               int L) {
+    const int tid = threadIdx.x;
+    const uint64_t low = (uint64_t(1) << L) - 1u;
+    for (int j = tid; j < m; j += SEG_BLOCK) {
+        S.key[0][j] = kin[cs + j];
+        S.val[0][j] = vin ? vin[cs + j] : (int32_t)(cs + j);
+    }
+    if (tid == 0) S.nmed = 0;
+    __syncthreads();
+    for (int c = tid; c < m; c += SEG_BLOCK) {
+        const uint64_t kc = S.key[0][c];
+        const uint32_t pc = seg_prefix(kc, L);
+        const bool first = c == 0 || seg_prefix(S.key[0][c - 1], L) != pc;
+        const bool last = c + 1 == m || seg_prefix(S.key[0][c + 1], L) != pc;
+        if (first && last) {  // a one-key segment is in place
+            kout[cs + c] = kc;
+            vout[cs + c] = S.val[0][c];
+            continue;
+        }
+        // the segment's bounds by binary search (the chunk is sorted by prefix)
+        int a = 0, e = c;
+        while (a < e) {
+            const int mid = (a + e) >> 1;
+            if (seg_prefix(S.key[0][mid], L) < pc) a = mid + 1;
+            else e = mid;
+        }
+        int b = c + 1, f = m;
+        while (b < f) {
+            const int mid = (b + f) >> 1;
+            if (seg_prefix(S.key[0][mid], L) > pc) f = mid;
+            else b = mid + 1;
+        }
+        if (b - a <= SEG_RANK_MAX) {
+            const uint64_t lc = kc & low;
+            int rank = 0;
+            for (int k = a; k < b; ++k) {
+                const uint64_t lk = S.key[0][k] & low;
+                rank += (lk < lc) || (lk == lc && k < c);
+            }
+            kout[cs + a + rank] = kc;
+            vout[cs + a + rank] = S.val[0][c];
+        } else if (a == c) {  // the first element of a longer segment lists it
+            const int q = atomicAdd(&S.nmed, 1);
+            S.med[q] = make_int2(a, b);
+        }
+    }
+    __syncthreads();
+    const int nmed = S.nmed;
+    for (int q = 0; q < nmed; ++q) {  // longer segments, one at a time by the CTA
+        const int a = S.med[q].x, sz = S.med[q].y - a;
+        __syncthreads();
+        for (int j = tid; j < sz; j += SEG_BLOCK) {
+            S.key[0][j] = kin[cs + a + j];
+            S.val[0][j] = j;
+        }
+        __syncthreads();
+        const int src = seg_block_sort(S, sz, L);
+        for (int j = tid; j < sz; j += SEG_BLOCK) {
+            const int from = a + S.val[src][j];
+            kout[cs + a + j] = kin[cs + from];
+            vout[cs + a + j] = vin ? vin[cs + from] : (int32_t)(cs + from);
+        }
+    }
+    __syncthreads();
+}
+
+// One CTA per window of SEG_WINDOW positions: the segments that start in it.
+// The window and the SEG_EXT positions after it are loaded once (coalesced);
+// the first segment start in the window and the first one after it are found
+// there. Only a segment running past the extension needs a binary search.
+constexpr int SEG_EXT = 256;
+constexpr int SEG_NONE = 0x7fffffff;
+
+__global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __restrict__ kin,
+                                                        const int32_t* __restrict__ vin,
+                                                        uint64_t* __restrict__ kout, int32_t* __restrict__ vout,
+                                                        int64_t n, int L, int2* big, uint32_t* big_count,
+                                                        int64_t big_cap, int* err) {
+    extern __shared__ __align__(16) unsigned char seg_raw[];
+    seg_smem& S = *reinterpret_cast<seg_smem*>(seg_raw);
+    const int tid = threadIdx.x;
+    const int64_t wb = (int64_t)blockIdx.x * SEG_WINDOW;
+    const int64_t we = min(wb + SEG_WINDOW, n);
+    const int64_t lo = wb > 0 ? wb - 1 : 0, hi = min(we + SEG_EXT, n);
+    int* first = reinterpret_cast<int*>(&S.range[2]);  // [0] first start in the window, [1] first after it
+    if (tid == 0) { first[0] = SEG_NONE; first[1] = SEG_NONE; }
+    for (int64_t j = lo + tid; j < hi; j += SEG_BLOCK) S.key[1][j - lo] = kin[j];
+    __syncthreads();
+    for (int64_t j = wb + tid; j < hi; j += SEG_BLOCK) {
+        const bool start = j == 0 || seg_prefix(S.key[1][j - lo], L) != seg_prefix(S.key[1][j - 1 - lo], L);
+        if (start) {
+            if (j < we) atomicMin(&first[0], (int)(j - wb));
+            else atomicMin(&first[1], (int)(j - we));
+        }
+    }
+    __syncthreads();
+    if (first[0] == SEG_NONE) return;  // a segment that started earlier covers the window
+    if (tid == 0) {
+        const int64_t cs = wb + first[0];
+        int64_t ce;
+        if (we == n) ce = n;
+        else if (first[1] != SEG_NONE) ce = we + first[1];
+        else if (hi == n) ce = n;
+        else ce = seg_end(kin, n, we - 1, L);  // the last segment runs past the extension
+        S.range[0] = cs;
+        S.range[1] = ce;
+    }
+    __syncthreads();
+    const int64_t cs = S.range[0], ce = S.range[1];
+    if (ce - cs <= SEG_CAP) {
+        seg_sort_chunk(S, kin, vin, kout, vout, cs, (int)(ce - cs), L);
+        return;
+    }
+    // A large run: batches of whole segments up to SEG_CAP keys; a segment
+    // larger than that goes to the list k_seg_big sorts.
+    int64_t cur = cs;
+    while (cur < ce) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t e1 = seg_end(kin, n, cur, L);
+            if (e1 - cur > SEG_CAP) {
+                const uint32_t slot = atomicAdd(big_count, 1u);
+                if ((int64_t)slot < big_cap) big[slot] = make_int2((int)cur, (int)e1);
+                else hp_report(err, HP_DEV_BAD_INDEX, (int)cur);
+                S.range[2] = e1;
+                S.range[3] = e1;  // nothing to sort here
+            } else {
+                int64_t be = e1;
+                while (be < ce) {
+                    const int64_t e2 = seg_end(kin, n, be, L);
+                    if (e2 - cur > SEG_CAP) break;
+                    be = e2;
+                }
+                S.range[2] = cur;
+                S.range[3] = be;
+            }
+        }
+        __syncthreads();
+        const int64_t b0 = S.range[2], b1 = S.range[3];
+        if (b1 > b0) seg_sort_chunk(S, kin, vin, kout, vout, b0, (int)(b1 - b0), L);
+        cur = b1;
+    }
+}
+
+// Segments larger than SEG_CAP: one CTA each, stable 8-bit passes over the
+// low L bits through global memory, tiles in order with running digit
+// offsets; the input and output ranges serve as the two buffers.
+__global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_big(uint64_t* kin, int32_t* vin_buf, const int32_t* vin,
+                                                       uint64_t* kout, int32_t* vout, int L, const int2* big,
+                                                       const uint32_t* big_count, int64_t big_cap) {
+    extern __shared__ __align__(16) unsigned char seg_raw[];
+    seg_smem& S = *reinterpret_cast<seg_smem*>(seg_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t count = min((int64_t)*big_count, big_cap);
+    const int passes = (L + 7) / 8;
+    for (int64_t g = blockIdx.x; g < count; g += gridDim.x) {
+        const int64_t s0 = big[g].x, s1 = big[g].y;
+        // the first pass reads the input buffers, then output and input
+        // ranges alternate; an even pass count ends with a copy to the output
+        for (int p = 0; p < passes; ++p) {
+            const bool to_out = (p & 1) == 0;
+            const uint64_t* ks = to_out ? kin : kout;
+            uint64_t* kd = to_out ? kout : kin;
+            const int32_t* vs = p == 0 ? vin : (to_out ? vin_buf : vout);
+            int32_t* vd = to_out ? vout : vin_buf;
+            const int shift = 8 * p;
+            // digit histogram of the segment, exclusive offsets
+            if (tid < 256) S.tot[tid] = 0;
+            __syncthreads();
+            for (int64_t j = s0 + tid; j < s1; j += SEG_BLOCK) atomicAdd(&S.tot[(uint32_t)(ks[j] >> shift) & 255u], 1u);
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t run = 0;
+                for (int d = 0; d < 256; ++d) { const uint32_t c = S.tot[d]; S.part[d] = run; run += c; }
+            }
+            __syncthreads();
+            for (int64_t t0 = s0; t0 < s1; t0 += SEG_CAP) {
+                const int m = (int)min((int64_t)SEG_CAP, s1 - t0);
+                uint64_t key[SEG_ITEMS];
+                int32_t val[SEG_ITEMS];
+#pragma unroll
+                for (int i = 0; i < SEG_ITEMS; ++i) {
+                    const int e = warp * 32 * SEG_ITEMS + i * 32 + lane;
+                    key[i] = e < m ? ks[t0 + e] : 0ull;
+                    val[i] = e < m ? (vs ? vs[t0 + e] : (int32_t)(t0 + e)) : 0;
+                }
+                uint32_t pos[SEG_ITEMS];
+                seg_block_rank(key, m, shift, S.cnt, S.dstart, S.tot, pos);
+#pragma unroll
+                for (int i = 0; i < SEG_ITEMS; ++i) {
+                    const int e = warp * 32 * SEG_ITEMS + i * 32 + lane;
+                    if (e < m) {
+                        const uint32_t d = (uint32_t)(key[i] >> shift) & 255u;
+                        const int64_t o = s0 + S.part[d] + (pos[i] - S.dstart[d]);
+                        kd[o] = key[i];
+                        vd[o] = val[i];
+                    }
+                }
+                __syncthreads();
+                if (tid < 256) S.part[tid] += S.tot[tid];
+                __syncthreads();
+            }
+        }
+        if ((passes & 1) == 0) {  // the last pass wrote the input range
+            for (int64_t j = s0 + tid; j < s1; j += SEG_BLOCK) {
+                kout[j] = kin[j];
+                vout[j] = vin_buf[j];
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename K, int BLOCK>
 hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream_t stream) {
     constexpr int ITEMS = sort_cfg<K>::ITEMS;
@@ -306,6 +698,50 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const K* kin = reinterpret_cast<const K*>(a.keys_in);
     const int32_t* vin = a.vals_in;
+    if constexpr (sizeof(K) == 8) {
+        if (hybrid_sort(n, 8, plan.bits)) {
+            // top 24 bits by three LSD passes, then every segment of equal prefix
+            const int s0 = plan.bits - 8 * SEG_TOP;
+            HP_CUDA(cudaMemsetAsync(a.hist, 0, 256 * SEG_TOP * sizeof(uint32_t), stream));
+            k_hist_top<<<std::max(1, (int)std::min<int64_t>(hp_div_up(n, 1024), 148 * 8)), 1024, 0, stream>>>(
+                kin, n, s0, a.hist);
+            HP_CUDA(cudaGetLastError());
+            hp_count_launch();
+            const uint32_t sl = a.ctx ? a.ctx->sort_spin_limit : LOOKBACK_SPIN_LIMIT;
+            const K* src_k = kin;
+            const int32_t* src_v = vin;
+            for (int d = 0; d < SEG_TOP; ++d) {  // in -> A -> B -> A
+                K* dk = (d & 1) ? kB : kA;
+                int32_t* dv = (d & 1) ? vB : vA;
+                k_onesweep<K, BLOCK, ITEMS><<<(unsigned)plan.tiles, BLOCK, smem, stream>>>(
+                    src_k, src_v, dk, dv, n, s0 + 8 * d, 0xffu, a.hist + 256 * d,
+                    status + (size_t)d * plan.tiles * 256, counters + d, a.status, sl);
+                HP_CUDA(cudaGetLastError());
+                hp_count_launch();
+                hp_mark(a.ctx, stream, "sort_pass");
+                src_k = dk;
+                src_v = dv;
+            }
+            uint64_t* sk = const_cast<uint64_t*>(reinterpret_cast<const uint64_t*>(src_k));
+            int32_t* sv = const_cast<int32_t*>(src_v);
+            uint32_t* big_count = counters + 32;  // zeroed with the status words
+            const int64_t big_cap = n / (SEG_CAP + 1) + 1;
+            int2* big = reinterpret_cast<int2*>(cv.take<int2>((size_t)big_cap));
+            const size_t seg_bytes = sizeof(seg_smem);
+            HP_CUDA(cudaFuncSetAttribute(k_seg_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_bytes));
+            HP_CUDA(cudaFuncSetAttribute(k_seg_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seg_bytes));
+            k_seg_sort<<<(unsigned)hp_div_up(n, SEG_WINDOW), SEG_BLOCK, seg_bytes, stream>>>(
+                sk, sv, reinterpret_cast<uint64_t*>(a.keys_out), a.vals_out, n, s0, big, big_count, big_cap,
+                a.status);
+            HP_CUDA(cudaGetLastError());
+            k_seg_big<<<(unsigned)std::min<int64_t>(big_cap, 296), SEG_BLOCK, seg_bytes, stream>>>(
+                sk, sv, sv, reinterpret_cast<uint64_t*>(a.keys_out), a.vals_out, s0, big, big_count, big_cap);
+            HP_CUDA(cudaGetLastError());
+            hp_count_launch(2);
+            hp_mark(a.ctx, stream, "sort_segments");
+            return HP_OK;
+        }
+    }
     for (int p = 0; p < plan.passes; ++p) {
         K* kout;
         int32_t* vout;
@@ -469,6 +905,8 @@ hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block) {
     p.tiles = std::max<int64_t>(1, (n + p.tile - 1) / p.tile);
     size_t kv = hp_carve::pad((size_t)n * key_bytes) + hp_carve::pad((size_t)n * 4);
     p.scratch_bytes = 2 * kv + hp_carve::pad(((size_t)p.passes * p.tiles * 256 + 64) * 4);
+    if (hybrid_sort(n, key_bytes, bits))  // the list of segments too large for one CTA's shared memory
+        p.scratch_bytes += hp_carve::pad((size_t)(n / (SEG_CAP + 1) + 1) * 8);
     return p;
 }
 
