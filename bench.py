@@ -18,8 +18,10 @@ e2e        the same metrics through the C ABI with pinned host buffers: the
            counts), then hp_trace_host over the host ray and result buffers
            (every ray uploaded and every hit record downloaded, in chunks whose
            copies overlap the traces of their neighbours).
-roofline   the radix-sort pass (the build's HBM-bound kernel): algorithmic
-           bytes n * 2 * (K + 4) per pass over its average CUDA-event duration;
+roofline   the radix-sort phase of the build (HBM-bound): the survey's algorithmic
+           bytes n * P * 2 * (K + 4) (P = ceil(bits / 8) LSD passes) over the
+           summed CUDA-event durations of its kernels (for 60-bit keys three
+           LSD passes and the segment sort);
            roofline.phases gives every HBM-bound build phase with the survey's
            algorithmic bytes (scene box + boxes + Morton, the sort), and
            large.roofline_phases_lbvh the same plus the refit climb on the
@@ -867,12 +869,15 @@ def main(argv=None):
     phases_l = profile_phases(ctx, build_step)
     phases = {k: sum(x) for k, x in phases_l.items()}
     passes = phases_l.get("sort_pass", [])
+    seg_ms = sum(phases_l.get("sort_segments", []))
     kb = 4 if cfg["bits"] <= 32 else 8
-    pass_bytes = n * 2 * (kb + 4)
+    lsd_passes = (cfg["bits"] + 7) // 8
+    sort_bytes = n * lsd_passes * 2 * (kb + 4)   # the survey's n * P * 2 * (K + 4)
+    sort_ms = sum(passes) + seg_ms
     pass_ms = float(np.mean(passes)) if passes else float("nan")
-    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    achieved = sort_bytes / (sort_ms * 1e-3) / 1e9
     peak, peak_kind = peak_hbm()
-    traffic = committed_traffic("sort_pass")
+    traffic = committed_traffic("sort_phase")
     parallelism = (f"replicas x{world}" if mode == "replicas" else
                    f"rays x{world}, BVH " + ("broadcast from rank 0 (NCCL)" if bcast else "built on every rank"))
 
@@ -895,10 +900,15 @@ def main(argv=None):
                 "h2d_bytes_per_step": int(world * (v.nbytes + t.nbytes) + job_rays * 32),
                 "d2h_bytes_per_step": int(job_rays * 16 + 8 * world)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "k_onesweep (radix sort pass)", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": pass_bytes,
-                     "launch_ms": pass_ms, "phases": phase_rooflines(n, cfg["bits"], phases_l, peak)},
+        "roofline": {"bound": "hbm",
+                     "kernel": (f"radix sort phase: {len(passes)} LSD passes (k_onesweep)" +
+                                (" + segment sort (k_seg_sort, k_seg_big)" if seg_ms > 0 else "")),
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": sort_bytes,
+                     "algorithmic_bytes": f"n * {lsd_passes} * 2 * ({kb} + 4): the 8-bit LSD sort's key and value "
+                                          "reads and writes (survey formula), n = triangles",
+                     "launch_ms": sort_ms, "per_pass_ms": pass_ms, "segments_ms": seg_ms,
+                     "phases": phase_rooflines(n, cfg["bits"], phases_l, peak)},
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

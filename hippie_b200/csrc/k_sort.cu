@@ -298,6 +298,7 @@ constexpr size_t onesweep_smem() {
 constexpr int SEG_BLOCK = 256, SEG_ITEMS = 8, SEG_CAP = SEG_BLOCK * SEG_ITEMS, SEG_WINDOW = 1536;
 constexpr int SEG_NW = SEG_BLOCK / 32;
 constexpr int SEG_RANK_MAX = 512;  // segments ranked element by element
+constexpr int SEG_MED_CAP = SEG_CAP / (SEG_RANK_MAX + 1) + 1;  // longer segments in one chunk
 constexpr int64_t HYBRID_MIN_N = int64_t(1) << 20;
 
 __host__ __device__ constexpr bool hybrid_sort(int64_t n, int key_bytes, int bits) {
@@ -412,7 +413,7 @@ struct seg_smem {
     uint32_t dstart[256 + 8];
     uint32_t tot[256];
     uint32_t part[SEG_BLOCK];
-    int2 med[SEG_CAP / (SEG_RANK_MAX + 1) + 1];  // segments longer than SEG_RANK_MAX keys
+    int2 med[SEG_MED_CAP];  // segments longer than SEG_RANK_MAX keys
     int64_t range[4];
     int nseg, nmed;
 };
@@ -457,9 +458,12 @@ __device__ int seg_block_sort(seg_smem& S, int m, int L) {
 // smaller (low bits, position) pairs in its segment and stores itself at
 // start + count. Longer segments are listed and sorted by the CTA with stable
 // 8-bit passes.
+// Every index is checked against the chunk: inputs whose prefixes are not in
+// order (only after an earlier pass gave up a bounded wait, which is reported)
+// must not make it read or write outside the chunk.
 __device__ void seg_sort_chunk(seg_smem& S, const uint64_t* __restrict__ kin, const int32_t* __restrict__ vin,
                                uint64_t* __restrict__ kout, int32_t* __restrict__ vout, int64_t cs, int m,
-                               int L) {
+                               int L, int* err) {
     const int tid = threadIdx.x;
     const uint64_t low = (uint64_t(1) << L) - 1u;
     for (int j = tid; j < m; j += SEG_BLOCK) {
@@ -502,14 +506,16 @@ __device__ void seg_sort_chunk(seg_smem& S, const uint64_t* __restrict__ kin, co
             vout[cs + a + rank] = S.val[0][c];
         } else if (a == c) {  // the first element of a longer segment lists it
             const int q = atomicAdd(&S.nmed, 1);
-            S.med[q] = make_int2(a, b);
+            if (q < SEG_MED_CAP) S.med[q] = make_int2(a, b);
+            else hp_report(err, HP_DEV_BAD_INDEX, (int)(cs + c));
         }
     }
     __syncthreads();
-    const int nmed = S.nmed;
+    const int nmed = min(S.nmed, SEG_MED_CAP);
     for (int q = 0; q < nmed; ++q) {  // longer segments, one at a time by the CTA
         const int a = S.med[q].x, sz = S.med[q].y - a;
         __syncthreads();
+        if (a < 0 || sz <= 0 || a + sz > m) continue;  // uniform: every thread reads the same entry
         for (int j = tid; j < sz; j += SEG_BLOCK) {
             S.key[0][j] = kin[cs + a + j];
             S.val[0][j] = j;
@@ -569,7 +575,7 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
     __syncthreads();
     const int64_t cs = S.range[0], ce = S.range[1];
     if (ce - cs <= SEG_CAP) {
-        seg_sort_chunk(S, kin, vin, kout, vout, cs, (int)(ce - cs), L);
+        seg_sort_chunk(S, kin, vin, kout, vout, cs, (int)(ce - cs), L, err);
         return;
     }
     // A large run: batches of whole segments up to SEG_CAP keys; a segment
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
         }
         __syncthreads();
         const int64_t b0 = S.range[2], b1 = S.range[3];
-        if (b1 > b0) seg_sort_chunk(S, kin, vin, kout, vout, b0, (int)(b1 - b0), L);
+        if (b1 > b0) seg_sort_chunk(S, kin, vin, kout, vout, b0, (int)(b1 - b0), L, err);
         cur = b1;
     }
 }
@@ -608,7 +614,8 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
 // offsets; the input and output ranges serve as the two buffers.
 __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_big(uint64_t* kin, int32_t* vin_buf, const int32_t* vin,
                                                        uint64_t* kout, int32_t* vout, int L, const int2* big,
-                                                       const uint32_t* big_count, int64_t big_cap) {
+                                                       const uint32_t* big_count, int64_t big_cap, int64_t n,
+                                                       int* err) {
     extern __shared__ __align__(16) unsigned char seg_raw[];
     seg_smem& S = *reinterpret_cast<seg_smem*>(seg_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -616,6 +623,10 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_big(uint64_t* kin, int32_t
     const int passes = (L + 7) / 8;
     for (int64_t g = blockIdx.x; g < count; g += gridDim.x) {
         const int64_t s0 = big[g].x, s1 = big[g].y;
+        if (s0 < 0 || s1 > n || s0 >= s1) {
+            if (threadIdx.x == 0) hp_report(err, HP_DEV_BAD_INDEX, (int)g);
+            continue;
+        }
         // the first pass reads the input buffers, then output and input
         // ranges alternate; an even pass count ends with a copy to the output
         for (int p = 0; p < passes; ++p) {
@@ -653,8 +664,12 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_big(uint64_t* kin, int32_t
                     if (e < m) {
                         const uint32_t d = (uint32_t)(key[i] >> shift) & 255u;
                         const int64_t o = s0 + S.part[d] + (pos[i] - S.dstart[d]);
-                        kd[o] = key[i];
-                        vd[o] = val[i];
+                        if (o >= s0 && o < s1) {  // always, unless ranges listed twice overlap
+                            kd[o] = key[i];
+                            vd[o] = val[i];
+                        } else {
+                            hp_report(err, HP_DEV_BAD_INDEX, (int)g);
+                        }
                     }
                 }
                 __syncthreads();
@@ -735,7 +750,8 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
                 a.status);
             HP_CUDA(cudaGetLastError());
             k_seg_big<<<(unsigned)std::min<int64_t>(big_cap, 296), SEG_BLOCK, seg_bytes, stream>>>(
-                sk, sv, sv, reinterpret_cast<uint64_t*>(a.keys_out), a.vals_out, s0, big, big_count, big_cap);
+                sk, sv, sv, reinterpret_cast<uint64_t*>(a.keys_out), a.vals_out, s0, big, big_count, big_cap, n,
+                a.status);
             HP_CUDA(cudaGetLastError());
             hp_count_launch(2);
             hp_mark(a.ctx, stream, "sort_segments");
