@@ -62,6 +62,9 @@ CONFIGS = {
                    mesh="clustered", n=4194304, rays=16777216, bits=60, method="ploc", config_id=1),
     "lbvh64k": dict(workload="uniform 65,536 tris, 1,048,576 targeted rays, 30-bit", mesh="uniform",
                     n=65536, rays=1048576, bits=30, method="lbvh", config_id=0),
+    # the headline scene built as an LBVH (for profiling the refit climb)
+    "lbvh4m": dict(workload="clustered 4,194,304 tris (1024 clusters), 16,777,216 sphere rays, 60-bit, LBVH",
+                   mesh="clustered", n=4194304, rays=16777216, bits=60, method="lbvh", config_id=1),
 }
 DEFAULT_CONFIG = "ploc4m"
 
