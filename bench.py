@@ -314,7 +314,8 @@ def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2, rank=0, world=1)
     the uniform generator; 4 rays per triangle, origins uniform in [-0.5,1.5]^3,
     directions uniform on the sphere) against the same meshes and rays built and
     traced one mesh at a time through the plain path: as host-loop launches, and
-    with those per-mesh launches captured into one CUDA graph. Under torchrun
+    with those per-mesh launches captured into one CUDA graph. The launch
+    choices are autotuned on the batch first and used by both. Under torchrun
     the meshes are split across ranks by LPT (no data-path collective) and the
     times are the max over ranks."""
     import torch
@@ -351,6 +352,30 @@ def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2, rank=0, world=1)
     batch = hp.Batch(ctx, meshes, counts, p)
     with torch.cuda.stream(s):
         plain()  # allocates every per-mesh BVH once
+        batch.build_trace(R, results=res_batch)
+        torch.cuda.synchronize()
+        ctx.check()
+        # Autotuned launch choices for this batch (result-neutral): the sort CTA
+        # size, the tracer's CTAs per SM and shared-stack depth, timed on the
+        # batched build + trace itself (direct launches: a CUDA graph keeps the
+        # launch choices it was captured with); the per-mesh baseline below
+        # uses the same choices. Ray-order tracing is not a batch option.
+        cand = [dict(sort_block=sb, trace_stack=st, trace_ctas_per_sm=ct, trace_sorted=0)
+                for sb in (512, 256) for st in (8, 16, 32) for ct in (0, 6, 4)]
+        times = []
+        for c in cand:
+            ctx.set_tune(**c)
+            batch.build_trace(R, results=res_batch, graph=False)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            batch.build_trace(R, results=res_batch, graph=False)
+            e1.record(s)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        tuned = cand[int(np.argmin(times))]
+        ctx.set_tune(**tuned)
+        batch.close()  # a fresh batch captures its graph with the tuned choices
+        batch = hp.Batch(ctx, meshes, counts, p)
         batch.build_trace(R, results=res_batch)
         torch.cuda.synchronize()
         ctx.check()
@@ -398,9 +423,12 @@ def extra_batched(ctx, steps=3, num_meshes=2048, seed=SEED + 2, rank=0, world=1)
            "speedup_vs_plain_host_loop": t_loop / t_batch, "speedup_vs_plain_graph": t_graph / t_batch,
            "batched_build_ms": t_build, "batched_trace_ms": t_trace,
            "batched_mtris_s": tris / t_batch / 1e3, "batched_mrays_s": rays / t_batch / 1e3,
-           "results_identical": bad == 0.0, "sharding": f"LPT over {world} rank(s), max over ranks"}
+           "results_identical": bad == 0.0, "sharding": f"LPT over {world} rank(s), max over ranks",
+           "autotuned": {"choice": tuned, "candidates": len(cand),
+                         "applied": "batched and per-mesh runs use the chosen launch choices"}}
     del g
     batch.close()
+    ctx.reset_tune()
     return out
 
 
