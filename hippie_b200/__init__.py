@@ -362,6 +362,16 @@ class Context:
         """Spins of one radix-sort look-back wait before it gives up (0: the default)."""
         check(load().hp_ctx_set_sort_spin_limit(self.h, int(spins)))
 
+    def set_checked(self, on: bool = True):
+        """Checked mode (hp_ctx_set_checked): every call synchronises and verifies
+        its output (BVH validation after build and refit, sortedness after a
+        sort, the device error words after a trace), raising HippieError."""
+        check(load().hp_ctx_set_checked(self.h, 1 if on else 0))
+
+    @property
+    def checked(self) -> bool:
+        return bool(load().hp_ctx_get_checked(self.h))
+
     def radix_sort(self, keys, vals=None, bits=None, stream=None):
         import torch
         kb = keys.element_size()

@@ -125,6 +125,8 @@ _SIGS = {
     "hp_radix_sort_noalloc": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "hp_ctx_set_sort_spin_limit": (C.c_int, [_P, C.c_uint32]),
     "hp_ctx_set_arithmetic": (C.c_int, [_P, C.c_int32]),
+    "hp_ctx_set_checked": (C.c_int, [_P, C.c_int32]),
+    "hp_ctx_get_checked": (C.c_int32, [_P]),
     "hp_bvh_reserve": (C.c_int, [_P, C.POINTER(hp_bvh), C.c_int64, C.c_int32]),
     "hp_bvh_set_info": (C.c_int, [_P, C.POINTER(hp_bvh), C.c_int32, C.c_int32, _P, _P, _P]),
     "hp_env_create": (C.c_int, [C.POINTER(C.c_void_p)]),

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -170,6 +171,36 @@ uint32_t f2ord_host(float f) {
 
 }  // namespace
 
+bool hp_checking(const hp_ctx* ctx, cudaStream_t s) {
+    if (!ctx->checked) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return false;
+    return cs == cudaStreamCaptureStatusNone;
+}
+
+namespace {
+
+// Checked mode after a build or refit: the device error words, the node counts
+// against the reference count, and the HipBVH::validate invariants
+// (rt/bvh/HipBVH.cpp:157-307) over the whole tree.
+hp_status checked_bvh(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, cudaStream_t s, const char* who) {
+    HP_TRY(hp_bvh_sync(ctx, bvh, s));
+    const int64_t n = bvh->num_refs;
+    const int64_t ni = bvh->num_interior, nl = bvh->num_leaf;
+    if (ni < 0 || nl < 1 || nl > std::max<int64_t>(n, 2) || ni + nl > 2 * n + 1)
+        return hp_fail(HP_ERR_DEVICE_STATUS, std::string("checked mode: ") + who + " produced " +
+                                                 std::to_string(ni) + " interior nodes and " + std::to_string(nl) +
+                                                 " leaves for " + std::to_string(n) + " references");
+    int32_t valid = 0;
+    HP_TRY(hp_bvh_validate(ctx, bvh, m, &valid, s));
+    if (!valid)
+        return hp_fail(HP_ERR_DEVICE_STATUS, std::string("checked mode: ") + who +
+                                                 " produced a BVH that fails validation");
+    return HP_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* hp_last_error(void) { return g_last_error.c_str(); }
@@ -201,6 +232,14 @@ hp_status hp_profile_get(hp_ctx* ctx, int32_t i, char* name, int64_t name_size, 
     return HP_OK;
 }
 
+hp_status hp_ctx_set_checked(hp_ctx* ctx, int32_t on) {
+    if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_set_checked: null context");
+    ctx->checked = on != 0;
+    return HP_OK;
+}
+
+int32_t hp_ctx_get_checked(const hp_ctx* ctx) { return ctx && ctx->checked ? 1 : 0; }
+
 hp_status hp_ctx_create(hp_ctx** out, int32_t device) {
     if (!out) return hp_fail(HP_ERR_ARG, "hp_ctx_create: null output");
     *out = nullptr;
@@ -215,6 +254,7 @@ hp_status hp_ctx_create(hp_ctx** out, int32_t device) {
     if (e != cudaSuccess) { delete c; return hp_cuda_fail(e, "cudaGetDeviceProperties"); }
     c->sm_count = prop.multiProcessorCount;
     c->l2_bytes = prop.l2CacheSize;
+    if (const char* chk = std::getenv("HP_CHECKED")) c->checked = chk[0] != '\0' && chk[0] != '0';
     e = cudaMalloc(&c->d_status, 64 * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(c->d_status, 0, 64 * sizeof(int));
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_status, 64 * sizeof(int));
@@ -264,6 +304,7 @@ hp_status hp_ctx_check(hp_ctx* ctx, void* stream) {
                          : code == HP_DEV_BAD_INDEX ? "index out of range"
                          : code == HP_DEV_STACK_OVERFLOW ? "traversal stack overflow"
                          : code == HP_DEV_BAD_INPUT ? "invalid input (vertex index out of range)"
+                         : code == HP_DEV_CHECK_FAILED ? "checked mode: output failed its verification"
                                                     : "device error";
         return hp_fail(HP_ERR_DEVICE_STATUS, std::string("kernel reported: ") + what + " (info " +
                                                  std::to_string(info) + ")");
@@ -291,6 +332,7 @@ void hp_build_params_default(hp_build_params* p) {
 
 hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh* out,
                    const hp_build_taps* taps, void* stream) {
+    hp_nvtx_range nvtx_("hp_build");
     if (!ctx || !out) return hp_fail(HP_ERR_ARG, "hp_build: null argument");
     HP_TRY(check_mesh(m));
     HP_TRY(check_params(p));
@@ -316,6 +358,7 @@ hp_status hp_build(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_b
     hp_mark(ctx, s, "begin");
     HP_TRY(hp_lbvh_build(ctx, m, p, b, taps, s));
     if (ctx->arith == HP_ARITH_REFERENCE) HP_TRY(hp_woop_ref_launch(ctx, b, n, m, s));
+    if (hp_checking(ctx, s)) HP_TRY(checked_bvh(ctx, out, m, s, "hp_build"));
     return HP_OK;
 }
 
@@ -427,6 +470,7 @@ hp_status hp_bvh_stats_get(hp_ctx* ctx, const hp_bvh* bvh, hp_bvh_stats* out, vo
 
 // HipBVH::validate (rt/bvh/HipBVH.cpp:157-307) on the device (k_stats.cu).
 hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, int32_t* valid, void* stream) {
+    hp_nvtx_range nvtx_("hp_bvh_validate");
     if (!ctx || !bvh || !valid || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_bvh_validate: null argument");
     HP_TRY(check_mesh(m));
     *valid = 0;
@@ -441,6 +485,7 @@ hp_status hp_bvh_validate(hp_ctx* ctx, const hp_bvh* bvh, const hp_mesh* m, int3
 }
 
 hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
+    hp_nvtx_range nvtx_("hp_refit");
     if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_refit: null argument");
     HP_TRY(check_mesh(m));
     if (m->num_triangles != bvh->num_refs) return hp_fail(HP_ERR_ARG, "hp_refit: mesh does not match the BVH");
@@ -452,6 +497,7 @@ hp_status hp_refit(hp_ctx* ctx, hp_bvh* bvh, const hp_mesh* m, void* stream) {
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     HP_TRY(hp_refit_launch(ctx, b, bvh->num_refs, m, s));
     if (ctx->arith == HP_ARITH_REFERENCE) HP_TRY(hp_woop_ref_launch(ctx, b, bvh->num_refs, m, s));
+    if (hp_checking(ctx, s)) HP_TRY(checked_bvh(ctx, bvh, m, s, "hp_refit"));
     return HP_OK;
 }
 
@@ -460,11 +506,18 @@ hp_status hp_trace(hp_ctx* ctx, const hp_bvh* bvh, const float* rays, int64_t nu
     if (!ctx || !bvh || !bvh->impl) return hp_fail(HP_ERR_ARG, "hp_trace: null argument");
     if (num_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace: negative ray count");
     if (num_rays > 0 && (!rays || !results)) return hp_fail(HP_ERR_ARG, "hp_trace: null ray or result buffer");
+    hp_nvtx_range nvtx_("hp_trace");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     // A context tuned for it traces large batches in ray Morton order (same results).
     if (ctx->tune.trace_sorted && num_rays >= 65536 && num_rays < (int64_t(1) << 30))
-        return hp_trace_sorted(ctx, bvh, rays, num_rays, results, stats, flags, 30, nullptr, stream);
-    return hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays,
-                           num_rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
+        HP_TRY(hp_trace_sorted(ctx, bvh, rays, num_rays, results, stats, flags, 30, nullptr, stream));
+    else
+        HP_TRY(hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays,
+                               num_rays, results, stats, flags, s));
+    // checked mode: a traversal stack overflow or an out-of-range node index
+    // reported by the tracer comes back from this call
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
+    return HP_OK;
 }
 
 hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, int64_t num_rays,
@@ -474,6 +527,7 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     if (num_rays < 0 || chunk_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_host: negative count");
     if (num_rays == 0) return HP_OK;
     if (!rays_host || !results_host) return hp_fail(HP_ERR_ARG, "hp_trace_host: null ray or result buffer");
+    hp_nvtx_range nvtx_("hp_trace_host");
     const int64_t C = std::min<int64_t>(chunk_rays > 0 ? chunk_rays : (int64_t(1) << 22), num_rays);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     // A context tuned for sorted tracing sorts each chunk by 30-bit ray keys, as
@@ -581,6 +635,7 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     }
     // the caller's stream completes once every result is home
     for (int k = 0; k < 2; ++k) HP_CUDA(cudaStreamWaitEvent(s, ctx->io_free[k], 0));
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
     return HP_OK;
 }
 
@@ -591,8 +646,11 @@ hp_status hp_trace_adjoint(hp_ctx* ctx, const hp_mesh* m, const float* rays, con
     if (num_rays < 0) return hp_fail(HP_ERR_ARG, "hp_trace_adjoint: negative ray count");
     if (num_rays > 0 && (!rays || !results || !dl_dtuv || !dl_dvertices))
         return hp_fail(HP_ERR_ARG, "hp_trace_adjoint: null buffer");
-    return hp_adjoint_launch(ctx, m, rays, results, dl_dtuv, num_rays, dl_dvertices,
-                             reinterpret_cast<cudaStream_t>(stream));
+    hp_nvtx_range nvtx_("hp_trace_adjoint");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_TRY(hp_adjoint_launch(ctx, m, rays, results, dl_dtuv, num_rays, dl_dvertices, s));
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
+    return HP_OK;
 }
 
 hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in, void* keys_out,
@@ -603,6 +661,7 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
     if (n < 0 || n >= (int64_t(1) << 30)) return hp_fail(HP_ERR_ARG, "hp_radix_sort: n out of range");
     if (n == 0) return HP_OK;
     if (!keys_in || !keys_out || !vals_out) return hp_fail(HP_ERR_ARG, "hp_radix_sort: null buffer");
+    hp_nvtx_range nvtx_("hp_radix_sort");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     hp_sort_plan plan = hp_sort_make_plan(n, key_bytes, bits, ctx->tune.sort_block);
     const size_t hist_bytes = hp_carve::pad(hp_sort_hist_bytes(plan.passes));
@@ -611,7 +670,12 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
     void* scratch = cv.take<char>(plan.scratch_bytes);
     uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
     hp_sort_args a{keys_in, vals_in, keys_out, vals_out, scratch, hist, false, ctx->d_status, ctx};
-    return hp_sort_run(plan, a, s);
+    HP_TRY(hp_sort_run(plan, a, s));
+    if (hp_checking(ctx, s)) {
+        HP_TRY(hp_sort_check_launch(ctx, keys_out, n, key_bytes, bits, s));
+        HP_TRY(hp_ctx_check(ctx, stream));
+    }
+    return HP_OK;
 }
 
 hp_status hp_ctx_set_arithmetic(hp_ctx* ctx, int32_t mode) {

@@ -20,7 +20,8 @@ enum hp_dev_error {
     HP_DEV_SPIN_LIMIT = 1,      // a bounded wait (look-back, barrier) gave up
     HP_DEV_BAD_INDEX = 2,       // an index read from memory was out of range
     HP_DEV_STACK_OVERFLOW = 3,  // traversal stack exceeded its capacity
-    HP_DEV_BAD_INPUT = 4        // e.g. a triangle references a vertex out of range
+    HP_DEV_BAD_INPUT = 4,       // e.g. a triangle references a vertex out of range
+    HP_DEV_CHECK_FAILED = 5     // checked mode: an output failed its verification
 };
 
 // Upper bound on iterations of any spin-wait in this library.

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <string>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include "../../include/hippie_b200.h"
 
 struct hp_node_bin;
@@ -69,6 +70,9 @@ struct hp_ctx {
     // reports HP_DEV_SPIN_LIMIT (hp_ctx_set_sort_spin_limit).
     uint32_t sort_spin_limit = HP_SORT_SPIN_LIMIT_DEFAULT;
     int arith = HP_ARITH_IEEE;  // hp_ctx_set_arithmetic
+    // Checked mode (hp_ctx_set_checked, or HP_CHECKED=1 in the environment at
+    // hp_ctx_create): every entry point synchronises and verifies its output.
+    bool checked = false;
     // hp_trace_host: copy streams, one trace stream per staging slot, events
     // and two device staging slots
     cudaStream_t io_h2d = nullptr, io_d2h = nullptr, io_trace[2] = {nullptr, nullptr};
@@ -77,6 +81,23 @@ struct hp_ctx {
     char* io_slot[2] = {nullptr, nullptr};
     size_t io_slot_bytes = 0;
 };
+
+// An NVTX range around a public entry point (header-only NVTX 3: a no-op
+// unless a profiler such as Nsight Systems injects its handler).
+struct hp_nvtx_range {
+    explicit hp_nvtx_range(const char* name) { nvtxRangePushA(name); }
+    ~hp_nvtx_range() { nvtxRangePop(); }
+    hp_nvtx_range(const hp_nvtx_range&) = delete;
+    hp_nvtx_range& operator=(const hp_nvtx_range&) = delete;
+};
+
+// Checked mode: true when the context verifies outputs and the stream can be
+// synchronised (a stream under capture is not: the checks are skipped there).
+bool hp_checking(const hp_ctx* ctx, cudaStream_t s);
+// Checked mode's verification of a sort output: keys_out ordered by their low
+// `bits` bits, else HP_DEV_CHECK_FAILED in the context's status word.
+hp_status hp_sort_check_launch(hp_ctx* ctx, const void* keys_out, int64_t n, int key_bytes, int bits,
+                               cudaStream_t s);
 
 // Record a phase boundary on the stream when profiling is enabled.
 void hp_mark(hp_ctx* ctx, cudaStream_t s, const char* name);

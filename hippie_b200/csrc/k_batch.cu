@@ -769,22 +769,34 @@ hp_status hp_batch_ray_offset(const hp_batch* b, int32_t mesh, int64_t* offset) 
 
 hp_status hp_batch_build(hp_ctx* ctx, hp_batch* b, uint32_t flags, void* stream) {
     if (!ctx || !b) return hp_fail(HP_ERR_ARG, "hp_batch_build: null argument");
-    HP_TRY(hp_ctx_reserve(ctx, b->scratch, reinterpret_cast<cudaStream_t>(stream)));
-    return batch_run(ctx, b, 0, nullptr, nullptr, nullptr, flags, reinterpret_cast<cudaStream_t>(stream));
+    hp_nvtx_range nvtx_("hp_batch_build");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_TRY(hp_ctx_reserve(ctx, b->scratch, s));
+    HP_TRY(batch_run(ctx, b, 0, nullptr, nullptr, nullptr, flags, s));
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
+    return HP_OK;
 }
 
 hp_status hp_batch_trace(hp_ctx* ctx, hp_batch* b, const float* rays, int32_t* results, int32_t* stats,
                          uint32_t flags, void* stream) {
     if (!ctx || !b || (b->R > 0 && (!rays || !results))) return hp_fail(HP_ERR_ARG, "hp_batch_trace: null argument");
-    return batch_run(ctx, b, 1, rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
+    hp_nvtx_range nvtx_("hp_batch_trace");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_TRY(batch_run(ctx, b, 1, rays, results, stats, flags, s));
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
+    return HP_OK;
 }
 
 hp_status hp_batch_build_trace(hp_ctx* ctx, hp_batch* b, const float* rays, int32_t* results, int32_t* stats,
                                uint32_t flags, void* stream) {
     if (!ctx || !b || (b->R > 0 && (!rays || !results)))
         return hp_fail(HP_ERR_ARG, "hp_batch_build_trace: null argument");
-    HP_TRY(hp_ctx_reserve(ctx, b->scratch, reinterpret_cast<cudaStream_t>(stream)));
-    return batch_run(ctx, b, 2, rays, results, stats, flags, reinterpret_cast<cudaStream_t>(stream));
+    hp_nvtx_range nvtx_("hp_batch_build_trace");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    HP_TRY(hp_ctx_reserve(ctx, b->scratch, s));
+    HP_TRY(batch_run(ctx, b, 2, rays, results, stats, flags, s));
+    if (hp_checking(ctx, s)) HP_TRY(hp_ctx_check(ctx, stream));
+    return HP_OK;
 }
 
 hp_status hp_batch_bvh(hp_batch* b, int32_t mesh, hp_bvh* out) {

@@ -908,7 +908,31 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_lb(
     }
 }
 
+// Checked mode: every adjacent pair of the output in order by its low `bits`
+// bits; the first pair found out of order is reported with its position.
+template <typename K>
+__global__ void k_sort_check(const K* __restrict__ keys, int64_t n, int bits, int* status) {
+    const K mask = bits >= (int)(8 * sizeof(K)) ? ~K(0) : ((K(1) << bits) - 1);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x + 1; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        if ((__ldg(keys + i - 1) & mask) > (__ldg(keys + i) & mask))
+            hp_report(status, HP_DEV_CHECK_FAILED, (int)i);
+}
+
 }  // namespace
+
+hp_status hp_sort_check_launch(hp_ctx* ctx, const void* keys_out, int64_t n, int key_bytes, int bits,
+                               cudaStream_t s) {
+    if (n < 2) return HP_OK;
+    const unsigned grid = (unsigned)std::min<int64_t>(hp_div_up(n, 256), 8 * (int64_t)ctx->sm_count);
+    if (key_bytes == 4)
+        k_sort_check<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(keys_out), n, bits, ctx->d_status);
+    else
+        k_sort_check<uint64_t><<<grid, 256, 0, s>>>(static_cast<const uint64_t*>(keys_out), n, bits, ctx->d_status);
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    return HP_OK;
+}
 
 hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block) {
     hp_sort_plan p;

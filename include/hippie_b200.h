@@ -459,6 +459,22 @@ hp_status hp_radix_sort(hp_ctx* ctx, const void* keys_in, const int32_t* vals_in
 #define HP_SORT_SPIN_LIMIT_DEFAULT 4194304u
 hp_status hp_ctx_set_sort_spin_limit(hp_ctx* ctx, uint32_t spins);
 
+/* Checked mode: every entry point verifies what it produced before it
+ * returns, at the cost of a host synchronisation per call. hp_build and
+ * hp_refit sync the BVH, check its node counts against the reference count
+ * and run hp_bvh_validate; hp_radix_sort checks that its output is ordered;
+ * hp_trace, hp_trace_host, hp_trace_adjoint and the batch calls return the
+ * device error words (traversal stack overflow, index out of range, a bounded
+ * wait that gave up) as HP_ERR_DEVICE_STATUS from the call itself instead of
+ * from a later hp_ctx_check. On a stream that is being captured into a CUDA
+ * graph the checks, which synchronise, are skipped. Off by default; a
+ * context created while the environment variable HP_CHECKED is set to a
+ * value other than "0" starts with it on. The bounds checks that report into
+ * the error words are always compiled in. The reference has no counterpart
+ * (it stops the process on the first HIP error, gpu/HipModule.cpp:216-222). */
+hp_status hp_ctx_set_checked(hp_ctx* ctx, int32_t on);
+int32_t hp_ctx_get_checked(const hp_ctx* ctx);
+
 /* The same sort for callers that must not allocate GPU memory: no context, no
  * cudaMalloc / cudaFree / allocating library call. This entry point has no
  * counterpart in the reference. It serves code that runs where the device
