@@ -170,9 +170,15 @@ struct hp_sort_plan {
     int block = 512;               // threads per pass CTA: 512 or 256
 };
 hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block = 512);
-// Histograms [passes][256] (uint32) must be zero before the first key is
-// counted; hp_sort_run zeroes them itself unless hist_ready is set, in which
-// case the caller has already filled them (the Morton kernel does).
+// The digit histograms a sort starts from: `count` 8-bit digits at shifts
+// shift0, shift0 + 8, ... (digit width min(8, bits - shift)), laid out
+// [count][256] (uint32). An LSD sort counts every pass's digit from shift 0;
+// the wide-key sort only the three digits below its top bit.
+void hp_sort_hist_digits(const hp_sort_plan& plan, int* shift0, int* count);
+// The histograms must be zero before the first key is counted; hp_sort_run
+// zeroes and fills them itself unless hist_ready is set, in which case the
+// caller has already filled them as hp_sort_hist_digits says (the Morton
+// kernels do).
 struct hp_sort_args {
     const void* keys_in;
     const int32_t* vals_in;        // nullptr: values are 0..n-1

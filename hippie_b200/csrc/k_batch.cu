@@ -48,7 +48,8 @@ struct bargs {
     int M;
     int64_t N;
     int bits;                // Morton bits (the mesh index sits above them)
-    int passes;
+    int passes;  // digits counted for the sort (hp_sort_hist_digits) from shift hshift
+    int hshift;
     hp_bvh_info* info;       // [M]
     float4* tbmin;
     float4* tbmax;
@@ -144,8 +145,8 @@ __global__ void __launch_bounds__(TB) k_b_morton(bargs B) {
         const uint64_t key = ((uint64_t)m << B.bits) |
                              hp_morton_key(a.x, a.y, a.z, b.x, b.y, b.z, smin, scale, B.bits);
         B.keys[g] = key;
-        for (int p = 0; p < B.passes; ++p)
-            atomicAdd(&sh[p * 256 + (uint32_t)((key >> (8 * p)) & 0xffu)], 1u);
+        for (int p = 0; p < B.passes; ++p)  // bits above the key width are zero
+            atomicAdd(&sh[p * 256 + (uint32_t)((key >> (B.hshift + 8 * p)) & 0xffu)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < B.passes * 256; i += TB)
@@ -492,7 +493,7 @@ hp_status batch_build_seq(hp_ctx* ctx, hp_batch* b, cudaStream_t s) {
     B.M = b->M;
     B.N = N;
     B.bits = b->bits;
-    B.passes = plan.passes;
+    hp_sort_hist_digits(plan, &B.hshift, &B.passes);
     B.info = b->d_info;
     B.tbmin = cv.take<float4>(N);
     B.tbmax = cv.take<float4>(N);

@@ -102,7 +102,7 @@ __global__ void k_init_build(hp_bvh_info* info, uint32_t* hist, int hist_words) 
 template <typename K>
 __global__ void __launch_bounds__(TB) k_morton(const float4* __restrict__ bmin,
                                                const float4* __restrict__ bmax, int64_t n,
-                                               hp_bvh_info* info, int bits, int passes,
+                                               hp_bvh_info* info, int bits, int hshift, int passes,
                                                K* __restrict__ keys, uint32_t* hist) {
     __shared__ uint32_t sh[8 * 256];
     for (int i = threadIdx.x; i < passes * 256; i += TB) sh[i] = 0;
@@ -119,9 +119,9 @@ __global__ void __launch_bounds__(TB) k_morton(const float4* __restrict__ bmin,
         float4 a = bmin[i], b = bmax[i];
         uint64_t key = hp_morton_key(a.x, a.y, a.z, b.x, b.y, b.z, smin, scale, bits);
         keys[i] = (K)key;
-        for (int p = 0; p < passes; ++p) {
-            int w = min(8, bits - 8 * p);
-            atomicAdd(&sh[p * 256 + (uint32_t)((key >> (8 * p)) & ((1u << w) - 1u))], 1u);
+        for (int p = 0; p < passes; ++p) {  // the sort's digits (hp_sort_hist_digits)
+            const int sh_p = hshift + 8 * p, w = min(8, bits - sh_p);
+            atomicAdd(&sh[p * 256 + (uint32_t)((key >> sh_p) & ((1u << w) - 1u))], 1u);
         }
     }
     __syncthreads();
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(TB) k_leaves(
 // nodes (those whose ranges cross a CTA boundary: about depth per boundary)
 // with the global counters and one acq_rel atomic per arrival.
 constexpr int CB = 512;
-constexpr size_t CLIMB_SMEM = (size_t)CB * (4 * sizeof(float4) + 6 * sizeof(int) + sizeof(int2));
+constexpr size_t CLIMB_SMEM = (size_t)CB * (4 * sizeof(float4) + 7 * sizeof(int) + sizeof(int2)) + 2 * sizeof(int);
 
 struct climb_args {
     int n;
@@ -288,11 +288,14 @@ __global__ void __launch_bounds__(CB, 4) k_climb_local(climb_args A) {
     int* s_up = s_right + CB;                               // parents of nodes base + k
     int* s_mh = s_up + CB;                                  // maxHi of positions base + k
     int* s_st = s_mh + CB;                                  // state of local nodes
+    int* s_front = s_st + CB;                               // this CTA's frontier entries
+    int* s_fn = s_front + CB;                               // [0] their count, [1] their offset
     const int n = A.n;
     const int base = blockIdx.x * CB, k = threadIdx.x, p = base + k;
     const int last = min(base + CB, n) - 1;  // this CTA's last leaf
     s_cnt[k] = 0;
     s_mh[k] = -1;
+    if (k == 0) s_fn[0] = 0;
     if (p < n - 1) {
         s_left[k] = __ldg(A.left + p);
         s_right[k] = __ldg(A.right + p);
@@ -317,9 +320,9 @@ __global__ void __launch_bounds__(CB, 4) k_climb_local(climb_args A) {
         const int kn = node - base;
         const int2 rg = ((unsigned)kn < (unsigned)CB) ? s_rng[kn] : make_int2(-1, -1);
         if (!(rg.x >= base && rg.y <= last && kn <= rg.y - base && kn >= rg.x - base)) {
-            // the next node's range crosses the CTA's: phase B continues from child
-            const unsigned slot = atomicAdd(A.frontier_count, 1u);
-            A.frontier[slot] = child;
+            // the next node's range crosses the CTA's: phase B continues from
+            // child (collected here, one global reservation per CTA below)
+            s_front[atomicAdd(s_fn, 1)] = child;  // one entry per leaf thread at most
             break;
         }
         if (++guard > CB) {
@@ -356,6 +359,9 @@ __global__ void __launch_bounds__(CB, 4) k_climb_local(climb_args A) {
         node = s_up[kn];
     }
     __syncthreads();
+    if (k == 0) s_fn[1] = s_fn[0] ? (int)atomicAdd(A.frontier_count, (unsigned)s_fn[0]) : 0;
+    __syncthreads();
+    for (int i = k; i < s_fn[0]; i += CB) A.frontier[s_fn[1] + i] = s_front[i];
     // write back the local nodes (index base + k) and the maxHi words of the
     // CTA's positions; phase B raises maxHi further with global atomics
     const int2 rg = s_rng[k];
@@ -558,6 +564,8 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     const int64_t n = m->num_triangles;
     const int bits = p->morton_bits;
     const hp_sort_plan plan = hp_sort_make_plan(n, (int)sizeof(K), bits, ctx->tune.sort_block);
+    int h_shift = 0, h_count = 0;  // digits the Morton kernel counts for the sort
+    hp_sort_hist_digits(plan, &h_shift, &h_count);
     const int64_t nn = 2 * n - 1;
     const bool ploc = p->method == HP_METHOD_PLOC;
     const bool hlbvh = p->method == HP_METHOD_HLBVH;  // binned SAH above the clusters, then the ATR collapse
@@ -606,7 +614,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                             info->box_ord, err, woop_src);
         hp_count_launch(2);
         hp_mark(ctx, s, "boxes");
-        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(ctx, s, "morton");
@@ -639,7 +647,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                             info->box_ord, err);
         hp_count_launch(2);
         hp_mark(ctx, s, "boxes");
-        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(ctx, s, "morton");
@@ -700,7 +708,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                         info->box_ord, err);
     hp_count_launch(2);
     hp_mark(ctx, s, "boxes");
-    k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, plan.passes, keys, hist);
+    k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "morton");

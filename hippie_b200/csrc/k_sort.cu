@@ -306,6 +306,7 @@ __host__ __device__ constexpr bool hybrid_sort(int64_t n, int key_bytes, int bit
 }
 
 constexpr int SEG_TOP = 3;  // 8-bit digits ordered by global passes
+constexpr int SEG_WALK = 6;  // steps of the linear search for a segment's bounds
 
 // Histograms of the SEG_TOP 8-bit digits at shifts s0, s0 + 8, ...
 __global__ void k_hist_top(const uint64_t* __restrict__ keys, int64_t n, int s0, uint32_t* __restrict__ hist) {
@@ -452,58 +453,88 @@ __device__ int seg_block_sort(seg_smem& S, int m, int L) {
 
 // Sorts in[cs, cs + m) (m <= SEG_CAP, whole segments of equal prefix) by the
 // low L bits within each segment and writes the result to out[cs, cs + m).
+// The chunk's keys and values are ck[0, m) and cv[0, m) in shared memory.
 // Segments of up to SEG_RANK_MAX keys (almost all of them) need no
-// coordination: every element finds its segment's bounds (its neighbours tell
-// a one-key segment; otherwise a binary search in shared memory), counts the
+// coordination: every element finds its segment's bounds (the warp's ballots
+// of segment starts and ends tell them for the segments inside its 32
+// elements; a short walk, then a binary search, for the others), counts the
 // smaller (low bits, position) pairs in its segment and stores itself at
 // start + count. Longer segments are listed and sorted by the CTA with stable
-// 8-bit passes.
+// 8-bit passes, which reuse all of the shared buffers (ck and cv included:
+// those segments are read again from in).
 // Every index is checked against the chunk: inputs whose prefixes are not in
 // order (only after an earlier pass gave up a bounded wait, which is reported)
 // must not make it read or write outside the chunk.
-__device__ void seg_sort_chunk(seg_smem& S, const uint64_t* __restrict__ kin, const int32_t* __restrict__ vin,
+__device__ void seg_sort_chunk(seg_smem& S, const uint64_t* ck, const int32_t* cv,
+                               const uint64_t* __restrict__ kin, const int32_t* __restrict__ vin,
                                uint64_t* __restrict__ kout, int32_t* __restrict__ vout, int64_t cs, int m,
                                int L, int* err) {
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint64_t low = (uint64_t(1) << L) - 1u;
-    for (int j = tid; j < m; j += SEG_BLOCK) {
-        S.key[0][j] = kin[cs + j];
-        S.val[0][j] = vin ? vin[cs + j] : (int32_t)(cs + j);
-    }
     if (tid == 0) S.nmed = 0;
     __syncthreads();
-    for (int c = tid; c < m; c += SEG_BLOCK) {
-        const uint64_t kc = S.key[0][c];
+    // warp-contiguous groups of 32 elements; the loop bound is uniform over the
+    // block, so every lane takes part in the ballots
+    for (int c0 = tid - lane; c0 < m; c0 += SEG_BLOCK) {
+        const int c = c0 + lane;
+        const bool valid = c < m;
+        const uint64_t kc = valid ? ck[c] : 0ull;
         const uint32_t pc = seg_prefix(kc, L);
-        const bool first = c == 0 || seg_prefix(S.key[0][c - 1], L) != pc;
-        const bool last = c + 1 == m || seg_prefix(S.key[0][c + 1], L) != pc;
-        if (first && last) {  // a one-key segment is in place
+        const bool head = valid && (c == 0 || seg_prefix(ck[c - 1], L) != pc);
+        const bool tail = valid && (c + 1 == m || seg_prefix(ck[c + 1], L) != pc);
+        const unsigned H = __ballot_sync(HP_FULL_MASK, head), T = __ballot_sync(HP_FULL_MASK, tail);
+        if (!valid) continue;
+        if (head && tail) {  // a one-key segment is in place
             kout[cs + c] = kc;
-            vout[cs + c] = S.val[0][c];
+            vout[cs + c] = cv[c];
             continue;
         }
-        // the segment's bounds by binary search (the chunk is sorted by prefix)
-        int a = 0, e = c;
-        while (a < e) {
-            const int mid = (a + e) >> 1;
-            if (seg_prefix(S.key[0][mid], L) < pc) a = mid + 1;
-            else e = mid;
+        // the segment's bounds (the chunk is sorted by prefix)
+        const unsigned hb = H & (lane == 31 ? HP_FULL_MASK : ((2u << lane) - 1u));  // starts at or below
+        const unsigned tb = T & (HP_FULL_MASK << lane);                             // ends at or above
+        int a, b;
+        if (hb) {
+            a = c0 + 31 - __clz(hb);
+        } else {  // the segment starts before this group
+            a = c0;
+            for (int w = 0; w < SEG_WALK && a > 0 && seg_prefix(ck[a - 1], L) == pc; ++w) --a;
+            if (a > 0 && seg_prefix(ck[a - 1], L) == pc) {
+                int e = a - 1;
+                a = 0;
+                while (a < e) {
+                    const int mid = (a + e) >> 1;
+                    if (seg_prefix(ck[mid], L) < pc) a = mid + 1;
+                    else e = mid;
+                }
+            }
         }
-        int b = c + 1, f = m;
-        while (b < f) {
-            const int mid = (b + f) >> 1;
-            if (seg_prefix(S.key[0][mid], L) > pc) f = mid;
-            else b = mid + 1;
+        if (tb) {
+            b = c0 + __ffs(tb);
+        } else {  // the segment ends after this group
+            b = min(c0 + 32, m);
+            for (int w = 0; w < SEG_WALK && b < m && seg_prefix(ck[b], L) == pc; ++w) ++b;
+            if (b < m && seg_prefix(ck[b], L) == pc) {
+                int f = m;
+                ++b;
+                while (b < f) {
+                    const int mid = (b + f) >> 1;
+                    if (seg_prefix(ck[mid], L) > pc) f = mid;
+                    else b = mid + 1;
+                }
+            }
         }
+        a = max(a, 0);
+        b = min(max(b, c + 1), m);
+        if (a > c) a = c;
         if (b - a <= SEG_RANK_MAX) {
             const uint64_t lc = kc & low;
             int rank = 0;
             for (int k = a; k < b; ++k) {
-                const uint64_t lk = S.key[0][k] & low;
+                const uint64_t lk = ck[k] & low;
                 rank += (lk < lc) || (lk == lc && k < c);
             }
             kout[cs + a + rank] = kc;
-            vout[cs + a + rank] = S.val[0][c];
+            vout[cs + a + rank] = cv[c];
         } else if (a == c) {  // the first element of a longer segment lists it
             const int q = atomicAdd(&S.nmed, 1);
             if (q < SEG_MED_CAP) S.med[q] = make_int2(a, b);
@@ -531,6 +562,17 @@ __device__ void seg_sort_chunk(seg_smem& S, const uint64_t* __restrict__ kin, co
     __syncthreads();
 }
 
+// A chunk read from global memory into the first key and value buffers.
+__device__ void seg_sort_chunk_global(seg_smem& S, const uint64_t* __restrict__ kin,
+                                      const int32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+                                      int32_t* __restrict__ vout, int64_t cs, int m, int L, int* err) {
+    for (int j = threadIdx.x; j < m; j += SEG_BLOCK) {
+        S.key[0][j] = kin[cs + j];
+        S.val[0][j] = vin ? vin[cs + j] : (int32_t)(cs + j);
+    }
+    seg_sort_chunk(S, S.key[0], S.val[0], kin, vin, kout, vout, cs, m, L, err);
+}
+
 // One CTA per window of SEG_WINDOW positions: the segments that start in it.
 // The window and the SEG_EXT positions after it are loaded once (coalesced);
 // the first segment start in the window and the first one after it are found
@@ -551,14 +593,22 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
     const int64_t lo = wb > 0 ? wb - 1 : 0, hi = min(we + SEG_EXT, n);
     int* first = reinterpret_cast<int*>(&S.range[2]);  // [0] first start in the window, [1] first after it
     if (tid == 0) { first[0] = SEG_NONE; first[1] = SEG_NONE; }
-    for (int64_t j = lo + tid; j < hi; j += SEG_BLOCK) S.key[1][j - lo] = kin[j];
+    for (int64_t j = lo + tid; j < hi; j += SEG_BLOCK) {
+        S.key[1][j - lo] = kin[j];
+        S.val[1][j - lo] = vin ? vin[j] : (int32_t)j;
+    }
     __syncthreads();
-    for (int64_t j = wb + tid; j < hi; j += SEG_BLOCK) {
-        const bool start = j == 0 || seg_prefix(S.key[1][j - lo], L) != seg_prefix(S.key[1][j - 1 - lo], L);
-        if (start) {
-            if (j < we) atomicMin(&first[0], (int)(j - wb));
-            else atomicMin(&first[1], (int)(j - we));
-        }
+    // one shared atomic per warp and step: the warp's lowest starting lane
+    // (the loop bound is uniform over the block, so every lane takes part)
+    for (int64_t j0 = wb; j0 < hi; j0 += SEG_BLOCK) {
+        const int64_t j = j0 + tid;
+        const bool start = j < hi &&
+                           (j == 0 || seg_prefix(S.key[1][j - lo], L) != seg_prefix(S.key[1][j - 1 - lo], L));
+        const unsigned in_win = __ballot_sync(HP_FULL_MASK, start && j < we);
+        const unsigned after = __ballot_sync(HP_FULL_MASK, start && j >= we);
+        const int lane = tid & 31;
+        if (in_win && lane == __ffs(in_win) - 1) atomicMin(&first[0], (int)(j - wb));
+        if (after && lane == __ffs(after) - 1) atomicMin(&first[1], (int)(j - we));
     }
     __syncthreads();
     if (first[0] == SEG_NONE) return;  // a segment that started earlier covers the window
@@ -575,7 +625,11 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
     __syncthreads();
     const int64_t cs = S.range[0], ce = S.range[1];
     if (ce - cs <= SEG_CAP) {
-        seg_sort_chunk(S, kin, vin, kout, vout, cs, (int)(ce - cs), L, err);
+        if (ce <= hi)  // the chunk was loaded with the window
+            seg_sort_chunk(S, S.key[1] + (cs - lo), S.val[1] + (cs - lo), kin, vin, kout, vout, cs,
+                           (int)(ce - cs), L, err);
+        else
+            seg_sort_chunk_global(S, kin, vin, kout, vout, cs, (int)(ce - cs), L, err);
         return;
     }
     // A large run: batches of whole segments up to SEG_CAP keys; a segment
@@ -604,7 +658,7 @@ __global__ void __launch_bounds__(SEG_BLOCK, 4) k_seg_sort(const uint64_t* __res
         }
         __syncthreads();
         const int64_t b0 = S.range[2], b1 = S.range[3];
-        if (b1 > b0) seg_sort_chunk(S, kin, vin, kout, vout, b0, (int)(b1 - b0), L, err);
+        if (b1 > b0) seg_sort_chunk_global(S, kin, vin, kout, vout, b0, (int)(b1 - b0), L, err);
         cur = b1;
     }
 }
@@ -699,7 +753,7 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
     uint32_t* status = cv.take<uint32_t>((size_t)plan.passes * plan.tiles * 256 + 64);
     uint32_t* counters = status + (size_t)plan.passes * plan.tiles * 256;
     HP_CUDA(cudaMemsetAsync(status, 0, ((size_t)plan.passes * plan.tiles * 256 + 64) * 4, stream));
-    if (!a.hist_ready) {
+    if (!a.hist_ready && !(sizeof(K) == 8 && hybrid_sort(n, 8, plan.bits))) {
         HP_CUDA(cudaMemsetAsync(a.hist, 0, hp_sort_hist_bytes(plan.passes), stream));
         int grid = (int)std::min<int64_t>(hp_div_up(n, 1024), 148 * 8);
         k_sort_hist<K><<<std::max(grid, 1), 1024, plan.passes * 256 * 4, stream>>>(
@@ -717,11 +771,13 @@ hp_status sort_run_t(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream
         if (hybrid_sort(n, 8, plan.bits)) {
             // top 24 bits by three LSD passes, then every segment of equal prefix
             const int s0 = plan.bits - 8 * SEG_TOP;
-            HP_CUDA(cudaMemsetAsync(a.hist, 0, 256 * SEG_TOP * sizeof(uint32_t), stream));
-            k_hist_top<<<std::max(1, (int)std::min<int64_t>(hp_div_up(n, 1024), 148 * 8)), 1024, 0, stream>>>(
-                kin, n, s0, a.hist);
-            HP_CUDA(cudaGetLastError());
-            hp_count_launch();
+            if (!a.hist_ready) {
+                HP_CUDA(cudaMemsetAsync(a.hist, 0, 256 * SEG_TOP * sizeof(uint32_t), stream));
+                k_hist_top<<<std::max(1, (int)std::min<int64_t>(hp_div_up(n, 1024), 148 * 8)), 1024, 0,
+                             stream>>>(kin, n, s0, a.hist);
+                HP_CUDA(cudaGetLastError());
+                hp_count_launch();
+            }
             const uint32_t sl = a.ctx ? a.ctx->sort_spin_limit : LOOKBACK_SPIN_LIMIT;
             const K* src_k = kin;
             const int32_t* src_v = vin;
@@ -951,6 +1007,16 @@ hp_sort_plan hp_sort_make_plan(int64_t n, int key_bytes, int bits, int block) {
 }
 
 size_t hp_sort_hist_bytes(int passes) { return (size_t)passes * 256 * 4; }
+
+void hp_sort_hist_digits(const hp_sort_plan& plan, int* shift0, int* count) {
+    if (hybrid_sort(plan.n, plan.key_bytes, plan.bits)) {
+        *shift0 = plan.bits - 8 * SEG_TOP;
+        *count = SEG_TOP;
+    } else {
+        *shift0 = 0;
+        *count = plan.passes;
+    }
+}
 
 hp_status hp_sort_run(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream_t stream) {
     if (plan.n <= 0) return HP_OK;
