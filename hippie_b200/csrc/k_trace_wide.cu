@@ -39,7 +39,7 @@ template <> struct wide_cfg<4> { static constexpr int STACK = 96; };
 template <> struct wide_cfg<8> { static constexpr int STACK = 128; };
 
 template <int N, bool ANY_HIT, bool STATS>
-__global__ void __launch_bounds__(TB) k_trace_wide(const float4* __restrict__ rays, int64_t num_rays,
+__global__ void __launch_bounds__(TB, 12) k_trace_wide(const float4* __restrict__ rays, int64_t num_rays,
                                                    int4* __restrict__ results, int2* __restrict__ stats,
                                                    const int4* __restrict__ nodes, const float4* __restrict__ woop,
                                                    const int32_t* __restrict__ tri_idx, int max_nodes, int num_refs,
