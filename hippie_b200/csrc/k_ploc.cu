@@ -98,6 +98,12 @@ struct ploc_args {
     int* parent;
     int2* counts;   // (surviving interior nodes, leaves) of the subtree if the node survives
     uint8_t* state;
+    // What the binary collapse needs of a node's children, written when the
+    // node is made (null for the wide layouts): the left child's counts, its
+    // index, its size with bit 31 set when the right child ends as a leaf;
+    // and the three box rows of the node's Bin record (children's boxes).
+    int4* cinfo;
+    float4* cbox;
     int* cl0;
     int* cl1;
     unsigned long long* status;    // look-back words of the iterations on long lists
@@ -149,6 +155,13 @@ __device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a,
     A.right[node] = b;
     A.parent[a] = node;
     A.parent[b] = node;
+    if (A.cinfo) {
+        __stcg(A.cinfo + node, make_int4(ca.x, ca.y, a, __float_as_int(amx.w) | (cb.x == 0 ? (int)0x80000000 : 0)));
+        float4* cbx = A.cbox + 3 * (int64_t)node;
+        __stcg(cbx, make_float4(amn.x, amx.x, amn.y, amx.y));
+        __stcg(cbx + 1, make_float4(bmn.x, bmx.x, bmn.y, bmx.y));
+        __stcg(cbx + 2, make_float4(amn.z, amx.z, bmn.z, bmx.z));
+    }
 }
 
 // Leaves: sorted reference p becomes leaf node n-1+p and cluster p.
@@ -623,6 +636,8 @@ struct td_args {
     const uint8_t* state;
     const float4* nbmin;
     const float4* nbmax;
+    const int4* cinfo;   // PLOC: per node, what its children contribute (ploc_args::cinfo)
+    const float4* cbox;  // PLOC: per node, its Bin record's three box rows
     int4* rec;          // [n-1] interior records: preorder index, first leaf, first triangle, status
     int* flag;          // [n-1] record published (build epoch)
     int epoch;
@@ -647,6 +662,10 @@ __device__ __forceinline__ void td_put(const td_args& T, int idx, const hp_node_
     else hp_report(T.err, HP_DEV_BAD_INDEX, idx);
 }
 
+// PRE: the PLOC build recorded, per node, its children's contribution
+// (cinfo, cbox), so a node reads its own row and its parent's instead of
+// gathering its sibling's and its children's counts, states and boxes.
+template <bool PRE>
 __global__ void __launch_bounds__(256) k_topdown(td_args T) {
     __shared__ unsigned s_tile;
     if (threadIdx.x == 0) s_tile = atomicAdd(T.ticket, 1u);
@@ -673,10 +692,20 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
             return;
         }
         // what does not depend on the parent's record is read before waiting for it
-        const bool is_left = T.left[p] == v;
-        const int sib = is_left ? T.right[p] : T.left[p];
-        const int2 cs = T.counts[sib];
-        const int ssize = __float_as_int(T.nbmax[sib].w);
+        bool is_left;
+        int2 cs;    // the left sibling's counts (used by a right child)
+        int ssize;  // the left sibling's size
+        if (PRE) {
+            const int4 ci = __ldcg(T.cinfo + p);
+            is_left = ci.z == v;
+            cs = make_int2(ci.x, ci.y);
+            ssize = ci.w & 0x7fffffff;
+        } else {
+            is_left = T.left[p] == v;
+            const int sib = is_left ? T.right[p] : T.left[p];
+            cs = T.counts[sib];
+            ssize = __float_as_int(T.nbmax[sib].w);
+        }
         const bool leaf = v >= n - 1 || T.state[v] == 0;
         unsigned spins = 0;
         while (ld_acquire_u32(reinterpret_cast<const unsigned*>(T.flag + p)) != (unsigned)T.epoch) {
@@ -708,7 +737,20 @@ __global__ void __launch_bounds__(256) k_topdown(td_args T) {
     }
     const float4 mn = T.nbmin[v], mx = T.nbmax[v];
     const int size = __float_as_int(mx.w);
-    if (status == ST_INTERIOR) {
+    if (status == ST_INTERIOR && PRE) {
+        // a left child ends as a leaf exactly when its counts are (0, 1)
+        const int4 ci = __ldcg(T.cinfo + v);
+        const bool l_leaf = ci.x == 0, r_leaf = ci.w < 0;
+        const int lref = l_leaf ? ~(num_int + lidx) : iidx + 1;
+        const int rref = r_leaf ? ~(num_int + lidx + ci.y) : iidx + 1 + ci.x;
+        const float4* cb = T.cbox + 3 * (int64_t)v;
+        hp_node_bin nd;
+        nd.c0xy = __ldcg(cb);
+        nd.c1xy = __ldcg(cb + 1);
+        nd.cz = __ldcg(cb + 2);
+        nd.meta = make_int4(lref, rref, size, par);
+        td_put(T, iidx, nd);
+    } else if (status == ST_INTERIOR) {
         const int l = T.left[v], r = T.right[v];
         const bool l_leaf = l >= n - 1 || T.state[l] == 0;
         const bool r_leaf = r >= n - 1 || T.state[r] == 0;
@@ -790,7 +832,7 @@ hp_status hp_topdown_collapse(hp_ctx* ctx, const hp_mesh* m, const hp_topdown_in
     T.info = out->info;
     T.max_nodes = (int)std::max<int64_t>(2 * out->capacity - 1, 3);
     T.err = ctx->d_status;
-    k_topdown<<<hp_div_up(nn, 256), 256, 0, s>>>(T);
+    k_topdown<false><<<hp_div_up(nn, 256), 256, 0, s>>>(T);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     return HP_OK;
@@ -808,6 +850,7 @@ size_t hp_ploc_scratch_bytes(int64_t n) {
     b += hp_carve::pad(((std::min<int64_t>(n, NB4_MIN_N) + LPB / 2 - 1) / (LPB / 2) + 1) * 8);
     b += hp_carve::pad(MAX_ITER * 4 + 64);
     b += hp_carve::pad(n * 16) + hp_carve::pad(n * 4);  // records, flags
+    b += hp_carve::pad(n * 16) + hp_carve::pad(n * 48);  // children's counts and boxes per node
     return b;
 }
 
@@ -849,6 +892,10 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     A.err = ctx->d_status;
     int4* rec = cv.take<int4>(n);
     int* flag = cv.take<int>(n);
+    if (hp_layout_of(p) == 2) {  // the binary collapse reads them
+        A.cinfo = cv.take<int4>(n);
+        A.cbox = cv.take<float4>(3 * (int64_t)n);
+    }
     HP_CUDA(cudaMemsetAsync(A.status, 0, mtiles * 8, s));
     HP_CUDA(cudaMemsetAsync(A.status_f, 0, ftiles * 8, s));
     HP_CUDA(cudaMemsetAsync(ctl, 0, (MAX_ITER + 16) * 4, s));
@@ -917,7 +964,9 @@ hp_status hp_ploc_stage(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p,
     T.info = out->info;
     T.max_nodes = (int)std::max<int64_t>(2 * out->capacity - 1, 3);
     T.err = ctx->d_status;
-    k_topdown<<<hp_div_up(nn, 256), 256, 0, s>>>(T);
+    T.cinfo = A.cinfo;
+    T.cbox = A.cbox;
+    k_topdown<true><<<hp_div_up(nn, 256), 256, 0, s>>>(T);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "collapse");
