@@ -56,7 +56,7 @@ __device__ __forceinline__ int seg_search(const int64_t* __restrict__ off, int n
 // BATCH: rays of many meshes in one launch; ray g belongs to the segment whose
 // ray range holds it, and the lane traverses that mesh's BVH.
 template <bool ANY_HIT, bool STATS, bool BATCH, int SST>
-__global__ void __launch_bounds__(TRACE_BLOCK, 12) k_trace(
+__global__ void __launch_bounds__(TRACE_BLOCK, BATCH ? 9 : 12) k_trace(
     const float4* __restrict__ rays, int64_t num_rays, int4* __restrict__ results,
     int2* __restrict__ stats, const float4* __restrict__ nodes_all, const float4* __restrict__ woop_all,
     const int32_t* __restrict__ tri_all, int max_nodes_all, int num_refs_all,
@@ -215,11 +215,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK, 12) k_trace(
                 }
                 for (int tri = begin; tri < end; ++tri) {
                     if (STATS) ++r.tris;
-                    // all three Woop rows at once: one memory round trip per triangle
-                    // instead of up to three dependent ones
+                    // Single-mesh launches load the first two Woop rows at once (the
+                    // second is needed whenever the plane is hit in range): one round
+                    // trip fewer per tested triangle. The batch variant, which holds
+                    // more state per lane, loads each row when it needs it.
                     const float4 v0 = __ldg(woop + 3 * (int64_t)tri);
-                    const float4 v1 = __ldg(woop + 3 * (int64_t)tri + 1);
-                    const float4 v2 = __ldg(woop + 3 * (int64_t)tri + 2);
+                    const float4 v1pre = BATCH ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
+                                               : __ldg(woop + 3 * (int64_t)tri + 1);
                     const float oz = __fmaf_rn(-r.oz, v0.z, __fmaf_rn(-r.oy, v0.y, __fmaf_rn(-r.ox, v0.x, v0.w)));
                     // The roundings of the reference's fast-math tracer, measured
                     // against its output on sm_100a: the chains o.w +- ... are
@@ -233,10 +235,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK, 12) k_trace(
                     if (!closer && t == r.hit_t && r.hit >= 0)
                         closer = __ldg(tri_idx + tri) < __ldg(tri_idx + r.hit);
                     if (t > r.tmin && closer) {
+                        const float4 v1 = BATCH ? __ldg(woop + 3 * (int64_t)tri + 1) : v1pre;
                         const float ox = __fmaf_rn(r.oz, v1.z, __fmaf_rn(r.oy, v1.y, __fmaf_rn(r.ox, v1.x, v1.w)));
                         const float dx = __fmaf_rn(r.dz, v1.z, __fmaf_rn(r.dy, v1.y, __fmul_rn(r.dx, v1.x)));
                         const float u = __fmaf_rn(t, dx, ox);
                         if (u >= 0.0f) {
+                            const float4 v2 = __ldg(woop + 3 * (int64_t)tri + 2);
                             const float oy = __fmaf_rn(r.oz, v2.z, __fmaf_rn(r.oy, v2.y, __fmaf_rn(r.ox, v2.x, v2.w)));
                             const float dy = __fmaf_rn(r.dz, v2.z, __fmaf_rn(r.dx, v2.x, __fmul_rn(r.dy, v2.y)));
                             const float v = __fmaf_rn(t, dy, oy);
