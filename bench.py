@@ -18,11 +18,11 @@ e2e        the same metrics through the C ABI with pinned host buffers: the
            counts), then hp_trace_host over the host ray and result buffers
            (every ray uploaded and every hit record downloaded, in chunks whose
            copies overlap the traces of their neighbours).
-roofline   the radix-sort phase of the build (HBM-bound): the survey's algorithmic
-           bytes n * P * 2 * (K + 4) (P = ceil(bits / 8) LSD passes) over the
+roofline   the radix-sort phase of the build (HBM-bound): the algorithmic bytes of
+           an 8-bit LSD sort, n * P * 2 * (K + 4) (P = ceil(bits / 8) passes), over the
            summed CUDA-event durations of its kernels (for 60-bit keys three
            LSD passes and the segment sort);
-           roofline.phases gives every HBM-bound build phase with the survey's
+           roofline.phases gives every HBM-bound build phase with its
            algorithmic bytes (scene box + boxes + Morton, the sort), and
            large.roofline_phases_lbvh the same plus the refit climb on the
            33,554,432-triangle LBVH.
@@ -204,7 +204,7 @@ def profile_phases(ctx, fn):
 
 
 def phase_rooflines(n, bits, phases, peak):
-    """HBM fractions of the build phases with the survey's algorithmic bytes
+    """HBM fractions of the build phases with their algorithmic bytes
     (K = key bytes, AABB = 24 B):
       scene box + boxes + Morton  36 n + n (12 idx + 36 verts + K + 4)
       radix sort                  n * P * 2 * (K + 4), P = ceil(bits / 8)
@@ -903,7 +903,7 @@ def main(argv=None):
     seg_ms = sum(phases_l.get("sort_segments", []))
     kb = 4 if cfg["bits"] <= 32 else 8
     lsd_passes = (cfg["bits"] + 7) // 8
-    sort_bytes = n * lsd_passes * 2 * (kb + 4)   # the survey's n * P * 2 * (K + 4)
+    sort_bytes = n * lsd_passes * 2 * (kb + 4)   # n * P * 2 * (K + 4): an 8-bit LSD sort's bytes
     sort_ms = sum(passes) + seg_ms
     pass_ms = float(np.mean(passes)) if passes else float("nan")
     achieved = sort_bytes / (sort_ms * 1e-3) / 1e9
@@ -937,7 +937,7 @@ def main(argv=None):
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes_per_launch": sort_bytes,
                      "algorithmic_bytes": f"n * {lsd_passes} * 2 * ({kb} + 4): the 8-bit LSD sort's key and value "
-                                          "reads and writes (survey formula), n = triangles",
+                                          "reads and writes, n = triangles",
                      "launch_ms": sort_ms, "per_pass_ms": pass_ms, "segments_ms": seg_ms,
                      "phases": phase_rooflines(n, cfg["bits"], phases_l, peak)},
         "clocks": clocks.summary(),
