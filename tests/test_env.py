@@ -7,7 +7,7 @@ import pytest
 import hippie_b200 as hp
 from hippie_b200 import HPError
 
-CFG1 = """
+PLOC_ENV = """
 Application {
     mode benchmark   # comment
 }
@@ -34,8 +34,8 @@ def test_defaults():
 
 
 def test_benchmark_config_file(tmp_path):
-    f = tmp_path / "cfg1.env"
-    f.write_text(CFG1)
+    f = tmp_path / "ploc_radius16.env"
+    f.write_text(PLOC_ENV)
     e = hp.Env().read_file(str(f))
     assert e.get_string("Application.mode") == "benchmark"
     p = e.build_params()
