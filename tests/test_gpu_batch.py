@@ -126,3 +126,34 @@ def test_batch_rejects_bad_input(ctx):
         hp.Batch(ctx, meshes, counts, hp.BuildParams(method="ploc", morton_bits=60))
     with pytest.raises(hp.HPError):
         hp.Batch(ctx, meshes * 20, counts * 20, hp.BuildParams(method="lbvh", morton_bits=60))
+
+
+def test_batch_wide_keys_equal_plain(ctx):
+    """60-bit Morton codes with the mesh index above them (62-bit keys) over
+    more than 2^20 triangles: the batch sorts them with the wide-key sort (three
+    passes over the top 24 bits, whose digit counts its Morton kernel takes,
+    then the segment sort); every mesh's BVH and hits equal the plain path's."""
+    sizes = [300000, 500000, 250000, 100000]
+    meshes, rays, counts = _setup(sizes, seed=77, rays_per_tri=2)
+    assert sum(sizes) >= 1 << 20
+    p = hp.BuildParams(method="lbvh", morton_bits=60)
+    batch = hp.Batch(ctx, meshes, counts, p)
+    R = torch.from_numpy(rays).cuda()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        res = batch.build_trace(R, results=torch.zeros((batch.num_rays, 4), dtype=torch.int32, device="cuda"))
+    s.synchronize()
+    ctx.check()
+    got = res.cpu().numpy()
+    for m, (V, T) in enumerate(meshes):
+        o0, o1 = batch.ray_offset(m), batch.ray_offset(m + 1)
+        plain = ctx.build(V, T, p)
+        pn, pw, pt = plain.download()
+        bn, bw, bt = batch.bvh(m).download()
+        np.testing.assert_array_equal(bn, pn)
+        np.testing.assert_array_equal(bt, pt)
+        np.testing.assert_array_equal(bw.view(np.int32), pw.view(np.int32))
+        Rm = R[o0:o1].contiguous()
+        exp = ctx.trace(plain, Rm, results=torch.zeros((Rm.shape[0], 4), dtype=torch.int32, device="cuda"))
+        np.testing.assert_array_equal(got[o0:o1], exp.cpu().numpy())
+    batch.close()
