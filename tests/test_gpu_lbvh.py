@@ -37,7 +37,8 @@ def build_with_taps(ctx, v, t, params):
 
 
 CASES = [("uniform", 2, 30), ("uniform", 3, 60), ("uniform", 1000, 30), ("uniform", 65536, 30),
-         ("uniform", 65536, 60), ("clustered", 100000, 60), ("clustered", 262144, 30)]
+         ("uniform", 65536, 60), ("clustered", 100000, 60), ("clustered", 262144, 30),
+         ("clustered", 1_200_000, 60)]  # over 2^20 keys of 60 bits: the wide-key sort
 
 
 def mesh(kind, n, seed):
