@@ -12,6 +12,9 @@
 //     and pushes the other hits farthest first, so the nearest of them is
 //     popped next; a sub-warp per ray left most lanes idle on nodes with few
 //     hit children and made every leaf's few triangles a shuffle reduction;
+//   * the first leaf a lane reaches is postponed until every lane still
+//     traversing holds one, then the leaves are tested together (as in the
+//     binary tracer);
 //   * persistent warps take rays with one atomic per warp when fewer than 20
 //     lanes still hold one, as in the binary tracer; the per-ray stack keeps
 //     its first entries in shared memory and the rest in local memory, and an
@@ -70,6 +73,7 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
     int hit = -1;  // leaf-ordered reference of the closest hit
     int64_t ray = -1;
     int node = SENT1, sp = 0, steps = 0, n_nodes = 0, n_tris = 0;
+    int leaf = 0;  // postponed leaf (~index), >= 0 when none
     bool exhausted = false;
     auto pop = [&]() {
         if (sp == 0) {
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
                     hit = -1; hit_u = hit_v = 0.0f;
                     sp = 0; steps = 0; n_nodes = n_tris = 0;
                     node = 0;
+                    leaf = 0;
                 } else {
                     exhausted = true;
                 }
@@ -125,6 +130,7 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
                     if (node >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
                         hp_report(err, HP_DEV_BAD_INDEX, node);
                         node = SENT1;
+                        leaf = 0;
                         break;
                     }
                     if (STATS) ++n_nodes;
@@ -177,16 +183,24 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
                             if (key[i] != 0xFFFFFFFFu) push(ref[i]);
                         node = ref[0];
                     }
+                    // The first leaf a lane reaches waits until every lane still
+                    // traversing holds one; then the leaves are tested together.
+                    if (node < 0 && leaf >= 0) {
+                        leaf = node;
+                        pop();
+                    }
+                    if (!__any_sync(__activemask(), leaf >= 0)) break;
                 }
-                // leaves
-                while (node < 0) {
-                    const int leaf = ~node;
-                    if (leaf >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
-                        hp_report(err, HP_DEV_BAD_INDEX, leaf);
+                // leaves: the postponed one, then `node` if it is a leaf too
+                while (leaf < 0) {
+                    const int li = ~leaf;
+                    if (li >= max_nodes || ++steps > TRAVERSAL_LIMIT) {
+                        hp_report(err, HP_DEV_BAD_INDEX, li);
                         node = SENT1;
+                        leaf = 0;
                         break;
                     }
-                    const int4 q = __ldg(nodes + (size_t)leaf * 2 * N + N);
+                    const int4 q = __ldg(nodes + (size_t)li * 2 * N + N);
                     int begin = q.z, end = q.w;
                     if (begin < 0 || end > num_refs || begin > end) {
                         hp_report(err, HP_DEV_BAD_INDEX, begin);
@@ -218,8 +232,9 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
                             }
                         }
                     }
-                    if (done) { sp = 0; node = SENT1; break; }
-                    pop();
+                    if (done) { sp = 0; node = SENT1; leaf = 0; break; }
+                    leaf = node;
+                    if (node < 0) pop();
                 }
                 if (node == SENT1) {
                     if (hit < 0) {
