@@ -21,11 +21,13 @@
 //      node starts from its binary children with the split of its budget and
 //      replaces, while it has fewer than N children, the first child whose
 //      split (l, r) has l + r < N by that child's two children (collapseWide);
-//      children whose budget says "leaf" become leaves. Per level one kernel
-//      counts the interior and leaf children, a scan places them, and a
-//      second kernel writes the next level, so interior nodes are numbered in
-//      breadth-first order and leaves after them in breadth-first order, as
-//      BVHConverter::convert numbers them;
+//      children whose budget says "leaf" become leaves. One cooperative
+//      launch runs every level (k_wide_levels): the CTAs count the interior
+//      and leaf children of their chunk of the level, and after a grid
+//      barrier each scans its chunk from the totals of the CTAs before it and
+//      writes the next level, so interior nodes are numbered in breadth-first
+//      order and leaves after them in breadth-first order, as
+//      BVHConverter::convert numbers them, with no host round trip;
 //   3. one kernel writes every wide node and the leaves below it, and walks
 //      each leaf's binary subtree (parent links, no stack) to write the leaf's
 //      references in left-first depth-first order with their Woop triangles.
@@ -207,40 +209,140 @@ __device__ int expand(const expand_args& E, const wide_entry& e, int* kv, int* k
     return m;
 }
 
-// Children counts of one level: interior into ni, leaves into nl.
-template <int N>
-__global__ void __launch_bounds__(WB) k_wide_count(expand_args E, const wide_entry* level, int m, int* ni, int* nl) {
-    const int i = blockIdx.x * WB + threadIdx.x;
-    if (i >= m) return;
-    int kv[N], kk[N], kb[N];
-    bool kl[N];
-    const int c = expand<N>(E, level[i], kv, kk, kb, kl);
-    if (c == 0) hp_report(E.err, HP_DEV_BAD_INDEX, level[i].v);
-    int a = 0, b = 0;
-    for (int j = 0; j < c; ++j) (kl[j] ? b : a)++;
-    ni[i] = a;
-    nl[i] = b;
+// All levels of the breadth-first expansion in one cooperative launch (the
+// counts, the exclusive scans and the placement of every level, with two grid
+// barriers a level instead of a host round trip). Level entries are split
+// into one contiguous chunk per CTA: a CTA counts its entries' interior and
+// leaf children, publishes its totals, and after the barrier takes its offset
+// from the totals of the CTAs before it and scans and places its chunk in
+// order. result[0] and result[1] receive the interior and leaf counts.
+constexpr int LB = 256;
+constexpr unsigned LEVEL_SPIN = 1u << 22;
+constexpr int LEVEL_MAX_CTAS = 1024;
+
+struct level_args {
+    expand_args E;
+    int n;
+    wide_entry* entries;  // [n]: level after level; the root is entries[0]
+    int2* kid_base;
+    int* ni;
+    int* nl;
+    int2* cta_sum;        // [grid]
+    unsigned* bar;        // [2] grid barrier words, zero
+    int* result;          // [2]
+    int* err;
+};
+
+__device__ __forceinline__ int2 lb_scan_excl(int x, int y, int2* s_w, int2& total) {
+    // exclusive block scan of (x, y) over LB threads
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ix = x, iy = y;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int ux = __shfl_up_sync(HP_FULL_MASK, ix, o), uy = __shfl_up_sync(HP_FULL_MASK, iy, o);
+        if (lane >= o) { ix += ux; iy += uy; }
+    }
+    if (lane == 31) s_w[warp] = make_int2(ix, iy);
+    __syncthreads();
+    int bx = 0, by = 0, tx = 0, ty = 0;
+#pragma unroll
+    for (int w = 0; w < LB / 32; ++w) {
+        const int2 v = s_w[w];
+        if (w < warp) { bx += v.x; by += v.y; }
+        tx += v.x; ty += v.y;
+    }
+    __syncthreads();
+    total = make_int2(tx, ty);
+    return make_int2(bx + ix - x, by + iy - y);
 }
 
-// Next level: interior children in order at next + int_off[i]; records where a
-// node's interior and leaf children start.
 template <int N>
-__global__ void __launch_bounds__(WB) k_wide_place(expand_args E, const wide_entry* level, int m, int base,
-                                                   const int* int_off, const int* leaf_off, wide_entry* next,
-                                                   int next_base, int leaf_before, int2* kid_base) {
-    const int i = blockIdx.x * WB + threadIdx.x;
-    if (i >= m) return;
-    int kv[N], kk[N], kb[N];
-    bool kl[N];
-    const int c = expand<N>(E, level[i], kv, kk, kb, kl);
-    int o = int_off[i];
-    for (int j = 0; j < c; ++j)
-        if (!kl[j]) next[o++] = wide_entry{kv[j], kk[j], kb[j], base + i};
-    kid_base[base + i] = make_int2(next_base + int_off[i], leaf_before + leaf_off[i]);
+__global__ void __launch_bounds__(LB) k_wide_levels(level_args L) {
+    __shared__ int2 s_w[LB / 32];
+    __shared__ int s_pre[4];
+    const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+    int base = 0, m = 1, leaves = 0;
+    while (m > 0) {
+        if (base + m > L.n) {  // every CTA sees the same counts
+            if (cta == 0 && tid == 0) hp_report(L.err, HP_DEV_BAD_INDEX, base + m);
+            break;
+        }
+        const wide_entry* level = L.entries + base;
+        const int chunk = (m + G - 1) / G;
+        const int lo = min(m, cta * chunk), hi = min(m, lo + chunk);
+        int a = 0, b = 0;
+        for (int i = lo + tid; i < hi; i += LB) {
+            int kv[N], kk[N], kb[N];
+            bool kl[N];
+            const int c = expand<N>(L.E, level[i], kv, kk, kb, kl);
+            if (c == 0) hp_report(L.err, HP_DEV_BAD_INDEX, level[i].v);
+            int x = 0, y = 0;
+            for (int j = 0; j < c; ++j) (kl[j] ? y : x)++;
+            L.ni[i] = x;
+            L.nl[i] = y;
+            a += x;
+            b += y;
+        }
+        int2 tot;
+        lb_scan_excl(a, b, s_w, tot);
+        if (tid == 0) __stcg(L.cta_sum + cta, tot);
+        if (!hp_grid_barrier(L.bar, L.err, LEVEL_SPIN)) return;
+        if (tid < 32) {  // this CTA's offset and the level's totals
+            int pa = 0, pb = 0, ta = 0, tb = 0;
+            for (int j = lane; j < G; j += 32) {
+                const int2 v = __ldcg(L.cta_sum + j);
+                if (j < cta) { pa += v.x; pb += v.y; }
+                ta += v.x;
+                tb += v.y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                pa += __shfl_xor_sync(HP_FULL_MASK, pa, o);
+                pb += __shfl_xor_sync(HP_FULL_MASK, pb, o);
+                ta += __shfl_xor_sync(HP_FULL_MASK, ta, o);
+                tb += __shfl_xor_sync(HP_FULL_MASK, tb, o);
+            }
+            if (lane == 0) { s_pre[0] = pa; s_pre[1] = pb; s_pre[2] = ta; s_pre[3] = tb; }
+        }
+        __syncthreads();
+        int run_a = s_pre[0], run_b = s_pre[1];
+        const int tot_a = s_pre[2], tot_b = s_pre[3];
+        const int next_base = base + m;
+        if (next_base + tot_a > L.n) {
+            if (cta == 0 && tid == 0) hp_report(L.err, HP_DEV_BAD_INDEX, next_base + tot_a);
+            break;
+        }
+        for (int r0 = lo; r0 < hi; r0 += LB) {  // uniform over the CTA
+            const int i = r0 + tid;
+            const int x = i < hi ? __ldcg(L.ni + i) : 0, y = i < hi ? __ldcg(L.nl + i) : 0;
+            int2 sum;
+            const int2 ex = lb_scan_excl(x, y, s_w, sum);
+            if (i < hi) {
+                int kv[N], kk[N], kb[N];
+                bool kl[N];
+                const int c = expand<N>(L.E, level[i], kv, kk, kb, kl);
+                int o = next_base + run_a + ex.x;
+                for (int j = 0; j < c; ++j)
+                    if (!kl[j]) L.entries[o++] = wide_entry{kv[j], kk[j], kb[j], base + i};
+                L.kid_base[base + i] = make_int2(next_base + run_a + ex.x, leaves + run_b + ex.y);
+            }
+            run_a += sum.x;
+            run_b += sum.y;
+        }
+        if (!hp_grid_barrier(L.bar, L.err, LEVEL_SPIN)) return;
+        leaves += tot_b;
+        base = next_base;
+        m = tot_a;
+    }
+    if (cta == 0 && tid == 0) {
+        L.result[0] = base;
+        L.result[1] = leaves;
+    }
 }
 
 struct emit_args {
-    int n, num_interior, num_refs;
+    int n, num_refs;
+    const int* counts;          // [0] interior records, [1] leaf records (k_wide_levels)
     const wide_entry* entries;  // [num_interior], breadth-first
     const int2* kid_base;
     const int* parent;
@@ -268,7 +370,8 @@ __device__ __forceinline__ void put_child(int4* nd, int i, const float4& mn, con
 template <int N>
 __global__ void __launch_bounds__(WB) k_wide_emit(expand_args E, emit_args M) {
     const int w = blockIdx.x * WB + threadIdx.x;
-    if (w >= M.num_interior) return;
+    const int num_interior = __ldg(M.counts);
+    if (w >= num_interior) return;
     const wide_entry e = M.entries[w];
     int kv[N], kk[N], kb[N];
     bool kl[N];
@@ -277,7 +380,7 @@ __global__ void __launch_bounds__(WB) k_wide_emit(expand_args E, emit_args M) {
     const int2 base = M.kid_base[w];
     int ni = 0, nl = 0;
     int refs[N];
-    for (int j = 0; j < c; ++j) refs[j] = kl[j] ? ~(M.num_interior + base.y + nl++) : base.x + ni++;
+    for (int j = 0; j < c; ++j) refs[j] = kl[j] ? ~(num_interior + base.y + nl++) : base.x + ni++;
     // spare words: child N-3 -> count, N-2 -> size, N-1 -> parent
     int spare[N];
     for (int i = 0; i < N; ++i) spare[i] = 0;
@@ -338,10 +441,10 @@ __global__ void __launch_bounds__(WB) k_wide_emit(expand_args E, emit_args M) {
     }
 }
 
-__global__ void k_wide_info(hp_bvh_info* info, int ni, int nl) {
+__global__ void k_wide_info(hp_bvh_info* info, const int* counts) {
     if (threadIdx.x == 0) {
-        info->num_interior = ni;
-        info->num_leaf = nl;
+        info->num_interior = counts[0];
+        info->num_leaf = counts[1];
     }
 }
 
@@ -389,10 +492,8 @@ hp_status wide_collapse_t(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, v
     int2* kid_base = cv.take<int2>(n);
     int* ni = cv.take<int>(n);
     int* nl = cv.take<int>(n);
-    int* oi = cv.take<int>(n);
-    int* ol = cv.take<int>(n);
-    int* totals = cv.take<int>(2);
-    void* scan = cv.take<char>(hp_scan2_scratch_bytes(n));
+    int2* cta_sum = cv.take<int2>(LEVEL_MAX_CTAS);
+    int* ctl = cv.take<int>(16);  // [0..1] grid barrier, [4..5] interior / leaf record counts
 
     HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
     wide_args A{n, in.parent, in.left, in.right, in.nbmin, in.nbmax, in.ct, in.ci, in.max_leaf,
@@ -405,32 +506,21 @@ hp_status wide_collapse_t(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, v
     expand_args E{n, in.left, in.right, cnt, size, root_split, err};
     const wide_entry root{0, 1, 0, -1};
     HP_CUDA(cudaMemcpyAsync(entries, &root, sizeof(root), cudaMemcpyHostToDevice, s));
-    int base = 0, m = 1, leaves = 0;
-    int host_tot[2];
-    while (m > 0) {
-        if (base + m > n) return hp_fail(HP_ERR_DEVICE_STATUS, "wide collapse: more interior nodes than references");
-        const wide_entry* level = entries + base;
-        k_wide_count<N><<<hp_div_up(m, WB), WB, 0, s>>>(E, level, m, ni, nl);
-        hp_scan2_sum(ni, m, nl, m, oi, ol, totals, scan, err, s);
-        HP_CUDA(cudaMemcpyAsync(host_tot, totals, sizeof(host_tot), cudaMemcpyDeviceToHost, s));
-        HP_CUDA(cudaStreamSynchronize(s));
-        HP_TRY(hp_ctx_check(ctx, s));
-        const int next_base = base + m;
-        if (next_base + host_tot[0] > n) return hp_fail(HP_ERR_DEVICE_STATUS, "wide collapse: level overflow");
-        k_wide_place<N><<<hp_div_up(m, WB), WB, 0, s>>>(E, level, m, base, oi, ol, entries + next_base, next_base,
-                                                       leaves, kid_base);
-        HP_CUDA(cudaGetLastError());
-        hp_count_launch(2);
-        leaves += host_tot[1];
-        base = next_base;
-        m = host_tot[0];
-    }
-    const int num_interior = base;
-    emit_args M{n, num_interior, n, entries, kid_base, in.parent, in.left, in.right, in.nbmin, in.nbmax,
+    HP_CUDA(cudaMemsetAsync(ctl, 0, 16 * sizeof(int), s));
+    int per_sm = 0;
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wide_levels<N>, LB, 0));
+    if (per_sm < 1) return hp_fail(HP_ERR_UNSUPPORTED, "wide collapse: level kernel does not fit on an SM");
+    const int grid = std::min(ctx->sm_count * std::min(per_sm, 4), LEVEL_MAX_CTAS);
+    level_args L{E, n, entries, kid_base, ni, nl, cta_sum, reinterpret_cast<unsigned*>(ctl),
+                 ctl + 4, err};
+    void* largs[] = {&L};
+    HP_CUDA(cudaLaunchCooperativeKernel((void*)k_wide_levels<N>, grid, LB, largs, 0, s));
+    hp_count_launch();
+    emit_args M{n, n, ctl + 4, entries, kid_base, in.parent, in.left, in.right, in.nbmin, in.nbmax,
                 in.sorted_tri, in.reorder, out->tri_idx, out->woop, in.verts, in.nv, in.tris,
                 reinterpret_cast<int4*>(out->nodes), err};
-    k_wide_emit<N><<<hp_div_up(num_interior, WB), WB, 0, s>>>(E, M);
-    k_wide_info<<<1, 32, 0, s>>>(out->info, num_interior, leaves);
+    k_wide_emit<N><<<hp_div_up(n, WB), WB, 0, s>>>(E, M);  // threads beyond the interior count leave
+    k_wide_info<<<1, 32, 0, s>>>(out->info, ctl + 4);
     HP_CUDA(cudaGetLastError());
     hp_count_launch(2);
     hp_mark(ctx, s, "wide_collapse");
@@ -448,8 +538,8 @@ size_t hp_wide_scratch_bytes(int64_t n, int width) {
     b += hp_carve::pad(n * 4) + hp_carve::pad(4);    // sizes, root split
     b += hp_carve::pad(n * sizeof(wide_entry));      // breadth-first entries
     b += hp_carve::pad(n * 8);                       // child bases
-    b += 4 * hp_carve::pad(n * 4) + hp_carve::pad(8);  // counts, offsets, totals
-    b += hp_scan2_scratch_bytes(n);
+    b += 2 * hp_carve::pad(n * 4);                   // child counts of a level
+    b += hp_carve::pad(LEVEL_MAX_CTAS * 8) + hp_carve::pad(64);  // CTA totals, barrier and counts
     return b;
 }
 
