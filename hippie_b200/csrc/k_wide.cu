@@ -343,6 +343,7 @@ __global__ void __launch_bounds__(LB) k_wide_levels(level_args L) {
 struct emit_args {
     int n, num_refs;
     const int* counts;          // [0] interior records, [1] leaf records (k_wide_levels)
+    int4* leaf_task;            // per leaf record: binary node, first reference, size, parent
     const wide_entry* entries;  // [num_interior], breadth-first
     const int2* kid_base;
     const int* parent;
@@ -394,50 +395,63 @@ __global__ void __launch_bounds__(WB) k_wide_emit(expand_args E, emit_args M) {
         if (i < c) put_child<N>(nd, i, __ldg(M.nbmin + kv[i]), __ldg(M.nbmax + kv[i]), refs[i], spare[i]);
         else put_child<N>(nd, i, mn0, mn0, d0, spare[i]);
     }
-    // the leaves below this node
+    // the leaves below this node: one task each for k_wide_leaf_emit
     for (int j = 0; j < c; ++j) {
         if (!kl[j]) continue;
         const int li = ~refs[j];
-        const int v = kv[j], b = kb[j], s = size_of(E, v);
-        const float4 mn = __ldg(M.nbmin + v), mx = __ldg(M.nbmax + v);
-        int4* lf = M.nodes + (size_t)li * 2 * N;
-        for (int i = 0; i < N; ++i) {
-            int sp = 0;
-            if (i == N - 3) sp = 0;
-            else if (i == N - 2) sp = ~s;
-            else if (i == N - 1) sp = w;
-            if (i == 0) put_child<N>(lf, 0, mn, mx, b, b + s);
-            else put_child<N>(lf, i, mn, mx, 0, sp);
-        }
-        if (b < 0 || b + s > M.num_refs) { hp_report(M.err, HP_DEV_BAD_INDEX, v); continue; }
-        if (!M.reorder) continue;
-        // the binary subtree's leaves, left first, through the parent links
-        const int n = M.n;
-        int x = v, pos = b, guard = 0;
-        while (x < n - 1) x = __ldg(M.left + x);
+        M.leaf_task[li - num_interior] = make_int4(kv[j], kb[j], size_of(E, kv[j]), w);
+    }
+}
+
+// One thread per leaf record: its N child slots (the leaf box in each, the
+// reference range in slot 0, size and parent in the spare words), and, when
+// the references are reordered, the binary subtree's leaves walked left first
+// through the parent links (no stack) with their triangle ids and Woop rows.
+template <int N>
+__global__ void __launch_bounds__(WB) k_wide_leaf_emit(expand_args E, emit_args M) {
+    const int t = blockIdx.x * WB + threadIdx.x;
+    const int num_interior = __ldg(M.counts), num_leaf = __ldg(M.counts + 1);
+    if (t >= num_leaf) return;
+    const int4 task = M.leaf_task[t];
+    const int li = num_interior + t, v = task.x, b = task.y, s = task.z, w = task.w;
+    const int n = M.n;
+    if ((unsigned)v >= (unsigned)(2 * n - 1)) { hp_report(M.err, HP_DEV_BAD_INDEX, v); return; }
+    const float4 mn = __ldg(M.nbmin + v), mx = __ldg(M.nbmax + v);
+    int4* lf = M.nodes + (size_t)li * 2 * N;
+    for (int i = 0; i < N; ++i) {
+        int sp = 0;
+        if (i == N - 3) sp = 0;
+        else if (i == N - 2) sp = ~s;
+        else if (i == N - 1) sp = w;
+        if (i == 0) put_child<N>(lf, 0, mn, mx, b, b + s);
+        else put_child<N>(lf, i, mn, mx, 0, sp);
+    }
+    if (b < 0 || b + s > M.num_refs) { hp_report(M.err, HP_DEV_BAD_INDEX, v); return; }
+    if (!M.reorder) return;
+    int x = v, pos = b, guard = 0;
+    while (x < n - 1) x = __ldg(M.left + x);
+    while (true) {
+        if (pos >= b + s || ++guard > 4 * s + 4) { hp_report(M.err, HP_DEV_BAD_INDEX, v); break; }
+        const int tri = __ldg(M.sorted_tri + (x - (n - 1)));
+        M.tri_out[pos] = tri;
+        tri_verts tv = load_tri(M.verts, M.nv, M.tris, tri, M.err);
+        float4 w0, w1, w2;
+        hp_woop(tv.x0, tv.y0, tv.z0, tv.x1, tv.y1, tv.z1, tv.x2, tv.y2, tv.z2, w0, w1, w2);
+        M.woop[3 * (int64_t)pos] = w0;
+        M.woop[3 * (int64_t)pos + 1] = w1;
+        M.woop[3 * (int64_t)pos + 2] = w2;
+        ++pos;
+        // next leaf: climb while x is a right child, then step right and descend left
+        bool done = false;
         while (true) {
-            if (pos >= b + s || ++guard > 4 * s + 4) { hp_report(M.err, HP_DEV_BAD_INDEX, v); break; }
-            const int tri = __ldg(M.sorted_tri + (x - (n - 1)));
-            M.tri_out[pos] = tri;
-            tri_verts t = load_tri(M.verts, M.nv, M.tris, tri, M.err);
-            float4 w0, w1, w2;
-            hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
-            M.woop[3 * (int64_t)pos] = w0;
-            M.woop[3 * (int64_t)pos + 1] = w1;
-            M.woop[3 * (int64_t)pos + 2] = w2;
-            ++pos;
-            // next leaf: climb while x is a right child, then step right and descend left
-            bool done = false;
-            while (true) {
-                if (x == v) { done = true; break; }
-                const int p = __ldg(M.parent + x);
-                if (p < 0) { done = true; break; }
-                if (__ldg(M.left + p) == x) { x = __ldg(M.right + p); break; }
-                x = p;
-            }
-            if (done) break;
-            while (x < n - 1) x = __ldg(M.left + x);
+            if (x == v) { done = true; break; }
+            const int p = __ldg(M.parent + x);
+            if (p < 0) { done = true; break; }
+            if (__ldg(M.left + p) == x) { x = __ldg(M.right + p); break; }
+            x = p;
         }
+        if (done) break;
+        while (x < n - 1) x = __ldg(M.left + x);
     }
 }
 
@@ -494,6 +508,7 @@ hp_status wide_collapse_t(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, v
     int* nl = cv.take<int>(n);
     int2* cta_sum = cv.take<int2>(LEVEL_MAX_CTAS);
     int* ctl = cv.take<int>(16);  // [0..1] grid barrier, [4..5] interior / leaf record counts
+    int4* leaf_task = cv.take<int4>(n);
 
     HP_CUDA(cudaMemsetAsync(counters, 0, (size_t)n * 4, s));
     wide_args A{n, in.parent, in.left, in.right, in.nbmin, in.nbmax, in.ct, in.ci, in.max_leaf,
@@ -516,13 +531,15 @@ hp_status wide_collapse_t(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, v
     void* largs[] = {&L};
     HP_CUDA(cudaLaunchCooperativeKernel((void*)k_wide_levels<N>, grid, LB, largs, 0, s));
     hp_count_launch();
-    emit_args M{n, n, ctl + 4, entries, kid_base, in.parent, in.left, in.right, in.nbmin, in.nbmax,
+    hp_mark(ctx, s, "wide_levels");
+    emit_args M{n, n, ctl + 4, leaf_task, entries, kid_base, in.parent, in.left, in.right, in.nbmin, in.nbmax,
                 in.sorted_tri, in.reorder, out->tri_idx, out->woop, in.verts, in.nv, in.tris,
                 reinterpret_cast<int4*>(out->nodes), err};
     k_wide_emit<N><<<hp_div_up(n, WB), WB, 0, s>>>(E, M);  // threads beyond the interior count leave
+    k_wide_leaf_emit<N><<<hp_div_up(n, WB), WB, 0, s>>>(E, M);  // threads beyond the leaf count leave
     k_wide_info<<<1, 32, 0, s>>>(out->info, ctl + 4);
     HP_CUDA(cudaGetLastError());
-    hp_count_launch(2);
+    hp_count_launch(3);
     hp_mark(ctx, s, "wide_collapse");
     return HP_OK;
 }
@@ -540,6 +557,7 @@ size_t hp_wide_scratch_bytes(int64_t n, int width) {
     b += hp_carve::pad(n * 8);                       // child bases
     b += 2 * hp_carve::pad(n * 4);                   // child counts of a level
     b += hp_carve::pad(LEVEL_MAX_CTAS * 8) + hp_carve::pad(64);  // CTA totals, barrier and counts
+    b += hp_carve::pad(n * 16);                      // leaf tasks
     return b;
 }
 
