@@ -185,13 +185,17 @@ __device__ int expand(const expand_args& E, const wide_entry& e, int* kv, int* k
     if (c == CNT_LEAF) c = (uint16_t)__ldg(E.root_split);  // only the root can be here
     const int l0 = __ldg(E.left + e.v), r0 = __ldg(E.right + e.v);
     if ((unsigned)l0 >= (unsigned)nn || (unsigned)r0 >= (unsigned)nn) return 0;
+    // each child's split is read once, when the child enters the list
+    uint16_t cs[N];
     kv[0] = l0; kk[0] = c & 0xFF; kb[0] = e.begin;
     kv[1] = r0; kk[1] = c >> 8; kb[1] = e.begin + size_of(E, l0);
+    cs[0] = cnt_of<N>(E, l0, kk[0]);
+    cs[1] = cnt_of<N>(E, r0, kk[1]);
     int m = 2;
     while (m < N) {
         int s = -1, l = 0, r = 0;
         for (int i = 0; i < m; ++i) {
-            const uint16_t ci = cnt_of<N>(E, kv[i], kk[i]);
+            const uint16_t ci = cs[i];
             if (ci == CNT_LEAF) continue;
             const int li = ci & 0xFF, ri = ci >> 8;
             if (li > 0 && ri > 0 && li + ri < N) { s = i; l = li; r = ri; break; }
@@ -200,12 +204,14 @@ __device__ int expand(const expand_args& E, const wide_entry& e, int* kv, int* k
         const int x = kv[s], b = kb[s];
         const int xl = __ldg(E.left + x), xr = __ldg(E.right + x);
         if ((unsigned)xl >= (unsigned)nn || (unsigned)xr >= (unsigned)nn) return 0;
-        for (int i = m; i > s + 1; --i) { kv[i] = kv[i - 1]; kk[i] = kk[i - 1]; kb[i] = kb[i - 1]; }
+        for (int i = m; i > s + 1; --i) { kv[i] = kv[i - 1]; kk[i] = kk[i - 1]; kb[i] = kb[i - 1]; cs[i] = cs[i - 1]; }
         kv[s] = xl; kk[s] = l; kb[s] = b;
         kv[s + 1] = xr; kk[s + 1] = r; kb[s + 1] = b + size_of(E, xl);
+        cs[s] = cnt_of<N>(E, xl, l);
+        cs[s + 1] = cnt_of<N>(E, xr, r);
         ++m;
     }
-    for (int i = 0; i < m; ++i) kl[i] = cnt_of<N>(E, kv[i], kk[i]) == CNT_LEAF;
+    for (int i = 0; i < m; ++i) kl[i] = cs[i] == CNT_LEAF;
     return m;
 }
 
