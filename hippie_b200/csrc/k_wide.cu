@@ -267,6 +267,9 @@ __global__ void __launch_bounds__(LB) k_wide_levels(level_args L) {
     __shared__ int2 s_w[LB / 32];
     __shared__ int s_pre[4];
     const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+    // the root entry (binary root 0 with the whole budget); the same thread
+    // expands it in the first level (chunk 0 of one entry)
+    if (cta == 0 && tid == 0) L.entries[0] = wide_entry{0, 1, 0, -1};
     int base = 0, m = 1, leaves = 0;
     while (m > 0) {
         if (base + m > L.n) {  // every CTA sees the same counts
@@ -525,8 +528,6 @@ hp_status wide_collapse_t(hp_ctx* ctx, const hp_wide_in& in, hp_bvh_impl* out, v
     hp_mark(ctx, s, "wide_costs");
 
     expand_args E{n, in.left, in.right, cnt, size, root_split, err};
-    const wide_entry root{0, 1, 0, -1};
-    HP_CUDA(cudaMemcpyAsync(entries, &root, sizeof(root), cudaMemcpyHostToDevice, s));
     HP_CUDA(cudaMemsetAsync(ctl, 0, 16 * sizeof(int), s));
     int per_sm = 0;
     HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wide_levels<N>, LB, 0));
