@@ -534,14 +534,12 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
     // hp_trace does for a batch of that size.
     const int sort_bits = 30;
     const bool sorted = ctx->tune.trace_sorted && C >= 65536 && C < (int64_t(1) << 30);
-    const hp_sort_plan plan = hp_sort_make_plan(std::max<int64_t>(C, 1), 8, sort_bits, ctx->tune.sort_block);
     // slot layout: rays (32 B per ray), results (16 B), stats (8 B), then, when
-    // sorting, keys, sorted keys, order and the sort's scratch and histograms
+    // sorting, the order and the ray sort's keys and scratch
     const size_t ray_b = hp_carve::pad((size_t)C * 32), res_b = hp_carve::pad((size_t)C * 16);
     const size_t st_b = hp_carve::pad((size_t)C * 8);
-    const size_t sort_b = sorted ? 2 * hp_carve::pad((size_t)C * 8) + hp_carve::pad((size_t)C * 4) +
-                                       hp_carve::pad(plan.scratch_bytes) +
-                                       hp_carve::pad(hp_sort_hist_bytes(plan.passes))
+    const size_t sort_b = sorted ? hp_carve::pad((size_t)C * 4) + hp_ray_order_scratch_bytes(C, sort_bits,
+                                                                                              ctx->tune.sort_block)
                                  : 0;
     const size_t need = ray_b + res_b + st_b + sort_b;
     if (!ctx->io_h2d) {
@@ -612,15 +610,9 @@ hp_status hp_trace_host(hp_ctx* ctx, const hp_bvh* bvh, const float* rays_host, 
         HP_CUDA(cudaMemsetAsync(d_res, 0, (size_t)m * 16, t));
         const int32_t* order = nullptr;
         if (sorted && m >= 65536) {
-            uint64_t* keys = cv.take<uint64_t>((size_t)C);
-            uint64_t* skeys = cv.take<uint64_t>((size_t)C);
             int32_t* ord = cv.take<int32_t>((size_t)C);
-            void* scratch = cv.take<char>(plan.scratch_bytes);
-            uint32_t* hist = cv.take<uint32_t>((size_t)plan.passes * 256);
-            const hp_sort_plan pm = hp_sort_make_plan(m, 8, sort_bits, ctx->tune.sort_block);
-            HP_TRY(hp_ray_keys(ctx, d_rays, m, nullptr, sort_bits, keys, t));
-            hp_sort_args sa{keys, nullptr, skeys, ord, scratch, hist, false, ctx->d_status, nullptr};
-            HP_TRY(hp_sort_run(pm, sa, t));
+            void* scratch = cv.take<char>(hp_ray_order_scratch_bytes(C, sort_bits, ctx->tune.sort_block));
+            HP_TRY(hp_ray_order(ctx, d_rays, m, sort_bits, ord, scratch, t));
             order = ord;
         }
         HP_TRY(hp_trace_launch(ctx, bi, bvh->num_refs, d_rays, m, d_res, d_stats, flags, t, order, counter));

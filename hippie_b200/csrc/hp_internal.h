@@ -191,6 +191,14 @@ struct hp_sort_args {
     hp_ctx* ctx;                   // for phase marks (may be null)
 };
 hp_status hp_sort_run(const hp_sort_plan& plan, const hp_sort_args& a, cudaStream_t stream);
+
+// Ray order of a sorted trace: the context's ray keys of `bits` bits
+// (32-bit keys with the digit histograms made in the key kernel when bits <=
+// 32), stably sorted; order[k] is the k-th ray. Scratch of
+// hp_ray_order_scratch_bytes(n, bits, ctx->tune.sort_block) bytes.
+size_t hp_ray_order_scratch_bytes(int64_t n, int bits, int block);
+hp_status hp_ray_order(hp_ctx* ctx, const float* rays, int64_t n, int bits, int32_t* order, void* scratch,
+                       cudaStream_t s);
 size_t hp_sort_hist_bytes(int passes);
 
 // ---- single-pass scans --------------------------------------------------------

@@ -260,6 +260,25 @@ __global__ void __launch_bounds__(256) k_ray_keys(const float4* __restrict__ ray
     keys[i] = k.bits == 64 ? c : c >> (64 - k.bits);
 }
 
+// Keys of at most 32 bits for a sorted trace, with the sort's digit histograms
+// (passes x 256, digit p at bits 8p) counted in shared memory as they are made.
+template <int M>
+__global__ void __launch_bounds__(256) k_ray_keys32(const float4* __restrict__ rays, int64_t n, key_args k,
+                                                    uint32_t* __restrict__ keys, uint32_t* hist, int passes) {
+    __shared__ uint32_t sh[4 * 256];
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = ray_code<M>(__ldg(rays + 2 * i), __ldg(rays + 2 * i + 1), k);
+        const uint32_t key = (uint32_t)(c >> (64 - k.bits));
+        keys[i] = key;
+        for (int p = 0; p < passes; ++p) atomicAdd(&sh[p * 256 + ((key >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
 // halton (RayGenKernels.cu:20-30): radical inverse of i in the given base.
 float halton(int i, int base) {
     double r = 0.0, f = 1.0 / base;
@@ -442,6 +461,65 @@ extern "C" hp_status hp_ray_keys(hp_ctx* ctx, const float* rays, int64_t num_ray
     return HP_OK;
 }
 
+namespace {
+
+key_args unit_key_args(const hp_ctx* ctx, int bits) {
+    key_args k{};
+    for (int a = 0; a < 3; ++a) {
+        k.mn[a] = 0.0f;
+        k.mx[a] = 1.0f;
+        k.inv[a] = 1.0f;
+    }
+    k.bits = bits;
+    k.ray_length = ctx->ray_length;
+    return k;
+}
+
+}  // namespace
+
+size_t hp_ray_order_scratch_bytes(int64_t n, int bits, int block) {
+    const int kb = bits <= 32 ? 4 : 8;
+    const hp_sort_plan plan = hp_sort_make_plan(std::max<int64_t>(n, 1), kb, bits, block);
+    return 2 * hp_carve::pad((size_t)n * kb) + hp_carve::pad(plan.scratch_bytes) +
+           hp_carve::pad(hp_sort_hist_bytes(plan.passes));
+}
+
+hp_status hp_ray_order(hp_ctx* ctx, const float* rays, int64_t n, int bits, int32_t* order, void* scratch,
+                       cudaStream_t s) {
+    if (n <= 0) return HP_OK;
+    const int kb = bits <= 32 ? 4 : 8;
+    const hp_sort_plan plan = hp_sort_make_plan(n, kb, bits, ctx->tune.sort_block);
+    hp_carve cv(reinterpret_cast<char*>(scratch));
+    void* keys = cv.take<char>((size_t)n * kb);
+    void* skeys = cv.take<char>((size_t)n * kb);
+    void* sort_scratch = cv.take<char>(plan.scratch_bytes);
+    uint32_t* hist = cv.take<uint32_t>((size_t)plan.passes * 256);
+    if (kb == 8) {  // wide keys: the public key kernel, histograms by the sort
+        HP_TRY(hp_ray_keys(ctx, rays, n, nullptr, bits, reinterpret_cast<uint64_t*>(keys), s));
+        hp_sort_args sa{keys, nullptr, skeys, order, sort_scratch, hist, false, ctx->d_status, nullptr};
+        return hp_sort_run(plan, sa, s);
+    }
+    HP_CUDA(cudaMemsetAsync(hist, 0, hp_sort_hist_bytes(plan.passes), s));
+    const key_args k = unit_key_args(ctx, bits);
+    const unsigned grid = (unsigned)std::min<int64_t>(hp_div_up(n, 256), (int64_t)ctx->sm_count * 8);
+    const float4* r4 = reinterpret_cast<const float4*>(rays);
+    uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
+    const int P = plan.passes;
+    switch (ctx->ray_key_method) {
+        case HP_RAY_KEYS_TWO_POINT: k_ray_keys32<HP_RAY_KEYS_TWO_POINT><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        case HP_RAY_KEYS_PARABOLOID: k_ray_keys32<HP_RAY_KEYS_PARABOLOID><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        case HP_RAY_KEYS_OCTAHEDRON: k_ray_keys32<HP_RAY_KEYS_OCTAHEDRON><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        case HP_RAY_KEYS_ORIGIN: k_ray_keys32<HP_RAY_KEYS_ORIGIN><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        case HP_RAY_KEYS_COSTA: k_ray_keys32<HP_RAY_KEYS_COSTA><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        case HP_RAY_KEYS_REIS: k_ray_keys32<HP_RAY_KEYS_REIS><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+        default: k_ray_keys32<HP_RAY_KEYS_AILA><<<grid, 256, 0, s>>>(r4, n, k, k32, hist, P); break;
+    }
+    HP_CUDA(cudaGetLastError());
+    hp_count_launch();
+    hp_sort_args sa{keys, nullptr, skeys, order, sort_scratch, hist, true, ctx->d_status, nullptr};
+    return hp_sort_run(plan, sa, s);
+}
+
 // RayBuffer::setMortonCodeMethod / setRayLength (rt/ray/RayBuffer.cpp:167-195).
 extern "C" hp_status hp_ctx_set_ray_keys(hp_ctx* ctx, int32_t method, float ray_length) {
     if (!ctx) return hp_fail(HP_ERR_ARG, "hp_ctx_set_ray_keys: null context");
@@ -475,21 +553,14 @@ extern "C" hp_status hp_trace_sorted(hp_ctx* ctx, const hp_bvh* bvh, const float
     if (num_rays >= (int64_t(1) << 30)) return hp_fail(HP_ERR_ARG, "hp_trace_sorted: too many rays");
     if (num_rays == 0) return HP_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const hp_sort_plan plan = hp_sort_make_plan(num_rays, 8, bits, ctx->tune.sort_block);
-    size_t need = 2 * hp_carve::pad(num_rays * 8) + hp_carve::pad(num_rays * 4) + hp_carve::pad(plan.scratch_bytes) +
-                  hp_carve::pad(hp_sort_hist_bytes(plan.passes));
-    HP_TRY(hp_ctx_reserve(ctx, need, s));
+    const size_t key_bytes = hp_ray_order_scratch_bytes(num_rays, bits, ctx->tune.sort_block);
+    HP_TRY(hp_ctx_reserve(ctx, hp_carve::pad(num_rays * 4) + key_bytes, s));
     hp_carve cv(ctx->arena);
-    uint64_t* keys = cv.take<uint64_t>(num_rays);
-    uint64_t* skeys = cv.take<uint64_t>(num_rays);
     int32_t* order_tmp = cv.take<int32_t>(num_rays);
     int32_t* order = order_out ? order_out : order_tmp;
-    void* scratch = cv.take<char>(plan.scratch_bytes);
-    uint32_t* hist = cv.take<uint32_t>(plan.passes * 256);
+    void* scratch = cv.take<char>(key_bytes);
     hp_mark(ctx, s, "ray_sort_begin");
-    HP_TRY(hp_ray_keys(ctx, rays, num_rays, nullptr, bits, keys, stream));
-    hp_sort_args sa{keys, nullptr, skeys, order, scratch, hist, false, ctx->d_status, nullptr};
-    HP_TRY(hp_sort_run(plan, sa, s));
+    HP_TRY(hp_ray_order(ctx, rays, num_rays, bits, order, scratch, s));
     hp_mark(ctx, s, "ray_sort");
     return hp_trace_launch(ctx, reinterpret_cast<const hp_bvh_impl*>(bvh->impl), bvh->num_refs, rays, num_rays,
                            results, stats, flags, s, order);
