@@ -128,9 +128,12 @@ __device__ __forceinline__ int radius_at(const ploc_args& a, int it) {
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err) { return hp_grid_barrier(bar, err, SPIN); }
 
 // Create node `node` = merge of clusters with node ids a (left) and b (right).
-__device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a, int b) {
-    const float4 amn = __ldcg(A.nbmin + a), amx = __ldcg(A.nbmax + a);
-    const float4 bmn = __ldcg(A.nbmin + b), bmx = __ldcg(A.nbmax + b);
+// From the children's boxes (w: cost / size bits) and counts; returns the new
+// node's min corner with its cost, max corner with its size, and its counts.
+__device__ __forceinline__ void make_parent_from(const ploc_args& A, int node, int a, int b, const float4& amn,
+                                                 const float4& amx, const float4& bmn, const float4& bmx,
+                                                 const int2& ca, const int2& cb, float4& omn, float4& omx,
+                                                 int2& ocnt) {
     const float mnx = fminf(amn.x, bmn.x), mny = fminf(amn.y, bmn.y), mnz = fminf(amn.z, bmn.z);
     const float mxx = fmaxf(amx.x, bmx.x), mxy = fmaxf(amx.y, bmx.y), mxz = fmaxf(amx.z, bmx.z);
     const int size = __float_as_int(amx.w) + __float_as_int(bmx.w);
@@ -146,10 +149,12 @@ __device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a,
         st = (size <= A.max_leaf) ? 0 : 1;
         c = 0.0f;
     }
-    const int2 ca = __ldcg(A.counts + a), cb = __ldcg(A.counts + b);
-    __stcg(A.nbmin + node, make_float4(mnx, mny, mnz, c));
-    __stcg(A.nbmax + node, make_float4(mxx, mxy, mxz, __int_as_float(size)));
-    __stcg(A.counts + node, st ? make_int2(1 + ca.x + cb.x, ca.y + cb.y) : make_int2(0, 1));
+    omn = make_float4(mnx, mny, mnz, c);
+    omx = make_float4(mxx, mxy, mxz, __int_as_float(size));
+    ocnt = st ? make_int2(1 + ca.x + cb.x, ca.y + cb.y) : make_int2(0, 1);
+    __stcg(A.nbmin + node, omn);
+    __stcg(A.nbmax + node, omx);
+    __stcg(A.counts + node, ocnt);
     A.state[node] = (uint8_t)st;
     A.left[node] = a;
     A.right[node] = b;
@@ -162,6 +167,15 @@ __device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a,
         __stcg(cbx + 1, make_float4(bmn.x, bmx.x, bmn.y, bmx.y));
         __stcg(cbx + 2, make_float4(amn.z, amx.z, bmn.z, bmx.z));
     }
+}
+
+__device__ __forceinline__ void make_parent(const ploc_args& A, int node, int a, int b) {
+    const float4 amn = __ldcg(A.nbmin + a), amx = __ldcg(A.nbmax + a);
+    const float4 bmn = __ldcg(A.nbmin + b), bmx = __ldcg(A.nbmax + b);
+    const int2 ca = __ldcg(A.counts + a), cb = __ldcg(A.counts + b);
+    float4 omn, omx;
+    int2 ocnt;
+    make_parent_from(A, node, a, b, amn, amx, bmn, bmx, ca, cb, omn, omx, ocnt);
 }
 
 // Leaves: sorted reference p becomes leaf node n-1+p and cluster p.
@@ -528,7 +542,7 @@ __global__ void __launch_bounds__(LPB, 2) k_ploc_loop(ploc_args A) {
 }
 
 // Finish the last <= TAIL clusters in one CTA.
-constexpr size_t TAIL_SMEM = 8 * TAIL * sizeof(float);
+constexpr size_t TAIL_SMEM = 12 * TAIL * sizeof(float);
 
 __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
     extern __shared__ float s_tail[];
@@ -536,6 +550,11 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
     float(*smx)[TAIL] = reinterpret_cast<float(*)[TAIL]>(s_tail + 3 * TAIL);
     int* snode = reinterpret_cast<int*>(s_tail + 6 * TAIL);
     int* snn = reinterpret_cast<int*>(s_tail + 7 * TAIL);
+    // the clusters' cost and size (the w words of their boxes) and counts, so
+    // that a merge reads nothing from global memory
+    float* scost = s_tail + 8 * TAIL;
+    int* ssize = reinterpret_cast<int*>(s_tail + 9 * TAIL);
+    int2* scnt = reinterpret_cast<int2*>(s_tail + 10 * TAIL);
     __shared__ int s_wa[PB / 32 + 1], s_wb[PB / 32 + 1];
     __shared__ int s_n;
     if (*((volatile int*)A.err) != 0) return;
@@ -549,6 +568,9 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
         snode[c] = node;
         smn[0][c] = mn.x; smn[1][c] = mn.y; smn[2][c] = mn.z;
         smx[0][c] = mx.x; smx[1][c] = mx.y; smx[2][c] = mx.z;
+        scost[c] = mn.w;
+        ssize[c] = __float_as_int(mx.w);
+        scnt[c] = __ldcg(A.counts + node);
     }
     __syncthreads();
     for (int it = it0; N > 1 && it < MAX_ITER; ++it) {
@@ -587,6 +609,9 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
         // new entries in registers, then compaction
         int nnode[TAIL_ITEMS];
         float nmn[TAIL_ITEMS][3], nmx[TAIL_ITEMS][3];
+        float ncost[TAIL_ITEMS];
+        int nsize[TAIL_ITEMS];
+        int2 ncnt[TAIL_ITEMS];
         int pos[TAIL_ITEMS];
         int mr = em, kr = ek;
 #pragma unroll
@@ -596,15 +621,24 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
             if (kind[q] == 0) continue;
             nnode[q] = snode[c];
             for (int a = 0; a < 3; ++a) { nmn[q][a] = smn[a][c]; nmx[q][a] = smx[a][c]; }
+            ncost[q] = scost[c];
+            nsize[q] = ssize[c];
+            ncnt[q] = scnt[c];
             if (kind[q] == 2) {
                 const int j = snn[c];
                 const int idx = (N - 2) - mr++;
-                make_parent(A, idx, snode[c], snode[j]);
+                const float4 amn = make_float4(smn[0][c], smn[1][c], smn[2][c], scost[c]);
+                const float4 amx = make_float4(smx[0][c], smx[1][c], smx[2][c], __int_as_float(ssize[c]));
+                const float4 bmn = make_float4(smn[0][j], smn[1][j], smn[2][j], scost[j]);
+                const float4 bmx = make_float4(smx[0][j], smx[1][j], smx[2][j], __int_as_float(ssize[j]));
+                float4 omn, omx;
+                make_parent_from(A, idx, snode[c], snode[j], amn, amx, bmn, bmx, scnt[c], scnt[j], omn, omx,
+                                 ncnt[q]);
                 nnode[q] = idx;
-                for (int a = 0; a < 3; ++a) {
-                    nmn[q][a] = fminf(nmn[q][a], smn[a][j]);
-                    nmx[q][a] = fmaxf(nmx[q][a], smx[a][j]);
-                }
+                nmn[q][0] = omn.x; nmn[q][1] = omn.y; nmn[q][2] = omn.z;
+                nmx[q][0] = omx.x; nmx[q][1] = omx.y; nmx[q][2] = omx.z;
+                ncost[q] = omn.w;
+                nsize[q] = __float_as_int(omx.w);
             }
             pos[q] = kr++;
         }
@@ -614,6 +648,9 @@ __global__ void __launch_bounds__(PB, 1) k_ploc_tail(ploc_args A) {
             if (pos[q] < 0) continue;
             snode[pos[q]] = nnode[q];
             for (int a = 0; a < 3; ++a) { smn[a][pos[q]] = nmn[q][a]; smx[a][pos[q]] = nmx[q][a]; }
+            scost[pos[q]] = ncost[q];
+            ssize[pos[q]] = nsize[q];
+            scnt[pos[q]] = ncnt[q];
         }
         if (threadIdx.x == 0) s_n = N - tot.x;
         __syncthreads();
