@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(AB) k_atr_iter(atr_args A) {
             if ((unsigned)tri >= (unsigned)n) {
                 hp_report(A.err, HP_DEV_BAD_INDEX, p);
             } else {
-                const float4 mn = A.tbmin[tri], mx = A.tbmax[tri];
+                const float4 mn = A.tbmin[2 * (int64_t)tri], mx = A.tbmax[2 * (int64_t)tri];
                 const float c = __fmul_rn(A.ci, atr_area(mn.x, mn.y, mn.z, mx.x, mx.y, mx.z));
                 __stcg(A.nbmin + leaf, make_float4(mn.x, mn.y, mn.z, c));
                 __stcg(A.nbmax + leaf, make_float4(mx.x, mx.y, mx.z, __int_as_float(1)));
@@ -588,8 +588,8 @@ __global__ void __launch_bounds__(256) k_atr_finish(fin_args F) {
     if (F.init) {
         const int tri = F.sorted_tri[p];
         if ((unsigned)tri >= (unsigned)n) { hp_report(F.err, HP_DEV_BAD_INDEX, p); return; }
-        mn = F.tbmin[tri];
-        mx = F.tbmax[tri];
+        mn = F.tbmin[2 * (int64_t)tri];  // interleaved corners
+        mx = F.tbmax[2 * (int64_t)tri];
     } else {
         mn = __ldcg(F.nbmin + leaf);
         mx = __ldcg(F.nbmax + leaf);

@@ -55,8 +55,8 @@ __global__ void __launch_bounds__(TB) k_tri_boxes(const float* __restrict__ vert
               az = fminf(fminf(t.z0, t.z1), t.z2);
         float bx = fmaxf(fmaxf(t.x0, t.x1), t.x2), by = fmaxf(fmaxf(t.y0, t.y1), t.y2),
               bz = fmaxf(fmaxf(t.z0, t.z1), t.z2);
-        bmin[i] = make_float4(ax, ay, az, 0.0f);
-        bmax[i] = make_float4(bx, by, bz, 0.0f);
+        bmin[2 * i] = make_float4(ax, ay, az, 0.0f);  // min / max interleaved (32 B per triangle)
+        bmax[2 * i] = make_float4(bx, by, bz, 0.0f);
         if (woop) {
             float4 w0, w1, w2;
             hp_woop(t.x0, t.y0, t.z0, t.x1, t.y1, t.z1, t.x2, t.y2, t.z2, w0, w1, w2);
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(TB) k_morton(const float4* __restrict__ bmin,
     if (blockIdx.x == 0 && threadIdx.x < 3) info->scale[threadIdx.x] = scale[threadIdx.x];
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)TB + threadIdx.x; i < n; i += (int64_t)gridDim.x * TB) {
-        float4 a = bmin[i], b = bmax[i];
+        float4 a = bmin[2 * i], b = bmax[2 * i];
         uint64_t key = hp_morton_key(a.x, a.y, a.z, b.x, b.y, b.z, smin, scale, bits);
         keys[i] = (K)key;
         for (int p = 0; p < passes; ++p) {  // the sort's digits (hp_sort_hist_digits)
@@ -594,8 +594,11 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     }
     HP_TRY(hp_ctx_reserve(ctx, need, s));
     hp_carve cv(ctx->arena);
-    float4* tbmin = cv.take<float4>(n);
-    float4* tbmax = cv.take<float4>(n);
+    // triangle boxes, min and max corners interleaved: element i at [2 i] of
+    // tbmin and tbmax, so that a gather in sorted order reads one 32-byte sector
+    float4* tbox = cv.take<float4>(2 * n);
+    float4* tbmin = tbox;
+    float4* tbmax = tbox + 1;
     K* keys = cv.take<K>(n);
     K* skeys = cv.take<K>(n);
     void* sort_scratch = cv.take<char>(plan.scratch_bytes);

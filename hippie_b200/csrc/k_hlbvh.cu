@@ -68,8 +68,8 @@ __global__ void __launch_bounds__(HB) k_hl_refit(int n, const int32_t* __restric
     const int tri = __ldg(sorted_tri + p);
     if ((unsigned)tri >= (unsigned)n) { hp_report(err, HP_DEV_BAD_INDEX, p); return; }
     const int leaf = n - 1 + p;
-    __stcg(nbmin + leaf, __ldg(tbmin + tri));
-    __stcg(nbmax + leaf, __ldg(tbmax + tri));
+    __stcg(nbmin + leaf, __ldg(tbmin + 2 * (int64_t)tri));  // interleaved corners
+    __stcg(nbmax + leaf, __ldg(tbmax + 2 * (int64_t)tri));
     int node = __ldcg(parent + leaf), guard = 0;
     while (node >= 0) {
         if (node >= n - 1 || ++guard > n) { hp_report(err, HP_DEV_BAD_INDEX, node); return; }

@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) k_ploc_leaves(ploc_args A, const int32_t*
     const int p = blockIdx.x * 256 + threadIdx.x;
     if (p >= A.n) return;
     const int tri = sorted_tri[p];
-    const float4 mn = tbmin[tri], mx = tbmax[tri];
+    const float4 mn = tbmin[2 * (int64_t)tri], mx = tbmax[2 * (int64_t)tri];  // interleaved corners
     const int j = A.n - 1 + p;
     const float cost = A.adaptive_leaf ? __fmul_rn(A.ci, hp_area(mn.x, mn.y, mn.z, mx.x, mx.y, mx.z)) : 0.0f;
     A.nbmin[j] = make_float4(mn.x, mn.y, mn.z, cost);
