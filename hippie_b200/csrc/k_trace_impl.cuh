@@ -215,13 +215,11 @@ __global__ void __launch_bounds__(TRACE_BLOCK, BATCH ? 9 : 12) k_trace(
                 }
                 for (int tri = begin; tri < end; ++tri) {
                     if (STATS) ++r.tris;
-                    // Single-mesh launches load the first two Woop rows at once (the
-                    // second is needed whenever the plane is hit in range): one round
-                    // trip fewer per tested triangle. The batch variant, which holds
-                    // more state per lane, loads each row when it needs it.
+                    // The first two Woop rows at once (the second is needed whenever the
+                    // plane is hit in range): one round trip fewer per tested triangle;
+                    // the third when u >= 0.
                     const float4 v0 = __ldg(woop + 3 * (int64_t)tri);
-                    const float4 v1pre = BATCH ? make_float4(0.0f, 0.0f, 0.0f, 0.0f)
-                                               : __ldg(woop + 3 * (int64_t)tri + 1);
+                    const float4 v1 = __ldg(woop + 3 * (int64_t)tri + 1);
                     const float oz = __fmaf_rn(-r.oz, v0.z, __fmaf_rn(-r.oy, v0.y, __fmaf_rn(-r.ox, v0.x, v0.w)));
                     // The roundings of the reference's fast-math tracer, measured
                     // against its output on sm_100a: the chains o.w +- ... are
@@ -235,7 +233,6 @@ __global__ void __launch_bounds__(TRACE_BLOCK, BATCH ? 9 : 12) k_trace(
                     if (!closer && t == r.hit_t && r.hit >= 0)
                         closer = __ldg(tri_idx + tri) < __ldg(tri_idx + r.hit);
                     if (t > r.tmin && closer) {
-                        const float4 v1 = BATCH ? __ldg(woop + 3 * (int64_t)tri + 1) : v1pre;
                         const float ox = __fmaf_rn(r.oz, v1.z, __fmaf_rn(r.oy, v1.y, __fmaf_rn(r.ox, v1.x, v1.w)));
                         const float dx = __fmaf_rn(r.dz, v1.z, __fmaf_rn(r.dy, v1.y, __fmul_rn(r.dx, v1.x)));
                         const float u = __fmaf_rn(t, dx, ox);
