@@ -608,6 +608,11 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
     hp_bvh_info* info = out->info;
     const int grid_n = hp_div_up(n, TB);
     const int grid_red = (int)std::min<int64_t>(grid_n, (int64_t)ctx->sm_count * 8);
+    // the Morton kernel's grid: the CTAs resident at once (a partial second
+    // round of CTAs would run at a fraction of the SMs' occupancy)
+    int occ_m = 0;
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_morton<K>, TB, 0));
+    const int grid_mor = (int)std::min<int64_t>(grid_n, (int64_t)ctx->sm_count * std::max(1, occ_m));
     if (ploc) {
         int32_t* sorted_refs = cv.take<int32_t>(n);
         void* ploc_scratch = cv.take<char>(hp_ploc_scratch_bytes(n));
@@ -617,7 +622,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                             info->box_ord, err, woop_src);
         hp_count_launch(2);
         hp_mark(ctx, s, "boxes");
-        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
+        k_morton<K><<<grid_mor, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(ctx, s, "morton");
@@ -650,7 +655,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                             info->box_ord, err);
         hp_count_launch(2);
         hp_mark(ctx, s, "boxes");
-        k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
+        k_morton<K><<<grid_mor, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
         HP_CUDA(cudaGetLastError());
         hp_count_launch();
         hp_mark(ctx, s, "morton");
@@ -711,7 +716,7 @@ hp_status lbvh_t(hp_ctx* ctx, const hp_mesh* m, const hp_build_params* p, hp_bvh
                                         info->box_ord, err);
     hp_count_launch(2);
     hp_mark(ctx, s, "boxes");
-    k_morton<K><<<grid_red, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
+    k_morton<K><<<grid_mor, TB, 0, s>>>(tbmin, tbmax, n, info, bits, h_shift, h_count, keys, hist);
     HP_CUDA(cudaGetLastError());
     hp_count_launch();
     hp_mark(ctx, s, "morton");

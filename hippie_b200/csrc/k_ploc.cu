@@ -45,7 +45,11 @@ constexpr int LPB = 512;            // threads per CTA of the iteration kernel (
 constexpr int MAXR = 512;           // largest radius kept in a shared-memory window
 constexpr int NB4 = 4;              // clusters per thread of the neighbour search on large lists
 constexpr int WIN = NB4 * LPB + 2 * MAXR;  // neighbour window
-constexpr int NB4_MIN_N = 2 * 148 * NB4 * 1024;  // lists at least this long use 4 clusters per thread
+// Lists at least this long use 4 clusters per thread (long tiles, about half as
+// many tiles as the loop has CTAs at this length). On a B200 this beat twice
+// and four times the length, half and a quarter of it, and long tiles at every
+// length, on clustered and uniform scenes of 1 M to 16 M triangles.
+constexpr int NB4_MIN_N = 148 * NB4 * 512;
 // Shorter lists run fused iterations: a tile of LPB clusters finds the nearest
 // neighbours of its clusters and of r clusters on each side itself, so each
 // iteration needs one grid barrier instead of two.
