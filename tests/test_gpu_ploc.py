@@ -43,8 +43,9 @@ def test_ploc_bit_exact(ctx, n):
 @pytest.mark.parametrize("n,radius,adaptive", [(1_500_000, 16, 0), (1_300_000, 2, 0), (1_250_000, 4, 0),
                                                (1_400_000, 7, 0), (1_300_000, 3, 1)])
 def test_ploc_bit_exact_long_lists(ctx, n, radius, adaptive):
-    """Lists of at least 2 * 148 * 4096 clusters take the neighbour search with
-    four clusters per thread (its run split for r >= 4, the tested path below)."""
+    """Lists of at least 148 * 4 * 512 clusters take the neighbour search with
+    four clusters per thread (its run split for r >= 4, the tested path below);
+    these builds run it down to that length and the one-cluster tiles after."""
     v, t = hp.gen.clustered_mesh(700 + n, n, clusters=1024)
     bvh, ref, V, T = _ploc(ctx, v, t, ploc_radius=radius, ploc_max_radius=max(radius, 9), ploc_adaptive=adaptive)
     nodes, woop, tri = bvh.download()
