@@ -169,7 +169,6 @@ struct treelet_lane {
 
 __device__ bool form_treelet(const atr_args& A, int T, int root, int l0, int r0, treelet_lane& L) {
     const int lane = threadIdx.x & 31;
-    const int n = A.n;
     int tl = lane == 0 ? l0 : (lane == 1 ? r0 : -1);
     int ti = lane == 0 ? root : -1;
     int kl = -1, kr = -1;

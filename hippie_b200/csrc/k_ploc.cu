@@ -66,11 +66,6 @@ constexpr int TAIL_ITEMS = TAIL / PB;
 constexpr int MAX_ITER = 1 << 16;
 constexpr unsigned SPIN = 1u << 22;
 
-__device__ __forceinline__ unsigned ld_vol_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 // Acquire load / release store at GPU scope: a record written before the
 // release store is visible to a thread whose acquire load sees the flag.
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
