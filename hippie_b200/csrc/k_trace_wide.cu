@@ -63,6 +63,9 @@ __global__ void __launch_bounds__(TB1, N == 4 ? 10 : 8) k_trace_wide1(const floa
     constexpr int STACK = wide1_cfg<N>::STACK, LST = STACK - SST1;
     __shared__ int s_stack[SST1 * TB1];
     int* sstack = s_stack + threadIdx.x;
+    // Entries past the shared part. Left uninitialised: sp counts the pushes
+    // that were stored (an overflowing push is dropped and reported), so a pop
+    // reads only entries a push wrote.
     int lstack[LST];
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
